@@ -1,0 +1,228 @@
+/*
+ * radb200.h -- C-ABI of the B200 (sm_100a) relaxation hot path for Radia.
+ *
+ * This library replaces Radia's CUDA plugin layer (the radGPU_* seam between
+ * radTInteraction / radTApplication and the device) with a new implementation:
+ *   - interaction-matrix assembly     (replaces radGPU_AssembleMatrix,
+ *                                       cpp/src/core/radgpu_asm.h:166-173)
+ *   - magnetization relaxation        (replaces radGPU_RelaxAuto / radGPU_RelaxNK,
+ *                                       cpp/src/core/radgpurlx.h:69-87)
+ *   - dense direct solve, adjoint     (no counterpart in the reference)
+ *   - B/H field evaluation            (replaces radGPU_ComputeField,
+ *                                       cpp/src/core/radgpu_fld.h:107-198, and
+ *                                       the host coil loop radgpu_fld.cpp:542-617)
+ *
+ * Every entry point takes plain pointers and sizes.  Geometry is handed over
+ * as flat arrays (RadB200Geom), which is what the reference's packers
+ * (radGPU_PackGeometryForAsm radgpu_asm.cpp:206-444, CollectElementsRecursive
+ * radgpu_fld.cpp:194-317) produce from the object tree; the difference is that
+ * symmetry / orientation images stay a separate transform table which the
+ * kernels apply in-kernel instead of duplicating records on the host.
+ *
+ * Conventions (identical to the reference): lengths in mm, B, H and M in
+ * Tesla (mu0*H), current density in A/mm^2.  All functions return 0 on
+ * success and a negative RADB200_E* code on failure; radb200_last_error()
+ * returns a message.  No function aborts or traps.  The library is not
+ * reentrant (one global device context, like the reference's static caches).
+ */
+#ifndef RADB200_H
+#define RADB200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RADB200_API __attribute__((visibility("default")))
+#else
+#define RADB200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ------------------------------------------------------- */
+#define RADB200_OK            0
+#define RADB200_E_ARG        -1   /* bad argument / size                     */
+#define RADB200_E_CUDA       -2   /* CUDA runtime error                      */
+#define RADB200_E_NOMEM      -3   /* device allocation failed / too large    */
+#define RADB200_E_HANDLE     -4   /* unknown interaction handle              */
+#define RADB200_E_NUMERIC    -5   /* non-finite result / breakdown           */
+#define RADB200_E_NOCONV     -6   /* iteration cap reached before tolerance  */
+#define RADB200_E_TIMEOUT    -7   /* a bounded device wait ran out           */
+#define RADB200_E_UNSUPPORTED -8  /* feature not available for this input    */
+
+/* ---- image transform record -------------------------------------------
+ * One record per (source, image).  Mirrors gmTrans (ext/genmath/gmtrans.h:22-84):
+ * an image maps a point of the source's own frame to the lab frame as
+ * P_lab = M*P + V and a field vector as F_lab = s*M*F (TrVectField).
+ * Stored as RADB200_TRF_STRIDE doubles:
+ *   [0..8]   M^-1 (row major)      P_obj = M^-1 * (P_lab - V)
+ *   [9..11]  V
+ *   [12..20] s*M (row major)       field map object frame -> lab frame
+ *   [21]     s                     [22] det(M)    [23] unused               */
+#define RADB200_TRF_STRIDE 24
+
+/* ---- source records ------------------------------------------------------ */
+#define RADB200_REC_STRIDE  12  /* cx cy cz  wx wy wz  mx my mz  jx jy jz      */
+#define RADB200_POLY_STRIDE 6   /* centre xyz (vertex mean), magnetization xyz */
+#define RADB200_FACE_STRIDE 10  /* R (9, object -> face-local rows), coordZ    */
+#define RADB200_ARC_STRIDE  10  /* cx cy cz rmin rmax phimin phimax h j nseg   */
+
+typedef struct RadB200Geom {
+  int32_t n_trf;             /* transform table                              */
+  const double *trf;         /* [n_trf * RADB200_TRF_STRIDE]                 */
+
+  int32_t n_rec;             /* rectangular blocks: radTRecMag (M and/or J)  */
+  const double *rec;         /* [n_rec * RADB200_REC_STRIDE], object frame   */
+  const int32_t *rec_img;    /* [n_rec * 2] first transform, image count     */
+
+  int32_t n_poly;            /* polyhedra: radTPolyhedron                    */
+  const double *poly;        /* [n_poly * RADB200_POLY_STRIDE]               */
+  const int32_t *poly_info;  /* [n_poly * 4] first face, faces, first trf, images */
+  int32_t n_face;
+  const double *face;        /* [n_face * RADB200_FACE_STRIDE]               */
+  const int32_t *face_vtx;   /* [n_face * 2] first 2-D vertex, vertex count  */
+  int32_t n_vtx;
+  const double *vtx2d;       /* [n_vtx * 2] counter-clockwise, face frame    */
+
+  int32_t n_arc;             /* arc currents: radTArcCur, trapezoid in phi   */
+  const double *arc;         /* [n_arc * RADB200_ARC_STRIDE]                 */
+  const int32_t *arc_img;    /* [n_arc * 2]                                  */
+
+  int32_t n_bkg;             /* uniform background fields: ObjBckg           */
+  const double *bkg;         /* [n_bkg * 3]                                  */
+  const int32_t *bkg_img;    /* [n_bkg * 2]                                  */
+
+  /* length-randomization guard magnitudes (radTConvergRepair,
+   * cpp/src/core/radcnvrg.h:29-92); all zero after FldLenRndSw('off'). */
+  double abs_rand, rel_rand, zero_rand;
+} RadB200Geom;
+
+/* ---- relaxable elements and materials -----------------------------------
+ * Element e is source rec[elem_src[2e+1]] (elem_src[2e]==0) or
+ * poly[elem_src[2e+1]] (elem_src[2e]==1).  Its FIRST image is its main
+ * transform (all symmetry powers zero, radintrc.cpp:557-573); magnetization
+ * and field of the relaxation live in that frame (the element's own frame).
+ * Material record, RADB200_MAT_STRIDE doubles per element:
+ *   kind 0 (linear):   [0..8] chi tensor, [9..11] Mr          (radmater.h:164-362)
+ *   kind 1 (tanh):     [0..2] ksi_i, [3..5] ms_i, [6] count, [9..11] Mr
+ *                      |M| = sum ms_i tanh(ksi_i |H| / ms_i)  (radmater.h:417-600)
+ *   kind 2 (table):    [0] first point, [1] count into mh_table (H, M, dM/dH)  */
+#define RADB200_MAT_STRIDE 12
+#define RADB200_MAT_LINEAR 0
+#define RADB200_MAT_TANH   1
+#define RADB200_MAT_TABLE  2
+
+typedef struct RadB200Relax {
+  int32_t n_elem;
+  const int32_t *elem_src;   /* [n_elem * 2] kind (0 rec, 1 poly), index     */
+  const int32_t *mat_kind;   /* [n_elem]                                     */
+  const double *mat;         /* [n_elem * RADB200_MAT_STRIDE]                */
+  int32_t n_mh;
+  const double *mh_table;    /* [n_mh * 3]  H, M, dM/dH                      */
+} RadB200Relax;
+
+/* ---- general ------------------------------------------------------------- */
+RADB200_API const char *radb200_last_error(void);
+RADB200_API int radb200_version(void);                      /* 100 * major + minor       */
+/* Number of this library's kernels launched since load (all entry points). */
+RADB200_API int64_t radb200_kernel_launches(void);
+RADB200_API int radb200_device_sync(void);
+
+/* ---- field evaluation ------------------------------------------------------
+ * Replaces radGPU_ComputeField (radgpu_fld.h:183-198) and the reference's
+ * host coil loop.  what: 0 = B, 1 = H, 2 = M (magnetization at the point).
+ * precision: 0 = FP64, 1 = FP32 polygon/cuboid terms with FP64 accumulation
+ * (the reference's use_gpu == 2).  pts/out are HOST arrays [npts*3]; the
+ * call copies them to and from the device.                                   */
+RADB200_API int radb200_field(const RadB200Geom *g, const double *pts, int64_t npts,
+                  int what, int precision, double *out);
+/* Same, with pts/out already in device memory (cudaStream 0 ordering).      */
+RADB200_API int radb200_field_dev(const RadB200Geom *g, const double *d_pts, int64_t npts,
+                      int what, int precision, double *d_out);
+
+/* ---- interaction (assembly + solver state) ---------------------------------
+ * Replaces radGPU_PackGeometryForAsm + radGPU_AssembleMatrix +
+ * radGPU_PublishAssembledMatrix (radgpu_asm.h:149-187): assembles the dense
+ * 3N x 3N interaction matrix (block (i,j) = H in element i's frame at i's
+ * centre from unit magnetization of element j, images folded in,
+ * radintrc.cpp:831-877) and the external field from every non-relaxable
+ * source (radintrc.cpp:1208-1234) into device memory, where it stays for the
+ * solves.  storage: 0 = FP32 matrix (the reference's layout),
+ * 1 = FP64 matrix, 2 = FP32 matrix plus an FP64 copy of the near blocks.
+ * ext may be NULL (no external sources).                                     */
+#define RADB200_STORE_F32   0
+#define RADB200_STORE_F64   1
+#define RADB200_STORE_MIXED 2
+RADB200_API int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r,
+                         const RadB200Geom *ext, int storage, int64_t *handle);
+RADB200_API int radb200_intrc_free(int64_t handle);
+RADB200_API int radb200_intrc_size(int64_t handle, int32_t *n_elem, int32_t *storage);
+/* Copy the interaction matrix (row major, 3N x 3N) to a host buffer, as FP32
+ * or FP64 (dtype 0 / 1), and the external field H_ext [3N].                 */
+RADB200_API int radb200_intrc_matrix(int64_t handle, int dtype, void *out);
+RADB200_API int radb200_intrc_extfield(int64_t handle, double *out);
+/* Replace the external field (e.g. after a source update, RlxUpdSrc).       */
+RADB200_API int radb200_intrc_set_extfield(int64_t handle, const double *h_ext);
+
+/* ---- relaxation ------------------------------------------------------------
+ * Replaces radGPU_AutoRelax (method 9) and radGPU_AutoRelaxNK (method 11),
+ * radrlmet_gpu.cpp:9-99.  method:
+ *   RADB200_RLX_JACOBI   device-resident under-relaxed Jacobi with per-element
+ *                        implicit material solve and Anderson mixing
+ *                        (methods 4/9/10 of the reference reach the same
+ *                        fixed point);
+ *   RADB200_RLX_NEWTON   Newton-Krylov with right-preconditioned GMRES (method 11).
+ * M_io: [3N] magnetization in each element's frame; read when reset == 0,
+ * always written.  H_out: [3N] or NULL.  status: [4] = misfit (RMS of the last
+ * undamped step, T), max|M|, max|H|, iterations (radsend.cpp:1009-1024).   */
+#define RADB200_RLX_JACOBI 0
+#define RADB200_RLX_NEWTON 1
+RADB200_API int radb200_relax(int64_t handle, int method, double prec, int max_iter,
+                  int reset, double omega, double *M_io, double *H_out,
+                  double *status);
+
+/* ---- dense direct solve (linear materials) --- no counterpart in the reference.
+ * Solves (I - X N) M = X H_ext + Mr by a blocked LU of A = I - X N on the
+ * device.  mode: RADB200_LU_F64 = FP64 LU (+ one FP64 refinement step);
+ * RADB200_LU_TF32 = LU with TF32 tensor-core trailing updates (tcgen05,
+ * FP32 accumulate) followed by FP64 GMRES iterative refinement to rtol.
+ * The factorization is kept with the interaction for later solves (adjoint).
+ * status: [4] = final relative FP64 residual, refinement (GMRES) iterations,
+ * factor seconds, total seconds.                                             */
+#define RADB200_LU_F64  0
+#define RADB200_LU_TF32 1
+RADB200_API int radb200_direct_solve(int64_t handle, int mode, double rtol, int max_iter,
+                         double *M_out, double *status);
+
+/* ---- adjoint --- no counterpart in the reference.
+ * Given the converged magnetization of the last solve and dL/dM [3N] (each
+ * element's frame), solves the transposed system (I - D N)^T lambda = dL/dM
+ * with D = dM/dH at the converged state (radmater.cpp:206-277) and returns
+ * lambda [3N].  Uses the LU factors when the last solve was direct (linear),
+ * otherwise GMRES on the transposed operator.                                */
+RADB200_API int radb200_adjoint_solve(int64_t handle, const double *dLdM, double rtol,
+                          int max_iter, double *lambda_out, double *status);
+
+/* Sensitivities of a scalar loss L(M) through the converged relaxation, with
+ * respect to the per-element remanence Mr [3N] (dL/dMr = D_r^T lambda, where
+ * D_r = dM/dMr = I for every law here), and the centre of each RECTANGULAR
+ * element (dL/dc [3N], from lambda^T (dN/dc) M recomputed on the fly by
+ * differentiating the block formulas; images included).                      */
+RADB200_API int radb200_adjoint_grad(int64_t handle, const double *lambda,
+                         double *dL_dMr, double *dL_dc);
+
+/* Field-operator part of the adjoint: for a loss on field values at points,
+ * given W = dL/dF [npts*3] (F = B or H at pts), returns
+ *   g_M [3N]  = (dF/dM)^T W       (the field operator's transpose applied to W)
+ *   g_c [3N]  = d(W.F)/dc_e       (rectangular element centres, M held fixed)
+ * evaluated for the current magnetization M [3N] of the relaxable elements
+ * of this interaction.                                                       */
+RADB200_API int radb200_field_vjp(int64_t handle, const double *M, const double *pts,
+                      int64_t npts, int what, const double *W,
+                      double *g_M, double *g_c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RADB200_H */

@@ -1,0 +1,204 @@
+// field.cu -- B / H / M at observation points from all field sources.
+//
+// Replaces radGPU_FldKernelT + radGPU_FldRecMagKernel + their partial-sum
+// reductions (reference radgpu_fld.cu:381-553, 788-909) and the host coil
+// loop (radgpu_fld.cpp:542-617).  Design:
+//   - one thread per observation point, FP64 accumulation in registers;
+//   - every thread of a CTA walks the same (source, image) unit list, so the
+//     source records are warp-uniform loads served by L1 broadcast -- no
+//     shared-memory staging is needed because each record feeds hundreds of
+//     transcendental operations;
+//   - symmetry / orientation images are applied in-kernel (point mapped into
+//     the source's own frame, field mapped back with s*M);
+//   - coils (arc currents, current cuboids) and background fields run on the
+//     device with the magnets;
+//   - when there are too few points to fill the GPU, the unit list is split
+//     over gridDim.y chunks whose partial sums land in a scratch buffer and
+//     are added in a fixed order (bitwise reproducible).
+#include "internal.cuh"
+
+namespace rb {
+
+template <typename T>
+__device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<double> P, int what)
+{
+  const double *Tr = g.trf + (size_t)u.z * RADB200_TRF_STRIDE;
+  // point in the source's own frame: q = M^-1 (P - V)
+  double dx = P.x - __ldg(Tr + 9), dy = P.y - __ldg(Tr + 10), dz = P.z - __ldg(Tr + 11);
+  V3<double> q = mk3<double>(__ldg(Tr + 0) * dx + __ldg(Tr + 1) * dy + __ldg(Tr + 2) * dz,
+                             __ldg(Tr + 3) * dx + __ldg(Tr + 4) * dy + __ldg(Tr + 5) * dz,
+                             __ldg(Tr + 6) * dx + __ldg(Tr + 7) * dy + __ldg(Tr + 8) * dz);
+  V3<double> f = mk3<double>(0, 0, 0);
+  if (u.x == 0) {
+    const double *r = g.rec + (size_t)u.y * RADB200_REC_STRIDE;
+    double jx = __ldg(r + 9), jy = __ldg(r + 10), jz = __ldg(r + 11);
+    V3<double> qc = mk3<double>(q.x - __ldg(r + 0), q.y - __ldg(r + 1), q.z - __ldg(r + 2));
+    V3<double> hd = mk3<double>(0.5 * __ldg(r + 3), 0.5 * __ldg(r + 4), 0.5 * __ldg(r + 5));
+    if (jx != 0.0 || jy != 0.0 || jz != 0.0) {
+      if (what != 2) f = cuboid_J(qc, hd, mk3<double>(jx, jy, jz), g.g);
+    } else {
+      double mx = __ldg(r + 6), my = __ldg(r + 7), mz = __ldg(r + 8);
+      if (what == 2) {
+        int in = (fabs(qc.x) < hd.x) && (fabs(qc.y) < hd.y) && (fabs(qc.z) < hd.z);
+        if (in) f = mk3<double>(mx, my, mz);
+      } else {
+        V3<T> Tt, Ss;
+        int in = cuboid_TS<T>(mk3<T>(T(qc.x), T(qc.y), T(qc.z)), mk3<T>(T(hd.x), T(hd.y), T(hd.z)), g.g, Tt, Ss);
+        double Tx = Tt.x, Ty = Tt.y, Tz = Tt.z, Sx = Ss.x, Sy = Ss.y, Sz = Ss.z;
+        f = mk3<double>(Tx * mx - Sz * my - Sy * mz, -Sz * mx + Ty * my - Sx * mz, -Sy * mx - Sx * my + Tz * mz);
+        if (what == 0 && in) { f.x += mx; f.y += my; f.z += mz; }
+      }
+    }
+  } else if (u.x == 1) {
+    const double *pr = g.poly + (size_t)u.y * RADB200_POLY_STRIDE;
+    double mx = __ldg(pr + 3), my = __ldg(pr + 4), mz = __ldg(pr + 5);
+    int f0 = __ldg(g.poly_info + 4 * u.y), nf = __ldg(g.poly_info + 4 * u.y + 1);
+    const double CH = 1.0 / (4.0 * 3.14159265358979);
+    int inside = 1;
+    double hx = 0, hy = 0, hz = 0;
+    for (int fi = f0; fi < f0 + nf; fi++) {
+      const double *R = g.face + (size_t)fi * RADB200_FACE_STRIDE;
+      double r0 = __ldg(R + 0), r1 = __ldg(R + 1), r2 = __ldg(R + 2), r3 = __ldg(R + 3), r4 = __ldg(R + 4),
+             r5 = __ldg(R + 5), r6 = __ldg(R + 6), r7 = __ldg(R + 7), r8 = __ldg(R + 8), cz = __ldg(R + 9);
+      // local normal component of M (row 2 of R)
+      double mloc = r6 * mx + r7 * my + r8 * mz;
+      int v0 = __ldg(g.face_vtx + 2 * fi), nv = __ldg(g.face_vtx + 2 * fi + 1);
+      const double *vt = g.vtx2d + 2 * (size_t)v0;
+      double cx = 0, cy = 0;
+      if (g.g.absr != 0.0 || g.g.relr != 0.0 || g.g.zeror != 0.0) {
+        for (int k = 0; k < nv; k++) { cx += __ldg(vt + 2 * k); cy += __ldg(vt + 2 * k + 1); }
+        cx /= nv; cy /= nv;
+      }
+      double plx = r0 * q.x + r1 * q.y + r2 * q.z, ply = r3 * q.x + r4 * q.y + r5 * q.z, plz = r6 * q.x + r7 * q.y + r8 * q.z;
+      int in;
+      double s0, s1, s2;
+      if (sizeof(T) == 8 || nv > 8) {
+        in = polygon_S<double, double>(vt, nv, cz, cx, cy, mk3<double>(plx, ply, plz), g.g, s0, s1, s2);
+      } else {
+        // single precision: shift to the first vertex so FP32 sees small numbers
+        float vbuf[16];
+        int nvc = nv;
+        double ox = __ldg(vt), oy = __ldg(vt + 1);
+        for (int k = 0; k < nvc; k++) { vbuf[2 * k] = float(__ldg(vt + 2 * k) - ox); vbuf[2 * k + 1] = float(__ldg(vt + 2 * k + 1) - oy); }
+        float a0, a1, a2;
+        in = polygon_S<float, float>(vbuf, nvc, float(cz - plz), float(cx - ox), float(cy - oy),
+                                     mk3<float>(float(plx - ox), float(ply - oy), 0.0f), g.g, a0, a1, a2);
+        s0 = a0; s1 = a1; s2 = a2;
+      }
+      if (!in) inside = 0;
+      if (what != 2) {
+        double w = -CH * mloc;
+        // H_obj += R^T (w S)
+        hx += w * (r0 * s0 + r3 * s1 + r6 * s2);
+        hy += w * (r1 * s0 + r4 * s1 + r7 * s2);
+        hz += w * (r2 * s0 + r5 * s1 + r8 * s2);
+      }
+    }
+    if (what == 2) f = inside ? mk3<double>(mx, my, mz) : mk3<double>(0, 0, 0);
+    else {
+      f = mk3<double>(hx, hy, hz);
+      if (what == 0 && inside) { f.x += mx; f.y += my; f.z += mz; }
+    }
+  } else if (u.x == 2) {
+    if (what != 2) f = arc_field(g.arc + (size_t)u.y * RADB200_ARC_STRIDE, q);
+  } else {
+    if (what != 2) {
+      const double *b = g.bkg + 3 * (size_t)u.y;
+      f = mk3<double>(__ldg(b), __ldg(b + 1), __ldg(b + 2));
+    }
+  }
+  const double *F = Tr + 12;  // s*M
+  return mk3<double>(__ldg(F + 0) * f.x + __ldg(F + 1) * f.y + __ldg(F + 2) * f.z,
+                     __ldg(F + 3) * f.x + __ldg(F + 4) * f.y + __ldg(F + 5) * f.z,
+                     __ldg(F + 6) * f.x + __ldg(F + 7) * f.y + __ldg(F + 8) * f.z);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) field_kernel(GeomView g, const double *__restrict__ pts, int64_t npts,
+                                                    int what, double *__restrict__ out, int chunk)
+{
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int u0 = blockIdx.y * chunk, u1 = min(g.n_units, u0 + chunk);
+  bool active = i < npts;
+  V3<double> P = mk3<double>(0, 0, 0);
+  if (active) P = mk3<double>(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+  double ax = 0, ay = 0, az = 0;
+  for (int u = u0; u < u1; u++) {
+    int4 un = __ldg(g.units + u);
+    V3<double> f = eval_unit<T>(g, un, P, what);
+    ax += f.x; ay += f.y; az += f.z;
+  }
+  if (active) {
+    double *o = out + ((size_t)blockIdx.y * npts + i) * 3;
+    o[0] = ax; o[1] = ay; o[2] = az;
+  }
+}
+
+// out[i] = sum_c partial[c][i], fixed order c = 0..nc-1
+__global__ void chunk_reduce_kernel(const double *__restrict__ part, int nc, int64_t n3, double *__restrict__ out)
+{
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n3) return;
+  double s = 0;
+  for (int c = 0; c < nc; c++) s += part[(size_t)c * n3 + i];
+  out[i] = s;
+}
+
+int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what, int precision, double *d_out,
+                 DBuf &scratch, cudaStream_t st)
+{
+  if (npts <= 0) return 0;
+  if (g.n_units == 0) {
+    RB_CUDA(cudaMemsetAsync(d_out, 0, (size_t)npts * 3 * sizeof(double), st));
+    return 0;
+  }
+  const int TPB = 128;
+  int64_t nblk = (npts + TPB - 1) / TPB;
+  if (nblk > INT32_MAX) { set_error("too many points"); return RADB200_E_ARG; }
+  // split the unit list when the points alone give fewer than ~8 CTAs per SM
+  int nchunk = 1;
+  const int64_t target = 148 * 8;
+  if (nblk < target) nchunk = (int)((target + nblk - 1) / nblk);
+  if (nchunk > g.n_units) nchunk = g.n_units;
+  if (nchunk > 65535) nchunk = 65535;
+  int chunk = (g.n_units + nchunk - 1) / nchunk;
+  nchunk = (g.n_units + chunk - 1) / chunk;
+  double *dst = d_out;
+  if (nchunk > 1) {
+    RB_TRY(scratch.alloc((size_t)nchunk * npts * 3 * sizeof(double)));
+    dst = scratch.as<double>();
+  }
+  dim3 grid((unsigned)nblk, (unsigned)nchunk);
+  if (precision == 1)
+    field_kernel<float><<<grid, TPB, 0, st>>>(g, d_pts, npts, what, dst, chunk);
+  else
+    field_kernel<double><<<grid, TPB, 0, st>>>(g, d_pts, npts, what, dst, chunk);
+  RB_TRY(check_launch("field_kernel"));
+  if (nchunk > 1) {
+    int64_t n3 = npts * 3;
+    chunk_reduce_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(dst, nchunk, n3, d_out);
+    RB_TRY(check_launch("chunk_reduce_kernel"));
+  }
+  return 0;
+}
+
+// out_i = rowT_i * in_i  (3x3 per element)
+__global__ void rowtrans_kernel(const double *__restrict__ rowT, const double *__restrict__ in, double *__restrict__ out, int n)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double *R = rowT + 9 * (size_t)i;
+  double x = in[3 * i], y = in[3 * i + 1], z = in[3 * i + 2];
+  out[3 * i] = R[0] * x + R[1] * y + R[2] * z;
+  out[3 * i + 1] = R[3] * x + R[4] * y + R[5] * z;
+  out[3 * i + 2] = R[6] * x + R[7] * y + R[8] * z;
+}
+
+int launch_rowtrans_vec(const double *rowT, const double *in, double *out, int n, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  rowtrans_kernel<<<(n + 127) / 128, 128, 0, st>>>(rowT, in, out, n);
+  return check_launch("rowtrans_kernel");
+}
+
+}  // namespace rb

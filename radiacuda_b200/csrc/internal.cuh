@@ -1,0 +1,160 @@
+// internal.cuh -- shared declarations of the libradb200 translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/radb200.h"
+#include "formulas.cuh"
+
+namespace rb {
+
+// ---- errors / bookkeeping --------------------------------------------------
+void set_error(const char *fmt, ...);
+extern long long g_launches;          // kernels launched by this library
+int check_launch(const char *what);   // cudaGetLastError after a launch
+
+#define RB_CUDA(x)                                                                  \
+  do {                                                                              \
+    cudaError_t e_ = (x);                                                           \
+    if (e_ != cudaSuccess) {                                                        \
+      ::rb::set_error("%s:%d %s: %s", __FILE__, __LINE__, #x, cudaGetErrorString(e_)); \
+      return RADB200_E_CUDA;                                                        \
+    }                                                                               \
+  } while (0)
+#define RB_TRY(x)            \
+  do {                       \
+    int r_ = (x);            \
+    if (r_ != 0) return r_;  \
+  } while (0)
+
+// ---- device buffers ----------------------------------------------------------
+struct DBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DBuf() {}
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { release(); }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  int alloc(size_t b)
+  {
+    if (b <= bytes && p) return 0;
+    release();
+    if (b == 0) return 0;
+    if (cudaMalloc(&p, b) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("device allocation of %zu bytes failed", b);
+      p = nullptr;
+      return RADB200_E_NOMEM;
+    }
+    bytes = b;
+    return 0;
+  }
+  int upload(const void *h, size_t b)
+  {
+    RB_TRY(alloc(b));
+    if (b) RB_CUDA(cudaMemcpy(p, h, b, cudaMemcpyHostToDevice));
+    return 0;
+  }
+  template <typename T> T *as() const { return (T *)p; }
+};
+
+// ---- geometry on the device --------------------------------------------------
+// Kernel-side view (passed by value).  Mirrors RadB200Geom plus a unit table:
+// one unit per (source, image), kinds 0 cuboid, 1 polyhedron, 2 arc, 3 background.
+struct GeomView {
+  const double *trf;
+  const double *rec;
+  const int *rec_img;
+  const double *poly;
+  const int *poly_info;
+  const double *face;
+  const int *face_vtx;
+  const double *vtx2d;
+  const double *arc;
+  const double *bkg;
+  const int4 *units;  // {kind, source, transform, 0}
+  int n_units;
+  Guard g;
+};
+
+struct DevGeom {
+  DBuf trf, rec, rec_img, poly, poly_info, face, face_vtx, vtx2d, arc, bkg, units;
+  int n_units = 0, n_rec = 0, n_poly = 0;
+  Guard g{0, 0, 0};
+  int upload(const RadB200Geom *G);
+  GeomView view() const;
+};
+
+// ---- interaction state -------------------------------------------------------
+struct Intrc {
+  int n = 0;        // elements
+  int n3 = 0;       // 3n
+  int ld = 0;       // padded leading dimension of N (multiple of 32)
+  int storage = 0;
+  DevGeom geom;     // relaxable elements (object frames, images)
+  DBuf elem_src, obs, rowT;           // [2n] int, [3n] obs points, [9n] s*Minv of main image
+  DBuf N32, N64;                      // [n3 x ld]
+  DBuf hext;                          // [ld]
+  DBuf mat_kind, mat, mh;             // materials
+  std::vector<int> h_mat_kind;
+  std::vector<double> h_mat;
+  // solver work buffers
+  DBuf M, H, Mp, F, part, work;
+  // LU factors (row-major [n3 x ld]) and solve state
+  DBuf LU32, LU64, lu_scratch;
+  int lu_mode = -1;                   // factors valid for this mode (-1 none)
+  DBuf lastM, lastH;                  // converged state of the last solve
+  int last_kind = -1;                 // 0 relax, 1 direct
+};
+
+// ---- small vector helpers (relax.cu) ---------------------------------------
+constexpr int MD_MAX = 16;
+struct DotSet {            // out[k] = <a_k, b_k>
+  const double *a[MD_MAX];
+  const double *b[MD_MAX];
+  int nd;
+};
+struct AxpySet {           // y = (accumulate ? y : 0) + sum_k c_k v_k
+  const double *v[MD_MAX];
+  double c[MD_MAX];
+  int nv;
+};
+int multidot(const DotSet &ds, int64_t len, double *host_out, DBuf &part, DBuf &scal, cudaStream_t st);
+int lincomb(const AxpySet &s, int64_t len, double *y, int accumulate, cudaStream_t st);
+int run_matvec(Intrc &I, const double *x, const double *b, double alpha, double *y, cudaStream_t st);
+int run_matvec_f32(Intrc &I, const double *x, const double *b, double alpha, double *y, cudaStream_t st);
+int launch_round_f32(const double *a, float *b, size_t n, cudaStream_t st);
+
+// linear operator + preconditioner for GMRES (krylov.cu)
+struct Op {
+  virtual int apply(const double *v, double *out) = 0;  // out = A v
+  virtual int precond(double *v) = 0;                   // v <- P v
+  virtual ~Op() {}
+};
+int gmres(Op &op, int n3, int ld, const double *b, double *x, double rtol, int max_iter, int restart, double *relres,
+          int *iters, cudaStream_t st);
+int lu_precond(Intrc &I, double *x, cudaStream_t st);
+int lu_precond_transposed(Intrc &I, double *x, cudaStream_t st);
+
+// TF32 tensor-core trailing update A -= L U (gemm_tc.cu); *used = 0 when the
+// shape is not supported and the caller must fall back to the CUDA-core GEMM.
+int tc_gemm_update_f32(float *A, int ld, int m, int n, int k, const float *L, const float *U, cudaStream_t st, int *used);
+
+// ---- kernels (launch wrappers) ---------------------------------------------
+int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what, int precision,
+                 double *d_out, DBuf &scratch, cudaStream_t st);
+int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int n,
+                    int ld, float *N32, double *N64, cudaStream_t st);
+int launch_rowtrans_vec(const double *rowT, const double *in, double *out, int n, cudaStream_t st);
+
+}  // namespace rb

@@ -1,0 +1,127 @@
+// material.cuh -- per-element constitutive laws on the device.
+//
+//   linear (isotropic or anisotropic):  M = chi H + Mr
+//       radTLinearAnisotropMaterial radmater.h:164-303, radTLinearIsotropMaterial :328-362
+//   saturating isotropic formula:       |M| = sum ms_i tanh(ksi_i |H| / ms_i), M || H
+//       radTNonlinearIsotropMaterial radmater.h:417-600, radmater.cpp:72-306
+// Record layout: RADB200_MAT_STRIDE doubles, see include/radb200.h.
+#pragma once
+#include "formulas.cuh"
+
+namespace rb {
+
+__device__ __forceinline__ void inv3x3(const double *A, double *B)
+{
+  double c0 = A[4] * A[8] - A[5] * A[7], c1 = A[5] * A[6] - A[3] * A[8], c2 = A[3] * A[7] - A[4] * A[6];
+  double id = 1.0 / (A[0] * c0 + A[1] * c1 + A[2] * c2);
+  B[0] = c0 * id; B[1] = (A[2] * A[7] - A[1] * A[8]) * id; B[2] = (A[1] * A[5] - A[2] * A[4]) * id;
+  B[3] = c1 * id; B[4] = (A[0] * A[8] - A[2] * A[6]) * id; B[5] = (A[2] * A[3] - A[0] * A[5]) * id;
+  B[6] = c2 * id; B[7] = (A[1] * A[6] - A[0] * A[7]) * id; B[8] = (A[0] * A[4] - A[1] * A[3]) * id;
+}
+
+// scalar law f(h) = |M|(|H|) and its derivative (radmater.cpp:279-306)
+__device__ __forceinline__ void tanh_law(const double *m, double h, double &f, double &df)
+{
+  f = 0.0; df = 0.0;
+  int n = (int)m[6];
+  for (int i = 0; i < n; i++) {
+    double ks = m[i], ms = m[3 + i];
+    if (ms == 0.0) continue;
+    double arg = ks * h / ms;
+    double th = tanh(arg);
+    f += ms * th;
+    df += ks * (1.0 - th * th);  // ks / cosh^2
+  }
+}
+
+__device__ __forceinline__ double tanh_ksi0(const double *m)
+{
+  double k = 0.0;
+  for (int i = 0; i < (int)m[6]; i++) k += m[i];
+  return k;
+}
+
+// M(H) for element material (kind, m)
+__device__ __forceinline__ V3<double> mat_M(int kind, const double *m, V3<double> H)
+{
+  if (kind == RADB200_MAT_LINEAR)
+    return mk3<double>(m[0] * H.x + m[1] * H.y + m[2] * H.z + m[9], m[3] * H.x + m[4] * H.y + m[5] * H.z + m[10],
+                       m[6] * H.x + m[7] * H.y + m[8] * H.z + m[11]);
+  double h = sqrt(H.x * H.x + H.y * H.y + H.z * H.z);
+  double ksi;
+  if (h <= 1e-10) ksi = tanh_ksi0(m);
+  else {
+    double f, df;
+    tanh_law(m, h, f, df);
+    ksi = f / h;
+  }
+  return mk3<double>(ksi * H.x + m[9], ksi * H.y + m[10], ksi * H.z + m[11]);
+}
+
+// dM/dH at H (radmater.cpp:206-277; linear: chi tensor)
+__device__ __forceinline__ void mat_D(int kind, const double *m, V3<double> H, double *D)
+{
+  if (kind == RADB200_MAT_LINEAR) {
+    for (int k = 0; k < 9; k++) D[k] = m[k];
+    return;
+  }
+  double h0 = sqrt(H.x * H.x + H.y * H.y + H.z * H.z);
+  double f, df;
+  tanh_law(m, h0, f, df);
+  if (h0 < 1e-10) {
+    for (int k = 0; k < 9; k++) D[k] = (k % 4 == 0) ? df : 0.0;
+    return;
+  }
+  double ih3 = 1.0 / (h0 * h0 * h0);
+  double off = ih3 * (h0 * df - f);
+  D[0] = ih3 * ((H.y * H.y + H.z * H.z) * f + H.x * H.x * h0 * df);
+  D[4] = ih3 * ((H.x * H.x + H.z * H.z) * f + H.y * H.y * h0 * df);
+  D[8] = ih3 * ((H.x * H.x + H.y * H.y) * f + H.z * H.z * h0 * df);
+  D[1] = D[3] = off * H.x * H.y;
+  D[2] = D[6] = off * H.x * H.z;
+  D[5] = D[7] = off * H.y * H.z;
+}
+
+// FindNewH: solve H = Hq + Q_ii M(H) for the element's own field.
+// Linear: H = (I - Q chi)^-1 (Hq + Q Mr)  (radmater.h:223-231).
+// Nonlinear: damped secant on |H| with at most 15 passes (radmater.cpp:72-164).
+__device__ __forceinline__ V3<double> find_new_h(int kind, const double *m, const double *Q, V3<double> Hq,
+                                                 V3<double> H0, double prec_e2)
+{
+  double A[9], Ai[9];
+  if (kind == RADB200_MAT_LINEAR) {
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++)
+        A[3 * a + b] = (a == b ? 1.0 : 0.0) - (Q[3 * a] * m[b] + Q[3 * a + 1] * m[3 + b] + Q[3 * a + 2] * m[6 + b]);
+    inv3x3(A, Ai);
+    double rx = Hq.x + Q[0] * m[9] + Q[1] * m[10] + Q[2] * m[11];
+    double ry = Hq.y + Q[3] * m[9] + Q[4] * m[10] + Q[5] * m[11];
+    double rz = Hq.z + Q[6] * m[9] + Q[7] * m[10] + Q[8] * m[11];
+    return mk3<double>(Ai[0] * rx + Ai[1] * ry + Ai[2] * rz, Ai[3] * rx + Ai[4] * ry + Ai[5] * rz,
+                       Ai[6] * rx + Ai[7] * ry + Ai[8] * rz);
+  }
+  double misfit = 3.0;
+  double ah = sqrt(H0.x * H0.x + H0.y * H0.y + H0.z * H0.z);
+  V3<double> H = H0;
+  for (int it = 0; it < 15; it++) {
+    double f = 0.0, df, ksi;
+    if (ah <= 1e-10) { ksi = tanh_ksi0(m); f = 0.0; }
+    else { tanh_law(m, ah, f, df); ksi = f / ah; }
+    for (int k = 0; k < 9; k++) A[k] = ((k % 4) == 0 ? 1.0 : 0.0) - ksi * Q[k];
+    inv3x3(A, Ai);
+    H = mk3<double>(Ai[0] * Hq.x + Ai[1] * Hq.y + Ai[2] * Hq.z, Ai[3] * Hq.x + Ai[4] * Hq.y + Ai[5] * Hq.z,
+                    Ai[6] * Hq.x + Ai[7] * Hq.y + Ai[8] * Hq.z);
+    double nah = sqrt(H.x * H.x + H.y * H.y + H.z * H.z);
+    double nmis = f - nah * ksi;
+    double am = fabs(misfit), anm = fabs(nmis);
+    double pn = am;
+    if (nmis * misfit > 0) pn += 0.5 * anm;
+    double alpha = pn / (pn + anm);
+    ah = alpha * nah + (1.0 - alpha) * ah;
+    misfit = f - ah * ksi;
+    if (misfit * misfit <= prec_e2) break;
+  }
+  return H;
+}
+
+}  // namespace rb

@@ -1,0 +1,601 @@
+"""Radia-compatible Python API for the B200 relaxation hot path.
+
+Function names, argument meanings, defaults, return shapes and error
+behaviour follow the reference binding (cpp/src/clients/python/radpy.cpp,
+method table :3341-3440) for the subset of Radia that builds and solves the
+models of the hot path: magnetized cuboids and polyhedra, containers,
+subdivision of cuboids, space transformations and symmetries, linear and
+saturating materials, current arcs / racetracks / current blocks, background
+fields, ``RlxPre`` / ``RlxAuto`` / ``Solve`` and ``Fld``.
+
+Everything numeric runs on the GPU through libradb200 (include/radb200.h);
+there is no CPU fallback -- a missing library or device raises.
+"""
+from __future__ import annotations
+
+import math
+from typing import Any, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _native
+from .model import (ArcCur, Bckg, Container, InteractionPack, Material, Obj, Polyhedron, RadiaError,
+                    RecMag, Trf, collect_leaves, pack_interaction, pack_sources, trf_field_inversion,
+                    trf_plane_sym, trf_rotation, trf_translation)
+
+__all__ = [
+    "ObjRecMag", "ObjRecCur", "ObjPolyhdr", "ObjThckPgn", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
+    "ObjCnt", "ObjAddToCnt", "ObjCntStuf", "ObjCntSize", "ObjDivMag", "ObjM", "ObjSetM",
+    "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
+    "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
+    "RlxPre", "RlxAuto", "Solve", "Fld", "FldLst", "FldLenRndSw", "FldLenTol",
+    "UtiDel", "UtiDelAll", "UtiVer", "UtiFldLastBackend", "UtiAsmLastBackend", "UtiGpuFallback",
+]
+
+# --------------------------------------------------------------------------
+# global state (the reference keeps the same in radTApplication)
+# --------------------------------------------------------------------------
+_objs: Dict[int, Any] = {}
+_next = [1]
+# radTConvergRepair defaults (radcnvrg.h:37-45); FldLenRndSw('off') zeroes them
+_rand_on = [1e-09, 1e-11, 1e-09]
+_rand = list(_rand_on)
+_last_fld = ["none"]
+_last_asm = ["none"]
+_fallback = ["cpu"]
+
+
+def _add(o) -> int:
+    h = _next[0]
+    _next[0] += 1
+    _objs[h] = o
+    return h
+
+
+def _get(h, cls=None):
+    o = _objs.get(int(h))
+    if o is None:
+        raise RadiaError(f"Radia::Error002: the element {h} does not exist")
+    if cls is not None and not isinstance(o, cls):
+        raise RadiaError(f"Radia::Error003: element {h} has the wrong type for this function")
+    return o
+
+
+def _v3(x, name="vector"):
+    a = np.asarray(x, dtype=np.float64).reshape(-1)
+    if a.size != 3:
+        raise RadiaError(f"Radia::Error000: {name} must have 3 components")
+    return a
+
+
+# --------------------------------------------------------------------------
+# objects
+# --------------------------------------------------------------------------
+def ObjRecMag(P, L, M=(0.0, 0.0, 0.0)) -> int:
+    """Rectangular block, centre P, dimensions L, magnetization M (radpy.cpp:3342)."""
+    L = _v3(L, "dimensions")
+    if np.any(L < 0):
+        raise RadiaError("Radia::Error001: negative dimensions")
+    return _add(RecMag(_v3(P), L, _v3(M)))
+
+
+def ObjRecCur(P, L, J) -> int:
+    """Current-carrying rectangular block with current density J (A/mm^2)."""
+    L = _v3(L, "dimensions")
+    if np.any(L < 0):
+        raise RadiaError("Radia::Error001: negative dimensions")
+    return _add(RecMag(_v3(P), L, np.zeros(3), _v3(J)))
+
+
+def ObjPolyhdr(V, F, M=(0.0, 0.0, 0.0)) -> int:
+    """Uniformly magnetized convex polyhedron; F lists 1-based vertex indices."""
+    faces = [[int(i) - 1 for i in f] for f in F]
+    return _add(Polyhedron(np.asarray(V, dtype=np.float64), faces, _v3(M)))
+
+
+def ObjThckPgn(x, lx, pts, a="x", M=(0.0, 0.0, 0.0)) -> int:
+    """Extruded convex polygon, converted to a polyhedron (radgpu_fld.cpp:511-536)."""
+    pts = np.asarray(pts, dtype=np.float64).reshape(-1, 2)
+    n = pts.shape[0]
+    ax = a.lower()
+    lo, hi = x - 0.5 * lx, x + 0.5 * lx
+
+    def p3(t, u, v):
+        if ax == "x":
+            return [t, u, v]
+        if ax == "y":
+            return [v, t, u]
+        return [u, v, t]
+
+    V = [p3(lo, *pts[k]) for k in range(n)] + [p3(hi, *pts[k]) for k in range(n)]
+    F = [list(range(1, n + 1)), list(range(n + 1, 2 * n + 1))]
+    for k in range(n):
+        k2 = (k + 1) % n
+        F.append([k + 1, k2 + 1, n + k2 + 1, n + k + 1])
+    return ObjPolyhdr(V, F, M)
+
+
+def _axis_trf(P, orient: str) -> Optional[Trf]:
+    """radTApplication::FindSpaceTransToOrientObjAlongMainAxis for the
+    default axis 'z' (radapl1.cpp:1486-1560)."""
+    o = orient.upper()
+    if o == "Z":
+        return None
+    if o == "X":
+        return trf_rotation(P, [1, 1, 1], 2.0 * math.pi / 3.0)
+    if o == "Y":
+        return trf_rotation(P, [1, 1, 1], 4.0 * math.pi / 3.0)
+    raise RadiaError("Radia::Error000: orientation must be 'x', 'y' or 'z'")
+
+
+def ObjArcCur(P, R, Phi, h, nseg, j, man_auto="man", a="z") -> int:
+    """Arc current (radTApplication::SetArcCur, radapl1.cpp:1664-1712)."""
+    R = list(R)
+    Phi = list(Phi)
+    if len(R) != 2 or R[0] < 0 or R[1] < 0 or R[1] < R[0]:
+        raise RadiaError("Radia::Error010: bad radii")
+    if len(Phi) != 2 or Phi[1] < Phi[0] or (Phi[1] - Phi[0]) > 2 * math.pi:
+        raise RadiaError("Radia::Error011: bad angles")
+    if h <= 0:
+        raise RadiaError("Radia::Error012: height must be positive")
+    if str(man_auto).lower() != "man":
+        raise RadiaError("ObjArcCur: only the 'man' (fixed nseg) field integration is supported")
+    o = ArcCur(_v3(P), R[0], R[1], Phi[0], Phi[1], h, j, max(int(nseg), 1))
+    t = _axis_trf(_v3(P), a)
+    if t is not None:
+        o.add_transform(1, t)
+    return _add(o)
+
+
+def ObjRaceTrk(P, R, L, h, nseg, j, man_auto="man", a="z") -> int:
+    """Racetrack = 4 arcs + straight current blocks (radapl1.cpp:1879-1975)."""
+    P = _v3(P)
+    R = list(R)
+    L = list(L)
+    if len(R) != 2 or R[0] < 0 or R[1] < 0 or R[1] < R[0]:
+        raise RadiaError("Radia::Error010: bad radii")
+    if len(L) != 2 or L[0] < 0 or L[1] < 0:
+        raise RadiaError("Radia::Error029: bad straight section lengths")
+    if h <= 0:
+        raise RadiaError("Radia::Error012: height must be positive")
+    pi = 3.14159265358979324
+    arcs = []
+    for cx, cy, p0, p1 in ((+1, +1, 0.0, 0.5 * pi), (-1, +1, 0.5 * pi, pi),
+                           (-1, -1, pi, 1.5 * pi), (+1, -1, 1.5 * pi, 1.999999999999 * pi)):
+        arcs.append(ObjArcCur([P[0] + cx * 0.5 * L[0], P[1] + cy * 0.5 * L[1], P[2]], R, [p0, p1],
+                              h, nseg, j, man_auto, "z"))
+    members = list(arcs)
+    if L[1] != 0.0:
+        er = 0.5 * (L[0] + R[0] + R[1])
+        d = [R[1] - R[0], L[1], h]
+        members.append(ObjRecCur([P[0] + er, P[1], P[2]], d, [0.0, j, 0.0]))
+        members.append(ObjRecCur([P[0] - er, P[1], P[2]], d, [0.0, -j, 0.0]))
+    if L[0] != 0.0:
+        er = 0.5 * (L[1] + R[0] + R[1])
+        d = [L[0], R[1] - R[0], h]
+        members.append(ObjRecCur([P[0], P[1] + er, P[2]], d, [-j, 0.0, 0.0]))
+        members.append(ObjRecCur([P[0], P[1] - er, P[2]], d, [j, 0.0, 0.0]))
+    g = ObjCnt(members)
+    t = _axis_trf(P, a)
+    if t is not None:
+        _get(g).add_transform(1, t)
+    return g
+
+
+def ObjBckg(B) -> int:
+    return _add(Bckg(_v3(B)))
+
+
+def ObjCnt(objs: Sequence[int]) -> int:
+    for h in objs:
+        _get(h)
+    return _add(Container(objs))
+
+
+def ObjAddToCnt(cnt: int, objs: Sequence[int]) -> int:
+    c = _get(cnt, Container)
+    for h in objs:
+        _get(h)
+    c.members = sorted(set(c.members) | set(int(h) for h in objs))
+    return cnt
+
+
+def ObjCntStuf(obj: int) -> List[int]:
+    o = _get(obj)
+    return list(o.members) if isinstance(o, Container) else [obj]
+
+
+def ObjCntSize(obj: int) -> int:
+    return len(collect_leaves(_objs, obj))
+
+
+def ObjDivMag(obj: int, k, *args, **kw) -> int:
+    """Subdivide a cuboid (or every cuboid of a container) by parallel planes
+    (radTRecMag::SubdivideItself, radrec.cpp:971-1082).  k = [kx,ky,kz] or
+    [[kx,qx],[ky,qy],[kz,qz]] with q the last-to-first size ratio."""
+    if args and isinstance(args[0], str) and args[0].lower() not in ("pln",):
+        raise RadiaError("ObjDivMag: only the default parallel-plane subdivision is supported")
+    kk = []
+    for x in k:
+        if isinstance(x, (list, tuple)):
+            kk.append((float(x[0]), float(x[1]) if len(x) > 1 else 1.0))
+        else:
+            kk.append((float(x), 1.0))
+    if len(kk) != 3:
+        raise RadiaError("Radia::Error000: subdivision needs 3 numbers")
+    _divide(obj, kk)
+    return obj
+
+
+def _divide(h: int, kk):
+    o = _get(h)
+    if isinstance(o, Container):
+        for m in list(o.members):
+            _divide(m, kk)
+        return
+    if not isinstance(o, RecMag) or np.any(o.j != 0.0):
+        return
+    (kx, qx), (ky, qy), (kz, qz) = kk
+    if abs(kx - 1) < 1e-10 and abs(ky - 1) < 1e-10 and abs(kz - 1) < 1e-10:
+        return
+    tol = 5e-12
+    q0 = []
+    a1 = []
+    for kq, dim in zip(kk, o.d):
+        kv, qv = kq
+        q0v = qv ** (1.0 / (kv - 1.0)) if abs(kv - 1.0) > tol else qv
+        buf = qv * q0v - 1.0
+        a1.append(dim * (q0v - 1.0) / buf if abs(buf) > tol else dim / kv)
+        q0.append(q0v)
+    init_dims = np.array(a1)
+    init_c = o.c - 0.5 * (o.d - init_dims)
+    members = []
+    dims = init_dims.copy()
+    c = init_c.copy()
+    for ix in range(int(kx)):
+        for iy in range(int(ky)):
+            for iz in range(int(kz)):
+                sub = RecMag(c.copy(), dims.copy(), o.m.copy())
+                sub.mat = o.mat
+                members.append(_add(sub))
+                c[2] += 0.5 * dims[2]
+                dims[2] *= q0[2]
+                c[2] += 0.5 * dims[2]
+            c[1] += 0.5 * dims[1]
+            dims[1] *= q0[1]
+            c[1] += 0.5 * dims[1]
+            c[2] = init_c[2]
+            dims[2] = init_dims[2]
+        c[0] += 0.5 * dims[0]
+        dims[0] *= q0[0]
+        c[0] += 0.5 * dims[0]
+        c[1] = init_c[1]
+        dims[1] = init_dims[1]
+    cnt = Container(members)
+    cnt.trfs = list(o.trfs)
+    cnt.mat = o.mat
+    _objs[h] = cnt
+
+
+def ObjM(obj: int):
+    """Centre point(s) and magnetization(s), element frame (radpy ObjM)."""
+    o = _get(obj)
+    if isinstance(o, Container):
+        return [ObjM(m) for m in o.members]
+    c = o.c if isinstance(o, RecMag) else getattr(o, "centre", np.zeros(3))
+    m = getattr(o, "m", np.zeros(3))
+    return [list(map(float, c)), list(map(float, m))]
+
+
+def ObjSetM(obj: int, M) -> int:
+    o = _get(obj)
+    if isinstance(o, Container):
+        for m in o.members:
+            ObjSetM(m, M)
+    elif hasattr(o, "m"):
+        o.m = _v3(M).copy()
+    return obj
+
+
+# --------------------------------------------------------------------------
+# transformations
+# --------------------------------------------------------------------------
+def TrfTrsl(V) -> int:
+    return _add(trf_translation(_v3(V)))
+
+
+def TrfRot(P, V, phi) -> int:
+    return _add(trf_rotation(_v3(P), _v3(V), float(phi)))
+
+
+def TrfPlSym(P, N) -> int:
+    return _add(trf_plane_sym(_v3(P), _v3(N), 1.0))
+
+
+def TrfInv() -> int:
+    return _add(trf_field_inversion())
+
+
+def TrfCmbL(orig: int, trf: int) -> int:
+    t0, t1 = _get(orig, Trf), _get(trf, Trf)
+    _objs[int(orig)] = t1 @ t0
+    return orig
+
+
+def TrfCmbR(orig: int, trf: int) -> int:
+    t0, t1 = _get(orig, Trf), _get(trf, Trf)
+    _objs[int(orig)] = t0 @ t1
+    return orig
+
+
+def TrfMlt(obj: int, trf: int, mlt: int) -> int:
+    o = _get(obj, Obj)
+    o.add_transform(int(mlt), _get(trf, Trf))
+    return obj
+
+
+def TrfOrnt(obj: int, trf: int) -> int:
+    return TrfMlt(obj, trf, 1)
+
+
+def TrfZerPara(obj: int, P, N) -> int:
+    """RadTrfZerPara, cpp/src/lib/radentry.cpp:1802-1822: PlSym * Inv, mult 2."""
+    t = trf_field_inversion() @ trf_plane_sym(_v3(P), _v3(N), 1.0)
+    _get(obj, Obj).add_transform(2, t)
+    return obj
+
+
+def TrfZerPerp(obj: int, P, N) -> int:
+    """RadTrfZerPerp, cpp/src/lib/radentry.cpp:1825-1840: PlSym, mult 2."""
+    _get(obj, Obj).add_transform(2, trf_plane_sym(_v3(P), _v3(N), 1.0))
+    return obj
+
+
+# --------------------------------------------------------------------------
+# materials
+# --------------------------------------------------------------------------
+def MatLin(ksi, mr) -> int:
+    """Linear anisotropic material (radTApplication::SetLinearMaterial,
+    radapl2.cpp:46-84): MatLin([ksipar,ksiper], mr|[mrx,mry,mrz])."""
+    ksi = list(ksi)
+    if len(ksi) != 2:
+        raise RadiaError("Radia::Error022: MatLin needs [ksipar, ksiper]")
+    if isinstance(mr, (list, tuple, np.ndarray)):
+        mrv = _v3(mr)
+        if not np.any(mrv != 0.0) and ksi[0] != ksi[1]:
+            raise RadiaError("Radia::Error023: zero remanence with anisotropic susceptibility")
+        return _add(Material(0, (float(ksi[0]), float(ksi[1])), mr=mrv))
+    return _add(Material(0, (float(ksi[0]), float(ksi[1])), mr_abs=float(mr)))
+
+
+def MatSatIsoFrm(*pairs) -> int:
+    """M = sum ms_i tanh(ksi_i H / ms_i); arguments [ksi_i, ms_i] (radpy.cpp:1972-2010)."""
+    if not 1 <= len(pairs) <= 3:
+        raise RadiaError("Radia::Error024: 1 to 3 [ksi, ms] pairs")
+    ks = tuple(float(p[0]) for p in pairs)
+    ms = tuple(float(p[1]) for p in pairs)
+    return _add(Material(1, ks, ms, mr=np.zeros(3)))
+
+
+def MatApl(obj: int, mat: int) -> int:
+    m = _get(mat, Material)
+    _apply_mat(int(obj), m)
+    return obj
+
+
+def _apply_mat(h: int, m: Material):
+    o = _get(h)
+    if isinstance(o, Container):
+        o.mat = m
+        for c in o.members:
+            _apply_mat(c, m)
+    elif isinstance(o, (RecMag, Polyhedron)):
+        if isinstance(o, RecMag) and np.any(o.j != 0.0):
+            return
+        if m.kind == 0 and m.mr is None:
+            m.resolve(o.m)   # raises Error107 for a zero magnetization
+        o.mat = m
+
+
+# --------------------------------------------------------------------------
+# relaxation
+# --------------------------------------------------------------------------
+class Interaction:
+    """Result of RlxPre: the device-resident interaction and its elements."""
+
+    def __init__(self, pack: InteractionPack, native: "_native.NativeInteraction"):
+        self.pack = pack
+        self.native = native
+        self.M: Optional[np.ndarray] = None
+        self.H: Optional[np.ndarray] = None
+        self.last_status = None
+
+    def writeback(self, M: np.ndarray):
+        for e, lf in enumerate(self.pack.leaves):
+            lf.obj.m = M[3 * e:3 * e + 3].copy()
+        self.M = M
+
+
+# RlxPre storage / solver selection; new method numbers are listed in
+# RlxAuto's docstring.
+_STORE = {"f32": 0, "f64": 1, "mixed": 2}
+
+
+def RlxPre(obj: int, srcobj: int = 0, use_gpu=True, storage: str = "f32") -> int:
+    """Builds the interaction for obj (and the extra source srcobj) on the
+    device.  storage='f32' keeps the reference's FP32 matrix; 'f64' an FP64
+    matrix; 'mixed' FP32 far blocks plus FP64 near blocks."""
+    pack = pack_interaction(_objs, int(obj), int(srcobj), tuple(_rand))
+    nat = _native.NativeInteraction(pack, _STORE[storage])
+    _last_asm[0] = "gpu"
+    return _add(Interaction(pack, nat))
+
+
+def _status_list(st):
+    return [float(st[0]), float(st[1]), float(st[2]), int(st[3])]
+
+
+def RlxAuto(intrc: int, prec: float, maxiter: int, meth: int = 4, *opts) -> list:
+    """Automatic relaxation (radpy RlxAuto).  meth 3/4/5/8/9/10 run the
+    device-resident Jacobi/Anderson solver (same fixed point as the
+    reference's methods), 11 the Newton-Krylov solver.  New: 12 = dense FP64
+    LU direct solve, 13 = TF32 tensor-core LU + FP64 GMRES refinement (linear
+    materials only).  Options 'ZeroM->True|False', 'omega->x'.
+    Returns [misfit, max|M|, max|H|, iterations]."""
+    it = _get(intrc, Interaction)
+    reset, omega = True, 0.0
+    for o in opts:
+        if not isinstance(o, str) or "->" not in o:
+            continue
+        key, val = [s.strip() for s in o.split("->", 1)]
+        if key.lower() == "zerom":
+            reset = val.lower() in ("true", "1", "yes")
+        elif key.lower() == "omega":
+            omega = float(val)
+    n = it.pack.elem_src.shape[0]
+    M0 = np.zeros(3 * n)
+    if not reset:
+        for e, lf in enumerate(it.pack.leaves):
+            M0[3 * e:3 * e + 3] = lf.obj.m
+    if meth in (12, 13):
+        if np.any(it.pack.mat_kind != 0):
+            raise RadiaError("RlxAuto: direct solve (meth 12/13) needs linear materials")
+        M, st = it.native.direct(0 if meth == 12 else 1, min(prec, 1e-12) if meth == 12 else 1e-13, maxiter)
+        st = [st[0], float(np.max(np.linalg.norm(M.reshape(-1, 3), axis=1))), 0.0, st[1]]
+    else:
+        method = 1 if meth == 11 else 0
+        M, H, st = it.native.relax(method, prec, maxiter, reset, omega, M0)
+        it.H = H
+    it.writeback(M)
+    it.last_status = st
+    return _status_list(st)
+
+
+def Solve(obj: int, prec: float, maxiter: int, meth: int = 4, *opts) -> list:
+    """RlxPre + RlxAuto (radapl2.cpp:1521-1601)."""
+    storage = "f64" if meth == 12 else "f32"
+    h = RlxPre(obj, storage=storage)
+    try:
+        return RlxAuto(h, prec, maxiter, meth, *opts)
+    finally:
+        UtiDel(h)
+
+
+# --------------------------------------------------------------------------
+# field
+# --------------------------------------------------------------------------
+_COMP = {"b": (0, None), "h": (1, None), "m": (2, None)}
+
+
+def _parse_id(fid: str):
+    s = fid.lower()
+    out = []
+    i = 0
+    while i < len(s):
+        ch = s[i]
+        if ch not in "bhm":
+            raise RadiaError(f"Radia::Error000: unsupported field id '{fid}'")
+        if i + 1 < len(s) and s[i + 1] in "xyz":
+            out.append((ch, "xyz".index(s[i + 1])))
+            i += 2
+        else:
+            out.append((ch, None))
+            i += 1
+    return out
+
+
+def Fld(obj: int, fid: str, pts, use_gpu=True, precision: str = "double"):
+    """Field at one point or a list of points (radpy Fld, radpy.cpp:2389-2445)."""
+    parts = _parse_id(fid)
+    P = np.asarray(pts, dtype=np.float64)
+    single = P.ndim == 1
+    P = P.reshape(-1, 3)
+    geom = pack_sources(_objs, int(obj), tuple(_rand))
+    prec = 1 if str(precision).lower() == "single" else 0
+    need = sorted({p[0] for p in parts})
+    vals = {}
+    for w in need:
+        vals[w] = _native.field(geom, P, {"b": 0, "h": 1, "m": 2}[w], prec)
+    _last_fld[0] = "gpu"
+    res = []
+    for i in range(P.shape[0]):
+        row = []
+        for ch, comp in parts:
+            v = vals[ch][i]
+            if comp is None:
+                row.extend(float(x) for x in v)
+            else:
+                row.append(float(v[comp]))
+        res.append(row[0] if len(row) == 1 else row)
+    return res[0] if single else res
+
+
+def FldLst(obj: int, fid: str, P1, P2, np_: int, arg: str = "noarg", strt: float = 0.0):
+    P1, P2 = _v3(P1), _v3(P2)
+    t = np.linspace(0.0, 1.0, int(np_))
+    pts = P1[None, :] + t[:, None] * (P2 - P1)[None, :]
+    vals = Fld(obj, fid, pts)
+    if arg == "arg":
+        step = np.linalg.norm(P2 - P1) / max(int(np_) - 1, 1)
+        return [[strt + i * step, v] for i, v in enumerate(vals)]
+    return vals
+
+
+def FldLenRndSw(onoff: str) -> int:
+    """Switches the length randomization guards (radapl2.cpp:2096-2111).
+    Unlike the reference, geometry is never jittered at creation; only the
+    near-singularity guard magnitudes change."""
+    s = onoff.lower()
+    if s == "on":
+        _rand[:] = _rand_on
+        return 1
+    if s == "off":
+        _rand[:] = [0.0, 0.0, 0.0]
+        return 0
+    raise RadiaError("Radia::Error043: 'on' or 'off' expected")
+
+
+def FldLenTol(absv: float = 1e-9, relv: float = 1e-11, zerov: float = 0.0) -> int:
+    _rand_on[:] = [abs(absv), abs(relv), abs(zerov) if zerov else abs(absv)]
+    _rand[:] = _rand_on
+    return 1
+
+
+# --------------------------------------------------------------------------
+# utilities
+# --------------------------------------------------------------------------
+def UtiDel(h: int) -> int:
+    o = _objs.pop(int(h), None)
+    if isinstance(o, Interaction):
+        o.native.free()
+    return 0
+
+
+def UtiDelAll() -> int:
+    for h in list(_objs):
+        UtiDel(h)
+    _next[0] = 1
+    return 0
+
+
+def UtiVer() -> float:
+    return 4.32
+
+
+def UtiFldLastBackend() -> str:
+    return _last_fld[0]
+
+
+def UtiAsmLastBackend() -> str:
+    return _last_asm[0]
+
+
+def UtiGpuFallback(mode: Optional[str] = None) -> str:
+    """Policy when the device cannot hold the interaction.  This library has
+    no CPU fallback: 'cpu' and 'break' both raise on such a failure; the
+    setting is kept for API compatibility."""
+    if mode is not None:
+        if mode not in ("cpu", "break", "gpu_streaming"):
+            raise RadiaError("Radia::Error000: mode must be 'cpu', 'break' or 'gpu_streaming'")
+        _fallback[0] = mode
+    return _fallback[0]
