@@ -1,0 +1,347 @@
+"""Benchmark of the relaxation hot path on the 20k-tetrahedron model.
+
+Workload (one step): the precision model -- 20,000 tetrahedra from a seeded
+jittered Kuhn lattice with 2% slivers, linear isotropic chi = 1000 in a
+uniform 1 T background field, a dense 60,000 x 60,000 interaction system --
+assembled on the device, solved by the mixed-precision direct solver (TF32
+tensor-core LU + FP64 GMRES refinement), then B evaluated at 1,000,000
+points outside the body.  Metric: seconds per solve+Fld step (lower is
+better), with the B error of the step against the plain FP64 GPU path
+(FP64 assembly, FP64 LU, FP64 field) reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: the path does not shard without a per-matvec exchange, so N GPUs
+run N independent replicas (weak scaling); the step time is the max over
+ranks.  Timing: CUDA events on the default stream (the library's stream),
+L2 flushed before every step, clocks sampled during the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "solve+Fld time at <=1e-6 rel B err vs plain FP64 GPU; adjoint/forward time ratio"
+WORKLOAD = dict(workload="tet20k: 20,000 tetrahedra (2% slivers), linear chi=1000, 1 T background, "
+                         "dense 60,000^2 system, B at 1e6 points outside the body",
+                n_tets=20000, n_points=1_000_000, chi=1000.0)
+NCELL = 15
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, out):
+        self.out = out
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.out, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self, dev=0):
+        try:
+            rows = [r.split(",") for r in open(self.out).read().strip().splitlines()]
+            rows = [[x.strip() for x in r] for r in rows if r and r[0].strip() == str(dev)]
+            sm = [float(r[1]) for r in rows]
+            mx = float(rows[0][2]) if rows else None
+            reasons = set()
+            for r in rows:
+                for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                    "samples": len(sm)}
+        except Exception as e:  # pragma: no cover
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world):
+    import torch
+    from radiacuda_b200 import _abi, _native, model, rad
+    import models as MD
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    L = _native.lib()
+    L.radb200_measure_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    fp64_peak = C.c_double(0)
+    _native.check(L.radb200_measure_fma_peak(1, C.byref(fp64_peak)), "fma peak")
+
+    m, body = MD.tet_mesh(rad, ncell=NCELL, n_tets=WORKLOAD["n_tets"], chi=WORKLOAD["chi"])
+    P = MD.tet_mesh_points(WORKLOAD["n_points"], ncell=NCELL)
+    pack = model.pack_interaction(rad._objs, m, 0, tuple(rad._rand))
+    src = model.pack_sources(rad._objs, m, tuple(rad._rand))
+    # element e -> polyhedron row of the field geometry (same traversal order)
+    poly_rows = np.arange(pack.elem_src.shape[0])
+    n3 = 3 * pack.elem_src.shape[0]
+    gE = _abi.GeomHolder(pack.elems)
+    gR = _abi.RelaxHolder(pack.elem_src, pack.mat_kind, pack.mat, pack.mh)
+    gX = _abi.GeomHolder(pack.ext)
+    d_pts = torch.from_numpy(P).to(dev)
+    d_B = torch.empty_like(d_pts)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    Mbuf = np.zeros(n3)
+    st = np.zeros(4)
+    _dp = C.POINTER(C.c_double)
+
+    def step(mode, storage, fprec, ev=None):
+        h = C.c_int64(0)
+        if ev:
+            ev[0].record()
+        _native.check(L.radb200_intrc_create(C.cast(gE.ptr, C.c_void_p), C.cast(gR.ptr, C.c_void_p),
+                                             C.cast(gX.ptr, C.c_void_p), storage, C.byref(h)), "intrc_create")
+        if ev:
+            ev[1].record()
+        _native.check(L.radb200_direct_solve(h.value, mode, 1e-12 if mode == 0 else 1e-13, 200,
+                                             Mbuf.ctypes.data_as(_dp), st.ctypes.data_as(_dp)), "direct_solve")
+        L.radb200_intrc_free(h.value)
+        src["poly"][poly_rows, 3:6] = Mbuf.reshape(-1, 3)
+        if ev:
+            ev[2].record()
+        _native.field_dev(src, d_pts.data_ptr(), P.shape[0], 0, d_B.data_ptr(), fprec)
+        if ev:
+            ev[3].record()
+        return st.copy()
+
+    # plain FP64 GPU path once: the error reference and the speed comparator
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    step(0, 1, 0)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    B_plain = d_B.cpu().numpy().copy()
+
+    launches0 = _native.kernel_launches()
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        step(1, 2, 0)
+    torch.cuda.synchronize()
+    B_mixed = d_B.cpu().numpy().copy()
+    err = float(np.abs(B_mixed - B_plain).max() / np.abs(B_plain).max())
+
+    times, t_asm, t_solve, t_fld = [], [], [], []
+    clocks = Clocks(os.path.join(ROOT, "gpurun_out", f"bench_clocks_r{rank}.csv") if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
+                    else f"/tmp/bench_clocks_r{rank}.csv")
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches_before = _native.kernel_launches()
+    with clocks:
+        for _ in range(args.steps):
+            flush.fill_(2.0)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            step(1, 2, 0, ev)
+            torch.cuda.synchronize()
+            t_asm.append(ev[0].elapsed_time(ev[1]) / 1e3)
+            t_solve.append(ev[1].elapsed_time(ev[2]) / 1e3)
+            t_fld.append(ev[2].elapsed_time(ev[3]) / 1e3)
+            times.append(ev[0].elapsed_time(ev[3]) / 1e3)
+    launches = (_native.kernel_launches() - launches_before) // max(args.steps, 1)
+    torch.cuda.synchronize()
+    t_step = float(np.mean(times))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([t_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_step = float(t.item())
+
+    # end to end through the public API with host buffers (rad.RlxPre/RlxAuto/Fld)
+    Ph = torch.from_numpy(P).pin_memory().numpy()
+    e2e = []
+    for _ in range(0 if args.profile else max(1, min(args.steps, 2))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        im = rad.RlxPre(m, storage="mixed")
+        rad.RlxAuto(im, 1e-13, 200, 13)
+        Bh = rad.Fld(m, "b", Ph)
+        torch.cuda.synchronize()
+        e2e.append(time.perf_counter() - t0)
+        rad.UtiDel(im)
+    e2e_err = float(np.abs(np.asarray(Bh) - B_plain).max() / np.abs(B_plain).max()) if e2e else None
+    if not e2e:
+        e2e = [float("nan")]
+
+    # roofline of the dominant kernel: the field evaluation (FP64 pipe)
+    n_faces = src["face"].shape[0]
+    ops_per_face = FIELD_OPS_PER_TRIANGLE
+    fld_s = float(np.mean(t_fld))
+    achieved = P.shape[0] * n_faces * ops_per_face / fld_s / 1e12
+    res = {
+        "metric": METRIC, "value": round(t_step, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * t_step, 2), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+tf32", "data": "synthetic (seeded)",
+        "config": dict(WORKLOAD, parallelism=f"replicas{world}", l2="flushed (256 MB write) before every step",
+                       solver="TF32 LU + FP64 GMRES-IR", field="FP64"),
+        "breakdown_s": {"assembly": round(float(np.mean(t_asm)), 4), "solve": round(float(np.mean(t_solve)), 4),
+                        "field": round(fld_s, 4)},
+        "b_rel_err_vs_plain_fp64": err, "plain_fp64_s": round(t_plain, 4),
+        "speedup_vs_plain_fp64": round(t_plain / t_step, 3),
+        "e2e": {"value": round(float(np.mean(e2e)), 4), "unit": "s", "b_rel_err_vs_plain_fp64": e2e_err,
+                "h2d_bytes_per_step": int(P.nbytes + sum(a.nbytes for a in src.values()) + sum(a.nbytes for a in pack.elems.values())),
+                "d2h_bytes_per_step": int(P.nbytes + n3 * 8)},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "field_kernel<double>", "bound": "fp64", "achieved": round(achieved, 3),
+                     "peak": round(fp64_peak.value, 3), "unit": "TFLOP/s", "frac": round(achieved / fp64_peak.value, 4),
+                     "peak_source": "measured FP64 FMA loop (radb200_measure_fma_peak) on this GPU",
+                     "algorithmic": f"{ops_per_face} FP64 ops per (point, triangular face)",
+                     "traffic": None},
+        "clocks": clocks.summary(int(os.environ.get("LOCAL_RANK", 0))),
+    }
+    return res
+
+
+# FP64 operations of one triangular face term of radTPolygon::B_comp as
+# restated in csrc/formulas.cuh, counting an add/mul/compare as 1, an FMA as
+# 2 and each elementary function by the cost of a standard implementation:
+# sqrt 8, div 8, log 20, atan2 30 (3 edges + the per-face log and frame).
+FIELD_OPS_PER_TRIANGLE = 3 * (2 * 8 + 5 * 8 + 20 + 30 + 75) + 20 + 60
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines: the reference CPU module (oracle/_ref) on a bounded sample
+# ---------------------------------------------------------------------------
+def _ref_module():
+    d = os.path.join(ROOT, "oracle", "_ref")
+    if not os.path.isdir(d) or not any(f.startswith("radia") and f.endswith(".so") for f in os.listdir(d)):
+        return None
+    sys.path.insert(0, d)
+    import radia
+    return radia
+
+
+def reference_sample(small=False):
+    """Extrapolated full-workload time of the reference CPU path from a
+    bounded sample: assembly per pair (1 core), dense FP64 solve (LAPACK on
+    all cores, scaled by n^3), field per (point, tetrahedron) (all cores)."""
+    R = _ref_module()
+    if R is None:
+        return None
+    import models as MD
+    cores = os.cpu_count() or 1
+    ns = 600 if small else 1500
+    t0 = time.perf_counter()
+    m, body = MD.tet_mesh(R, ncell=NCELL, n_tets=ns, chi=WORKLOAD["chi"])
+    t1 = time.perf_counter()
+    R.RlxPre(m)
+    t_asm = time.perf_counter() - t1
+    n_full = WORKLOAD["n_tets"]
+    asm_full = t_asm * (n_full / ns) ** 2
+    # LAPACK dgesv timed at a size where it already runs at its large-matrix rate
+    n3s = 4000 if small else 8000
+    A = np.random.default_rng(0).standard_normal((n3s, n3s)) + n3s * np.eye(n3s)
+    b = np.ones(n3s)
+    t2 = time.perf_counter()
+    np.linalg.solve(A, b)
+    t_lu = time.perf_counter() - t2
+    lu_full = t_lu * (3 * n_full / n3s) ** 3
+    npts = 400 if small else 2000
+    # field: per point cost of the full model on one core, times the full point count / cores
+    mm, _ = MD.tet_mesh(R, ncell=NCELL, n_tets=n_full, chi=WORKLOAD["chi"])
+    P = MD.tet_mesh_points(npts, ncell=NCELL, seed=11)
+    t3 = time.perf_counter()
+    R.Fld(mm, "b", P.tolist())
+    t_f = time.perf_counter() - t3
+    fld_full = t_f * WORKLOAD["n_points"] / npts / cores
+    total = asm_full + lu_full + fld_full
+    return {"value": round(total, 2), "unit": "s", "cores": cores, "kind": "reference",
+            "sample": (f"reference CPU module: RlxPre of a {ns}-tet subset ({t_asm:.2f} s, 1 core, scaled by n^2), "
+                       f"LAPACK dense solve n={n3s} ({t_lu:.2f} s, all cores, scaled by n^3), Fld of {npts} points on the "
+                       f"full model ({t_f:.2f} s, 1 core, scaled to 1e6 points over {cores} cores)"),
+            "parts_s": {"assembly": round(asm_full, 2), "solve": round(lu_full, 2), "field": round(fld_full, 2)}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="launch-list run: skip the end-to-end and CPU-baseline legs (keeps the launch count small)")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    rank = int(os.environ.get("RANK", 0))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        times = []
+        last = None
+        for i in range(args.warmup + args.steps):
+            r = reference_sample(small=True)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference CPU module (oracle/_ref) not built"}))
+                return
+            if i >= args.warmup:
+                times.append(r["value"])
+                last = r
+        v = float(np.mean(times))
+        out = {"metric": METRIC, "value": round(v, 2), "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": round(1e3 * v, 1), "higher_is_better": False, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+               "config": dict(WORKLOAD, parallelism="cpu"),
+               "cpu_baseline": {"value": round(v, 2), "unit": "s", "cores": last["cores"], "kind": "reference",
+                                "sample": last["sample"]},
+               "e2e": {"value": round(v, 2), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    res = run_ours(args, rank, world)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = reference_sample()
+        res["cpu_baseline"] = cb if cb is not None else {"value": None, "unavailable": "oracle/_ref missing"}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

@@ -128,6 +128,10 @@ RADB200_API int radb200_version(void);                      /* 100 * major + min
 /* Number of this library's kernels launched since load (all entry points). */
 RADB200_API int64_t radb200_kernel_launches(void);
 RADB200_API int radb200_device_sync(void);
+/* Diagnostics, no counterpart in the reference: measured FMA throughput of
+ * the FP64 (fp64 != 0) or FP32 pipe of the current device in TFLOP/s, the
+ * roofline denominator of the transcendental-bound assembly / field kernels. */
+RADB200_API int radb200_measure_fma_peak(int fp64, double *tflops);
 
 /* ---- field evaluation ------------------------------------------------------
  * Replaces radGPU_ComputeField (radgpu_fld.h:183-198) and the reference's

@@ -144,6 +144,7 @@ struct Op {
 int gmres(Op &op, int n3, int ld, const double *b, double *x, double rtol, int max_iter, int restart, double *relres,
           int *iters, cudaStream_t st);
 int lu_precond(Intrc &I, double *x, cudaStream_t st);
+int relax_jacobi(Intrc &I, double prec, int max_iter, double omega0, double *status);
 int lu_precond_transposed(Intrc &I, double *x, cudaStream_t st);
 
 // TF32 tensor-core trailing update A -= L U (gemm_tc.cu); *used = 0 when the

@@ -246,6 +246,19 @@ int relax_newton(Intrc &I, double prec, int max_iter, double *status)
   double misfit;
   RB_TRY(eval(M, &misfit));
   int matvecs = 1, newton = 0;
+  if (misfit > prec) {
+    // Globalization: Newton from the remanent state overshoots deep into
+    // saturation for soft iron (initial chi ~ 1e4).  A short Anderson-mixed
+    // Jacobi phase (the method-9 iteration) brings M into the basin first;
+    // its iterations count as matvecs.
+    double st[4];
+    int warm = std::min(300, std::max(1, max_iter / 4));
+    double loose = std::max(prec, 1e-3 * std::max(misfit, 1e-12));
+    RB_TRY(relax_jacobi(I, loose, warm, 0.0, st));
+    matvecs += (int)st[3];
+    RB_TRY(eval(M, &misfit));
+    matvecs++;
+  }
   while (misfit > prec && matvecs < max_iter && newton < 200) {
     newton++;
     if (I.N64.p) nk_precond_build<double><<<(n + 127) / 128, 128>>>(I.N64.as<double>(), ld, D, n, P);

@@ -275,6 +275,10 @@ __global__ void __launch_bounds__(256) panel_gemv_kernel(const T *__restrict__ A
 template <typename T>
 static int lu_factor(T *A, int n3, int ld, int *d_err, bool use_tc, cudaStream_t st, int *tc_used)
 {
+  const int smax = LU_NB * LU_NB * (int)sizeof(double);
+  RB_CUDA(cudaFuncSetAttribute(diag_lu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  RB_CUDA(cudaFuncSetAttribute(trsm_right_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  RB_CUDA(cudaFuncSetAttribute(trsm_left_lower_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   for (int k0 = 0; k0 < n3; k0 += LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
     size_t sm = (size_t)nb * nb * sizeof(double);

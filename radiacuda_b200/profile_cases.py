@@ -1,0 +1,71 @@
+"""Small, self-contained launches of the hot kernels for profiling.
+
+    python -m radiacuda_b200.profile_cases field    [--tets N] [--points P] [--fp32]
+    python -m radiacuda_b200.profile_cases assemble [--tets N]
+    python -m radiacuda_b200.profile_cases lu       [--tets N] [--mode 0|1]
+    python -m radiacuda_b200.profile_cases relax    [--blocks N]
+
+Each case builds a seeded model of the benchmark's shapes (tetrahedral mesh
+of chi = 1000 material, magnet array) at a size that keeps one launch of the
+kernel of interest short and the device footprint to a few GB, runs it once
+and prints the wall time.  Meant to be run under ncu with -k / -c.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import time
+
+import numpy as np
+
+
+def _models():
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(here, "tests"))
+    import models
+    return models
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["field", "assemble", "lu", "relax"])
+    ap.add_argument("--tets", type=int, default=20000)
+    ap.add_argument("--points", type=int, default=20000)
+    ap.add_argument("--blocks", type=int, default=16)
+    ap.add_argument("--mode", type=int, default=1)
+    ap.add_argument("--fp32", action="store_true")
+    a = ap.parse_args(argv)
+    from . import _native, model, rad
+    MD = _models()
+    t0 = time.perf_counter()
+    if a.case in ("field", "assemble", "lu"):
+        ncell = int(np.ceil((a.tets / 6) ** (1 / 3)))
+        m, body = MD.tet_mesh(rad, ncell=ncell, n_tets=a.tets)
+        if a.case == "field":
+            rng = np.random.default_rng(0)
+            for lf in model.collect_leaves(rad._objs, body):
+                lf.obj.m = rng.normal(size=3)
+            P = MD.tet_mesh_points(a.points, ncell=ncell)
+            t0 = time.perf_counter()
+            B = rad.Fld(m, "b", P, precision="single" if a.fp32 else "double")
+            print("field", P.shape[0], "points", time.perf_counter() - t0, "s", float(np.abs(B).max()))
+        elif a.case == "assemble":
+            im = rad.RlxPre(m, storage="f32")
+            print("assembly", time.perf_counter() - t0, "s")
+        else:
+            im = rad.RlxPre(m, storage="f64")
+            t0 = time.perf_counter()
+            st = rad.RlxAuto(im, 1e-13, 200, 12 if a.mode == 0 else 13)
+            print("lu mode", a.mode, time.perf_counter() - t0, "s", st)
+    else:
+        h = MD.magnet_array(rad, nside=int(np.sqrt(a.blocks)), div=3)
+        im = rad.RlxPre(h)
+        t0 = time.perf_counter()
+        st = rad.RlxAuto(im, 1e-10, 1000, 4)
+        print("relax", time.perf_counter() - t0, "s", st)
+    _native.lib().radb200_device_sync()
+
+
+if __name__ == "__main__":
+    main()

@@ -20,7 +20,7 @@ import numpy as np
 
 from . import _native
 from .model import (ArcCur, Bckg, Container, InteractionPack, Material, Obj, Polyhedron, RadiaError,
-                    RecMag, Trf, collect_leaves, pack_interaction, pack_sources, trf_field_inversion,
+                    RecMag, Trf, collect_leaves, images_of, pack_interaction, pack_sources, trf_field_inversion,
                     trf_plane_sym, trf_rotation, trf_translation)
 
 __all__ = [
@@ -277,14 +277,31 @@ def _divide(h: int, kk):
     _objs[h] = cnt
 
 
+def _objm(h: int, outer: Trf) -> list:
+    o = _get(h)
+    out = []
+    for T in images_of(o.trfs):
+        Tt = outer @ T
+        if isinstance(o, Container):
+            for m in o.members:
+                out.extend(_objm(m, Tt))
+        elif isinstance(o, (ArcCur, Bckg)) or (isinstance(o, RecMag) and np.any(o.j != 0.0)):
+            continue   # current sources and backgrounds carry no magnetization
+        else:
+            c = o.c if isinstance(o, RecMag) else getattr(o, "centre", np.zeros(3))
+            m = getattr(o, "m", np.zeros(3))
+            out.append([list(map(float, Tt.point(c))), list(map(float, Tt.s * (Tt.M @ m)))])
+    return out
+
+
 def ObjM(obj: int):
-    """Centre point(s) and magnetization(s), element frame (radpy ObjM)."""
+    """Centre point(s) and magnetization(s) in the lab frame, one entry per
+    member and symmetry image (radpy ObjM)."""
     o = _get(obj)
-    if isinstance(o, Container):
-        return [ObjM(m) for m in o.members]
-    c = o.c if isinstance(o, RecMag) else getattr(o, "centre", np.zeros(3))
-    m = getattr(o, "m", np.zeros(3))
-    return [list(map(float, c)), list(map(float, m))]
+    res = _objm(int(obj), Trf.identity())
+    if not isinstance(o, Container) and len(res) == 1:
+        return res[0]
+    return res
 
 
 def ObjSetM(obj: int, M) -> int:
@@ -517,6 +534,12 @@ def Fld(obj: int, fid: str, pts, use_gpu=True, precision: str = "double"):
     for w in need:
         vals[w] = _native.field(geom, P, {"b": 0, "h": 1, "m": 2}[w], prec)
     _last_fld[0] = "gpu"
+    if isinstance(pts, np.ndarray) and pts.ndim == 2:
+        # array in, array out (an extension: the reference returns lists)
+        cols = []
+        for ch, comp in parts:
+            cols.append(vals[ch] if comp is None else vals[ch][:, comp:comp + 1])
+        return cols[0] if len(cols) == 1 else np.concatenate(cols, axis=1)
     res = []
     for i in range(P.shape[0]):
         row = []

@@ -240,3 +240,40 @@ def mixed_sym(R, seed=3):
     coil = R.ObjRaceTrk([0, 0, 40], [60, 80], [10, 20], 15, 8, 2.0, "man", "z")
     arc = R.ObjArcCur([20, -30, -20], [5, 9], [0.3, 2.9], 6, 10, 3.0, "man", "x")
     return R.ObjCnt([ga, gb, coil, arc])
+
+
+# ---------------------------------------------------------------------------
+# the reference's MPI-solve regression models (tests/test_mpi_solve.py of the
+# reference), rebuilt with the same seeded draws so the golden B values of
+# its tests/_mpi_solve_reference.json apply
+# ---------------------------------------------------------------------------
+def mpi_solve_model(R, kind="small"):
+    R.UtiDelAll()
+    R.FldLenRndSw("on")   # the golden values were made with the default setting
+    rng = np.random.default_rng(11)
+    ids = []
+    if kind == "large":
+        for _ in range(1100):
+            c = rng.uniform([-80, -80, -40], [80, 80, 40]).tolist()
+            d = rng.uniform(2.0, 4.0, 3).tolist()
+            ids.append(R.ObjRecMag(c, d))
+        body = R.ObjCnt(ids)
+    else:
+        for _ in range(60):
+            base = rng.uniform([20, 5, 5], [90, 40, 40])
+            v = base + rng.uniform(2, 10, size=(4, 3))
+            ids.append(R.ObjPolyhdr(v.tolist(), TET_FACES))
+        if kind == "mixed":
+            for i in range(3):
+                for j in range(2):
+                    for k in range(2):
+                        ids.append(R.ObjRecMag([30.0 + i * 12, 10.0 + j * 11, 8.0 + k * 9], [10.0, 8.0, 7.0]))
+        body = R.ObjCnt(ids)
+        R.TrfZerPerp(body, [0, 0, 0], [1, 0, 0])
+        R.TrfZerPara(body, [0, 0, 0], [0, 0, 1])
+    R.MatApl(body, R.MatSatIsoFrm([20000, 2], [0.1, 2], [0.1, 2]))
+    coil = R.ObjRaceTrk([0, 0, 30], [70, 90], [0, 0], 15, 10, 3.0, "man", "z")
+    return R.ObjCnt([body, coil])
+
+
+MPI_SOLVE_POINTS = [[25.0, 10.0, 0.0], [60.0, 30.0, 5.0]]
