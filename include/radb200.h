@@ -136,8 +136,9 @@ RADB200_API int radb200_measure_fma_peak(int fp64, double *tflops);
 /* ---- field evaluation ------------------------------------------------------
  * Replaces radGPU_ComputeField (radgpu_fld.h:183-198) and the reference's
  * host coil loop.  what: 0 = B, 1 = H, 2 = M (magnetization at the point).
- * precision: 0 = FP64, 1 = FP32 polygon/cuboid terms with FP64 accumulation
- * (the reference's use_gpu == 2).  pts/out are HOST arrays [npts*3]; the
+ * precision: 0 = FP64 with the reference's face-by-face polygon form;
+ * 1 = FP32 terms (FP64 vertex offsets and accumulation; the reference's
+ * use_gpu == 2); 2 = FP64 with the vertex/edge polyhedron form.  pts/out are HOST arrays [npts*3]; the
  * call copies them to and from the device.                                   */
 RADB200_API int radb200_field(const RadB200Geom *g, const double *pts, int64_t npts,
                   int what, int precision, double *out);
@@ -158,6 +159,10 @@ RADB200_API int radb200_field_dev(const RadB200Geom *g, const double *d_pts, int
 #define RADB200_STORE_F32   0
 #define RADB200_STORE_F64   1
 #define RADB200_STORE_MIXED 2
+/* OR-ed into storage: polyhedron blocks by the vertex/edge form (solid angles
+ * + edge logarithms, exact like the face-by-face form of the reference but
+ * with ~4x fewer transcendentals); cuboid blocks are unaffected.            */
+#define RADB200_ASM_FAST    16
 RADB200_API int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r,
                          const RadB200Geom *ext, int storage, int64_t *handle);
 RADB200_API int radb200_intrc_free(int64_t handle);

@@ -66,9 +66,127 @@ static int validate_geom(const RadB200Geom *G)
   return 0;
 }
 
-int DevGeom::upload(const RadB200Geom *G)
+// Vertex/edge topology of every polyhedron, rebuilt from the face frames:
+// vertex 3-D positions P = R^T (x, y, coordZ) deduplicated per polyhedron,
+// edges shared by two faces, fan triangles of every face, and the
+// coefficients of the field (a_f = sigma_f n_f, g_e = sum sigma_f nu_{e,f},
+// sigma_f = M.n_f) and of the tensor (G_e = sum nu_{e,f} n_f^T).
+struct HostTopo {
+  std::vector<int4> tinfo, tinfo2, tt;
+  std::vector<int2> te;
+  std::vector<double> tv, tel, teg, teG, ttm, tfn, tfa;
+};
+
+static void build_topo(const RadB200Geom *G, bool tensor, HostTopo &h)
+{
+  h.tinfo.resize(G->n_poly);
+  h.tinfo2.resize(G->n_poly);
+  for (int p = 0; p < G->n_poly; p++) {
+    int f0 = G->poly_info[4 * p], nf = G->poly_info[4 * p + 1];
+    const double *M = G->poly + (size_t)p * RADB200_POLY_STRIDE + 3;
+    int v0 = (int)(h.tv.size() / 3), e0 = (int)h.tel.size(), t0 = (int)h.tt.size(), ff0 = (int)(h.tfn.size() / 3);
+    std::vector<double> V;  // local vertices
+    std::vector<std::vector<int>> loops(nf);
+    double scale = 0.0;
+    for (int k = 0; k < nf; k++) {
+      const double *R = G->face + (size_t)(f0 + k) * RADB200_FACE_STRIDE;
+      int a0 = G->face_vtx[2 * (f0 + k)], na = G->face_vtx[2 * (f0 + k) + 1];
+      for (int j = 0; j < na; j++) {
+        double x = G->vtx2d[2 * (size_t)(a0 + j)], y = G->vtx2d[2 * (size_t)(a0 + j) + 1], z = R[9];
+        double P[3] = {x * R[0] + y * R[3] + z * R[6], x * R[1] + y * R[4] + z * R[7], x * R[2] + y * R[5] + z * R[8]};
+        scale = std::max(scale, std::max(fabs(P[0]), std::max(fabs(P[1]), fabs(P[2]))));
+        int found = -1;
+        for (size_t q = 0; q < V.size() / 3; q++) {
+          double tol = 1e-10 * (1.0 + scale);
+          if (fabs(V[3 * q] - P[0]) <= tol && fabs(V[3 * q + 1] - P[1]) <= tol && fabs(V[3 * q + 2] - P[2]) <= tol) {
+            found = (int)q;
+            break;
+          }
+        }
+        if (found < 0) {
+          found = (int)(V.size() / 3);
+          V.insert(V.end(), P, P + 3);
+        }
+        loops[k].push_back(found);
+      }
+    }
+    int nv = (int)(V.size() / 3);
+    if (nv > POLY_NV_FAST) {  // too many vertices for the register form: reference form only
+      h.tinfo[p] = make_int4(v0, -1, e0, 0);
+      h.tinfo2[p] = make_int4(t0, 0, ff0, 0);
+      continue;
+    }
+    h.tv.insert(h.tv.end(), V.begin(), V.end());
+    std::vector<int2> edges;
+    std::vector<double> g_e, G_e;
+    for (int k = 0; k < nf; k++) {
+      const double *R = G->face + (size_t)(f0 + k) * RADB200_FACE_STRIDE;
+      double n[3] = {R[6], R[7], R[8]};
+      double sigma = M[0] * n[0] + M[1] * n[1] + M[2] * n[2];
+      h.tfn.insert(h.tfn.end(), n, n + 3);
+      double af[3] = {sigma * n[0], sigma * n[1], sigma * n[2]};
+      h.tfa.insert(h.tfa.end(), af, af + 3);
+      const std::vector<int> &L = loops[k];
+      int m = (int)L.size();
+      for (int j = 1; j + 1 < m; j++) {
+        const double *a = &V[3 * L[0]], *b = &V[3 * L[j]], *c = &V[3 * L[j + 1]];
+        double u[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, w[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        h.tt.push_back(make_int4(L[0], L[j], L[j + 1], k));
+        h.ttm.push_back(u[1] * w[2] - u[2] * w[1]);
+        h.ttm.push_back(u[2] * w[0] - u[0] * w[2]);
+        h.ttm.push_back(u[0] * w[1] - u[1] * w[0]);
+      }
+      for (int j = 0; j < m; j++) {
+        int a = L[j], b = L[(j + 1) % m];
+        int lo = std::min(a, b), hi = std::max(a, b);
+        int ei = -1;
+        for (size_t q = 0; q < edges.size(); q++)
+          if (edges[q].x == lo && edges[q].y == hi) { ei = (int)q; break; }
+        if (ei < 0) {
+          ei = (int)edges.size();
+          edges.push_back(make_int2(lo, hi));
+          g_e.insert(g_e.end(), 3, 0.0);
+          G_e.insert(G_e.end(), 9, 0.0);
+        }
+        double t[3] = {V[3 * b] - V[3 * a], V[3 * b + 1] - V[3 * a + 1], V[3 * b + 2] - V[3 * a + 2]};
+        double tl = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        for (int c = 0; c < 3; c++) t[c] /= tl;
+        double nu[3] = {t[1] * n[2] - t[2] * n[1], t[2] * n[0] - t[0] * n[2], t[0] * n[1] - t[1] * n[0]};
+        for (int c = 0; c < 3; c++) g_e[3 * ei + c] += sigma * nu[c];
+        for (int r = 0; r < 3; r++)
+          for (int c = 0; c < 3; c++) G_e[9 * ei + 3 * r + c] += nu[r] * n[c];
+      }
+    }
+    for (auto &e : edges) {
+      h.te.push_back(e);
+      const double *a = &V[3 * e.x], *b = &V[3 * e.y];
+      h.tel.push_back(sqrt((b[0] - a[0]) * (b[0] - a[0]) + (b[1] - a[1]) * (b[1] - a[1]) + (b[2] - a[2]) * (b[2] - a[2])));
+    }
+    h.teg.insert(h.teg.end(), g_e.begin(), g_e.end());
+    if (tensor) h.teG.insert(h.teG.end(), G_e.begin(), G_e.end());
+    h.tinfo[p] = make_int4(v0, nv, e0, (int)edges.size());
+    h.tinfo2[p] = make_int4(t0, (int)h.tt.size() - t0, ff0, nf);
+  }
+}
+
+int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs)
 {
   RB_TRY(validate_geom(G));
+  if (G->n_poly > 0) {
+    HostTopo h;
+    build_topo(G, tensor_coeffs, h);
+    RB_TRY(tinfo.upload(h.tinfo.data(), h.tinfo.size() * sizeof(int4)));
+    RB_TRY(tinfo2.upload(h.tinfo2.data(), h.tinfo2.size() * sizeof(int4)));
+    RB_TRY(tv.upload(h.tv.data(), h.tv.size() * sizeof(double)));
+    RB_TRY(te.upload(h.te.data(), h.te.size() * sizeof(int2)));
+    RB_TRY(tel.upload(h.tel.data(), h.tel.size() * sizeof(double)));
+    RB_TRY(teg.upload(h.teg.data(), h.teg.size() * sizeof(double)));
+    RB_TRY(teG.upload(h.teG.data(), h.teG.size() * sizeof(double)));
+    RB_TRY(tt.upload(h.tt.data(), h.tt.size() * sizeof(int4)));
+    RB_TRY(ttm.upload(h.ttm.data(), h.ttm.size() * sizeof(double)));
+    RB_TRY(tfn.upload(h.tfn.data(), h.tfn.size() * sizeof(double)));
+    RB_TRY(tfa.upload(h.tfa.data(), h.tfa.size() * sizeof(double)));
+  }
   RB_TRY(trf.upload(G->trf, (size_t)G->n_trf * RADB200_TRF_STRIDE * sizeof(double)));
   RB_TRY(rec.upload(G->rec, (size_t)G->n_rec * RADB200_REC_STRIDE * sizeof(double)));
   RB_TRY(rec_img.upload(G->rec_img, (size_t)G->n_rec * 2 * sizeof(int)));
@@ -97,13 +215,17 @@ int DevGeom::upload(const RadB200Geom *G)
   return 0;
 }
 
-GeomView DevGeom::view() const
+GeomView DevGeom::view(int fast) const
 {
   GeomView v;
   v.trf = trf.as<double>(); v.rec = rec.as<double>(); v.rec_img = rec_img.as<int>();
   v.poly = poly.as<double>(); v.poly_info = poly_info.as<int>(); v.face = face.as<double>();
   v.face_vtx = face_vtx.as<int>(); v.vtx2d = vtx2d.as<double>(); v.arc = arc.as<double>();
   v.bkg = bkg.as<double>(); v.units = units.as<int4>(); v.n_units = n_units; v.g = g;
+  v.tp.tinfo = tinfo.as<int4>(); v.tp.tinfo2 = tinfo2.as<int4>(); v.tp.tv = tv.as<double>();
+  v.tp.te = te.as<int2>(); v.tp.tel = tel.as<double>(); v.tp.teg = teg.as<double>(); v.tp.teG = teG.as<double>();
+  v.tp.tt = tt.as<int4>(); v.tp.ttm = ttm.as<double>(); v.tp.tfn = tfn.as<double>(); v.tp.tfa = tfa.as<double>();
+  v.fast = (fast && tinfo.p) ? 1 : 0;
   return v;
 }
 
@@ -147,7 +269,7 @@ int radb200_field_dev(const RadB200Geom *g, const double *d_pts, int64_t npts, i
   if (npts < 0 || what < 0 || what > 2 || precision < 0 || precision > 1) { set_error("bad field arguments"); return RADB200_E_ARG; }
   DevGeom dg;
   RB_TRY(dg.upload(g));
-  RB_TRY(launch_field(dg.view(), d_pts, npts, what, precision, d_out, g_fld_scratch, 0));
+  RB_TRY(launch_field(dg.view(precision != 0), d_pts, npts, what, precision == 1 ? 1 : 0, d_out, g_fld_scratch, 0));
   RB_CUDA(cudaStreamSynchronize(0));
   return 0;
 }
@@ -167,6 +289,8 @@ int radb200_field(const RadB200Geom *g, const double *pts, int64_t npts, int wha
 int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const RadB200Geom *ext, int storage,
                          int64_t *handle)
 {
+  int fast = (storage & RADB200_ASM_FAST) ? 1 : 0;
+  storage &= ~RADB200_ASM_FAST;
   if (!elems || !r || !handle || storage < 0 || storage > 2) { set_error("bad arguments"); return RADB200_E_ARG; }
   int n = r->n_elem;
   if (n <= 0) { set_error("no relaxable elements"); return RADB200_E_ARG; }
@@ -186,7 +310,8 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   I->n3 = 3 * n;
   I->ld = (I->n3 + 31) / 32 * 32;
   I->storage = storage;
-  RB_TRY(I->geom.upload(elems));
+  RB_TRY(I->geom.upload(elems, fast != 0));
+  I->fast = fast;
   // observation points and row transforms from each element's main image
   std::vector<double> obs(3 * (size_t)n), rowT(9 * (size_t)n);
   for (int e = 0; e < n; e++) {
@@ -214,7 +339,7 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   if (storage == RADB200_STORE_F32 || storage == RADB200_STORE_MIXED) RB_TRY(I->N32.alloc(nn * sizeof(float)));
   if (I->N64.p) RB_CUDA(cudaMemsetAsync(I->N64.p, 0, nn * sizeof(double)));
   if (I->N32.p) RB_CUDA(cudaMemsetAsync(I->N32.p, 0, nn * sizeof(float)));
-  RB_TRY(launch_assemble(I->geom.view(), I->elem_src.as<int>(), I->obs.as<double>(), I->rowT.as<double>(), n, I->ld,
+  RB_TRY(launch_assemble(I->geom.view(fast), I->elem_src.as<int>(), I->obs.as<double>(), I->rowT.as<double>(), n, I->ld,
                          I->N32.as<float>(), I->N64.as<double>(), 0));
   // external field at element centres, in element frames
   size_t vb = (size_t)I->ld * sizeof(double);
@@ -225,7 +350,7 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
     RB_TRY(xg.upload(ext));
     DBuf tmp, scratch;
     RB_TRY(tmp.alloc(3 * (size_t)n * sizeof(double)));
-    RB_TRY(launch_field(xg.view(), I->obs.as<double>(), n, 1, 0, tmp.as<double>(), scratch, 0));
+    RB_TRY(launch_field(xg.view(fast), I->obs.as<double>(), n, 1, 0, tmp.as<double>(), scratch, 0));
     RB_TRY(launch_rowtrans_vec(I->rowT.as<double>(), tmp.as<double>(), I->hext.as<double>(), n, 0));
   }
   RB_TRY(I->M.alloc(vb)); RB_TRY(I->H.alloc(vb)); RB_TRY(I->Mp.alloc(vb)); RB_TRY(I->F.alloc(vb));

@@ -43,11 +43,21 @@ __device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<do
         if (in) f = mk3<double>(mx, my, mz);
       } else {
         V3<T> Tt, Ss;
-        int in = cuboid_TS<T>(mk3<T>(T(qc.x), T(qc.y), T(qc.z)), mk3<T>(T(hd.x), T(hd.y), T(hd.z)), g.g, Tt, Ss);
+        int in = cuboid_TS<T>(qc, hd, g.g, Tt, Ss);
         double Tx = Tt.x, Ty = Tt.y, Tz = Tt.z, Sx = Ss.x, Sy = Ss.y, Sz = Ss.z;
         f = mk3<double>(Tx * mx - Sz * my - Sy * mz, -Sz * mx + Ty * my - Sx * mz, -Sy * mx - Sx * my + Tz * mz);
         if (what == 0 && in) { f.x += mx; f.y += my; f.z += mz; }
       }
+    }
+  } else if (u.x == 1 && g.fast && __ldg(&g.tp.tinfo[u.y].y) >= 0) {
+    // vertex/edge form (formulas.cuh, poly_fast)
+    const double *pr = g.poly + (size_t)u.y * RADB200_POLY_STRIDE;
+    double h[3];
+    int in = poly_fast<T, false>(g.tp, u.y, q, h);
+    if (what == 2) f = in ? mk3<double>(__ldg(pr + 3), __ldg(pr + 4), __ldg(pr + 5)) : mk3<double>(0, 0, 0);
+    else {
+      f = mk3<double>(h[0], h[1], h[2]);
+      if (what == 0 && in) { f.x += __ldg(pr + 3); f.y += __ldg(pr + 4); f.z += __ldg(pr + 5); }
     }
   } else if (u.x == 1) {
     const double *pr = g.poly + (size_t)u.y * RADB200_POLY_STRIDE;
@@ -70,21 +80,10 @@ __device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<do
         cx /= nv; cy /= nv;
       }
       double plx = r0 * q.x + r1 * q.y + r2 * q.z, ply = r3 * q.x + r4 * q.y + r5 * q.z, plz = r6 * q.x + r7 * q.y + r8 * q.z;
-      int in;
+      // the face-by-face form stays in FP64: its products of powers of the edge
+      // slope overflow the FP32 range for near-vertical edges
       double s0, s1, s2;
-      if (sizeof(T) == 8 || nv > 8) {
-        in = polygon_S<double, double>(vt, nv, cz, cx, cy, mk3<double>(plx, ply, plz), g.g, s0, s1, s2);
-      } else {
-        // single precision: shift to the first vertex so FP32 sees small numbers
-        float vbuf[16];
-        int nvc = nv;
-        double ox = __ldg(vt), oy = __ldg(vt + 1);
-        for (int k = 0; k < nvc; k++) { vbuf[2 * k] = float(__ldg(vt + 2 * k) - ox); vbuf[2 * k + 1] = float(__ldg(vt + 2 * k + 1) - oy); }
-        float a0, a1, a2;
-        in = polygon_S<float, float>(vbuf, nvc, float(cz - plz), float(cx - ox), float(cy - oy),
-                                     mk3<float>(float(plx - ox), float(ply - oy), 0.0f), g.g, a0, a1, a2);
-        s0 = a0; s1 = a1; s2 = a2;
-      }
+      int in = polygon_S<double, double>(vt, nv, cz, cx, cy, mk3<double>(plx, ply, plz), g.g, s0, s1, s2);
       if (!in) inside = 0;
       if (what != 2) {
         double w = -CH * mloc;

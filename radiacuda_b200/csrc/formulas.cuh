@@ -64,17 +64,19 @@ template <typename T> __device__ __forceinline__ T atan4(T a, T b, T c, T d)
 // tensor entries T = (Txx,Tyy,Tzz) and S = (Sx,Sy,Sz) scaled by 1/(4 pi):
 //   Q = [[Tx,-Sz,-Sy],[-Sz,Ty,-Sx],[-Sy,-Sx,Tz]]    (radrec.cpp:265-283)
 template <typename T>
-__device__ __forceinline__ int cuboid_TS(V3<T> q, V3<T> hd, const Guard &g, V3<T> &Tt, V3<T> &Ss)
+__device__ __forceinline__ int cuboid_TS(V3<double> q, V3<double> hd, const Guard &g, V3<T> &Tt, V3<T> &Ss)
 {
-  T x0 = -q.x - hd.x, x1 = -q.x + hd.x;
-  T y0 = -q.y - hd.y, y1 = -q.y + hd.y;
-  T z0 = -q.z - hd.z, z1 = -q.z + hd.z;
-  if (x0 == T(0)) x0 = abs_rand(g, hd.x);
-  if (x1 == T(0)) x1 = abs_rand(g, hd.x);
-  if (y0 == T(0)) y0 = abs_rand(g, hd.y);
-  if (y1 == T(0)) y1 = abs_rand(g, hd.y);
-  if (z0 == T(0)) z0 = abs_rand(g, hd.z);
-  if (z1 == T(0)) z1 = abs_rand(g, hd.z);
+  // corner offsets in FP64 (exact zeros and guards decided before any rounding to T)
+  double dx0 = -q.x - hd.x, dx1 = -q.x + hd.x;
+  double dy0 = -q.y - hd.y, dy1 = -q.y + hd.y;
+  double dz0 = -q.z - hd.z, dz1 = -q.z + hd.z;
+  if (dx0 == 0.0) dx0 = abs_rand(g, hd.x);
+  if (dx1 == 0.0) dx1 = abs_rand(g, hd.x);
+  if (dy0 == 0.0) dy0 = abs_rand(g, hd.y);
+  if (dy1 == 0.0) dy1 = abs_rand(g, hd.y);
+  if (dz0 == 0.0) dz0 = abs_rand(g, hd.z);
+  if (dz1 == 0.0) dz1 = abs_rand(g, hd.z);
+  T x0 = T(dx0), x1 = T(dx1), y0 = T(dy0), y1 = T(dy1), z0 = T(dz0), z1 = T(dz1);
   int inside = (x0 * x1 < T(0)) && (y0 * y1 < T(0)) && (z0 * z1 < T(0));
   T x0e2 = x0 * x0, x1e2 = x1 * x1, y0e2 = y0 * y0, y1e2 = y1 * y1, z0e2 = z0 * z0, z1e2 = z1 * z1;
   T D000 = sqrtT(x0e2 + y0e2 + z0e2), D100 = sqrtT(x1e2 + y0e2 + z0e2);
@@ -343,6 +345,145 @@ __device__ __forceinline__ V3<double> arc_field(const double *a, V3<double> P)
   }
   double f = 0.0001 * Jaz * step;
   return mk3<double>(f * SBx, f * SBy, f * SBz);
+}
+
+// ---------------------------------------------------------------------------
+// Polyhedron, vertex/edge form.
+//
+// The field of a uniformly magnetized polyhedron is that of the surface
+// charge sigma_f = M.n_f on its faces:
+//   H(q) = 1/(4 pi) sum_f sigma_f I_f,   I_f = int_f (q - r')/|q - r'|^3 dS'
+// and for a planar face   I_f = Omega_f n_f + sum_{e in f} nu_{e,f} L_e
+// with Omega_f the signed solid angle of the face seen from q (sign of
+// n_f.(q - face)), nu_{e,f} the outward in-plane normal of edge e in face f
+// and L_e = int_e dl/|q - r'| = log1p(l (Ra + Rb + l) / D),
+// D = Ra Rb + ra.rb  (evaluated as |ra x rb|^2 / (Ra Rb - ra.rb) when ra.rb < 0
+// to avoid cancellation).  Solid angles per triangle by the Van Oosterom-
+// Strackee formula, with the triple product taken from the face's fixed edge
+// cross product (ra . m_t, m_t = (vb - va) x (vc - va)) so it does not cancel
+// for distant points.  Per tetrahedron this is 4 sqrt, 6 log1p, 4 atan2,
+// against 12 edge terms (24 sqrt, 24 log, 12 atan2) of the face-by-face form
+// radplnr2.cpp:29-388; both are exact, so they agree to rounding away from
+// the edges themselves.
+//
+// Topology record per polyhedron (built on the host from the face frames):
+//   tinfo  = {v0, nv, e0, ne},  tinfo2 = {t0, nt, f0, nf}
+//   tv[v]  vertex (object frame)          te[e] = {a, b} (local), tel[e] = l
+//   tt[t]  = {a, b, c, f} (local), ttm[t] = m_t
+//   tfn[f] = n_f
+// Field mode adds per face a_f = sigma_f n_f and per edge g_e = sum_f sigma_f nu_{e,f};
+// tensor mode uses per edge G_e = sum_f nu_{e,f} n_f^T (9 doubles).
+struct TopoView {
+  const int4 *tinfo, *tinfo2;
+  const double *tv;     // [V*3]
+  const int2 *te;       // [E]
+  const double *tel;    // [E]
+  const double *teg;    // [E*3] field coefficients g_e (or null)
+  const double *teG;    // [E*9] tensor coefficients G_e (or null)
+  const int4 *tt;       // [T]
+  const double *ttm;    // [T*3]
+  const double *tfn;    // [F*3]
+  const double *tfa;    // [F*3] field coefficients a_f (or null)
+};
+
+constexpr int POLY_NV_FAST = 8;  // vertices handled in registers
+
+template <typename T>
+__device__ __forceinline__ T log1pT(T x);
+template <> __device__ __forceinline__ double log1pT<double>(double x) { return log1p(x); }
+template <> __device__ __forceinline__ float log1pT<float>(float x) { return log1pf(x); }
+
+// Solid angles and edge logs of polyhedron p at q (object frame).
+// Accumulates H (field mode, a_f / g_e set) or the tensor Q (tensor mode).
+// Returns 1 when q is inside.  T = arithmetic type after the FP64 vertex shift.
+template <typename T, bool TENSOR>
+__device__ __forceinline__ int poly_fast(const TopoView &tp, int p, V3<double> q, double *out)
+{
+  const double C = 1.0 / (4.0 * 3.141592653589793238);
+  int4 i1 = __ldg(tp.tinfo + p), i2 = __ldg(tp.tinfo2 + p);
+  const int v0 = i1.x, nv = i1.y, e0 = i1.z, ne = i1.w, t0 = i2.x, nt = i2.y, f0 = i2.z, nf = i2.w;
+  T rx[POLY_NV_FAST], ry[POLY_NV_FAST], rz[POLY_NV_FAST], R[POLY_NV_FAST];
+#pragma unroll
+  for (int k = 0; k < POLY_NV_FAST; k++) {
+    if (k < nv) {
+      const double *v = tp.tv + 3 * (size_t)(v0 + k);
+      rx[k] = T(__ldg(v) - q.x); ry[k] = T(__ldg(v + 1) - q.y); rz[k] = T(__ldg(v + 2) - q.z);
+      R[k] = sqrtT(rx[k] * rx[k] + ry[k] * ry[k] + rz[k] * rz[k]);
+    } else {
+      rx[k] = ry[k] = rz[k] = R[k] = T(0);
+    }
+  }
+  double acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) acc[k] = 0.0;
+  // edges
+  for (int e = e0; e < e0 + ne; e++) {
+    int2 ab = __ldg(tp.te + e);
+    T l = T(__ldg(tp.tel + e));
+    T ax = T(0), ay = T(0), az = T(0), Ra = T(0), bx = T(0), by = T(0), bz = T(0), Rb = T(0);
+#pragma unroll
+    for (int k = 0; k < POLY_NV_FAST; k++) {
+      if (k == ab.x) { ax = rx[k]; ay = ry[k]; az = rz[k]; Ra = R[k]; }
+      if (k == ab.y) { bx = rx[k]; by = ry[k]; bz = rz[k]; Rb = R[k]; }
+    }
+    T s = ax * bx + ay * by + az * bz;
+    T D;
+    if (s >= T(0)) D = Ra * Rb + s;
+    else {
+      T cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+      D = (cx * cx + cy * cy + cz * cz) / (Ra * Rb - s);
+    }
+    T L = log1pT<T>(l * (Ra + Rb + l) / D);
+    double Ld = (double)L;
+    if (TENSOR) {
+      const double *G = tp.teG + 9 * (size_t)e;
+#pragma unroll
+      for (int k = 0; k < 9; k++) acc[k] += Ld * __ldg(G + k);
+    } else {
+      const double *g = tp.teg + 3 * (size_t)e;
+      acc[0] += Ld * __ldg(g); acc[1] += Ld * __ldg(g + 1); acc[2] += Ld * __ldg(g + 2);
+    }
+  }
+  // triangles -> face solid angles
+  double omega_tot = 0.0;
+  int fcur = -1;
+  double om = 0.0;
+  for (int t = t0; t <= t0 + nt; t++) {
+    int4 tr = (t < t0 + nt) ? __ldg(tp.tt + t) : make_int4(0, 0, 0, -1);
+    if (tr.w != fcur) {
+      if (fcur >= 0) {  // flush face fcur
+        const double *n = tp.tfn + 3 * (size_t)(f0 + fcur);
+        if (TENSOR) {
+          double n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2);
+          acc[0] += om * n0 * n0; acc[1] += om * n0 * n1; acc[2] += om * n0 * n2;
+          acc[3] += om * n1 * n0; acc[4] += om * n1 * n1; acc[5] += om * n1 * n2;
+          acc[6] += om * n2 * n0; acc[7] += om * n2 * n1; acc[8] += om * n2 * n2;
+        } else {
+          const double *a = tp.tfa + 3 * (size_t)(f0 + fcur);
+          acc[0] += om * __ldg(a); acc[1] += om * __ldg(a + 1); acc[2] += om * __ldg(a + 2);
+        }
+        omega_tot += om;
+      }
+      fcur = tr.w;
+      om = 0.0;
+      if (t == t0 + nt) break;
+    }
+    T xa = 0, ya = 0, za = 0, Ra = 0, xb = 0, yb = 0, zb = 0, Rb = 0, xc = 0, yc = 0, zc = 0, Rc = 0;
+#pragma unroll
+    for (int k = 0; k < POLY_NV_FAST; k++) {
+      if (k == tr.x) { xa = rx[k]; ya = ry[k]; za = rz[k]; Ra = R[k]; }
+      if (k == tr.y) { xb = rx[k]; yb = ry[k]; zb = rz[k]; Rb = R[k]; }
+      if (k == tr.z) { xc = rx[k]; yc = ry[k]; zc = rz[k]; Rc = R[k]; }
+    }
+    const double *m = tp.ttm + 3 * (size_t)t;
+    T num = xa * T(__ldg(m)) + ya * T(__ldg(m + 1)) + za * T(__ldg(m + 2));
+    T den = Ra * Rb * Rc + (xa * xb + ya * yb + za * zb) * Rc + (xa * xc + ya * yc + za * zc) * Rb +
+            (xb * xc + yb * yc + zb * zc) * Ra;
+    om += 2.0 * (double)atan2T(-num, den);
+  }
+#pragma unroll
+  for (int k = 0; k < (TENSOR ? 9 : 3); k++) out[k] = C * acc[k];
+  return omega_tot < -6.283185307179586;
 }
 
 }  // namespace rb

@@ -85,14 +85,18 @@ struct GeomView {
   const int4 *units;  // {kind, source, transform, 0}
   int n_units;
   Guard g;
+  TopoView tp;        // vertex/edge form of the polyhedra (tinfo.y < 0: not available)
+  int fast;           // 1: evaluate polyhedra in the vertex/edge form
 };
 
 struct DevGeom {
   DBuf trf, rec, rec_img, poly, poly_info, face, face_vtx, vtx2d, arc, bkg, units;
+  // polyhedron topology (vertex/edge form), see TopoView in formulas.cuh
+  DBuf tinfo, tinfo2, tv, te, tel, teg, teG, tt, ttm, tfn, tfa;
   int n_units = 0, n_rec = 0, n_poly = 0;
   Guard g{0, 0, 0};
-  int upload(const RadB200Geom *G);
-  GeomView view() const;
+  int upload(const RadB200Geom *G, bool tensor_coeffs = false);
+  GeomView view(int fast = 0) const;
 };
 
 // ---- interaction state -------------------------------------------------------
@@ -101,6 +105,7 @@ struct Intrc {
   int n3 = 0;       // 3n
   int ld = 0;       // padded leading dimension of N (multiple of 32)
   int storage = 0;
+  int fast = 0;     // polyhedra in the vertex/edge form
   DevGeom geom;     // relaxable elements (object frames, images)
   DBuf elem_src, obs, rowT;           // [2n] int, [3n] obs points, [9n] s*Minv of main image
   DBuf N32, N64;                      // [n3 x ld]

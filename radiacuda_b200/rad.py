@@ -438,12 +438,14 @@ class Interaction:
 _STORE = {"f32": 0, "f64": 1, "mixed": 2}
 
 
-def RlxPre(obj: int, srcobj: int = 0, use_gpu=True, storage: str = "f32") -> int:
+def RlxPre(obj: int, srcobj: int = 0, use_gpu=True, storage: str = "f32", fast: bool = False) -> int:
     """Builds the interaction for obj (and the extra source srcobj) on the
     device.  storage='f32' keeps the reference's FP32 matrix; 'f64' an FP64
-    matrix; 'mixed' FP32 far blocks plus FP64 near blocks."""
+    matrix; 'mixed' both (FP32 for the tensor-core factorization, FP64 for
+    the refinement residual).  fast=True assembles polyhedron blocks with the
+    vertex/edge form instead of the reference's face-by-face form."""
     pack = pack_interaction(_objs, int(obj), int(srcobj), tuple(_rand))
-    nat = _native.NativeInteraction(pack, _STORE[storage])
+    nat = _native.NativeInteraction(pack, _STORE[storage] | (16 if fast else 0))
     _last_asm[0] = "gpu"
     return _add(Interaction(pack, nat))
 
@@ -528,7 +530,11 @@ def Fld(obj: int, fid: str, pts, use_gpu=True, precision: str = "double"):
     single = P.ndim == 1
     P = P.reshape(-1, 3)
     geom = pack_sources(_objs, int(obj), tuple(_rand))
-    prec = 1 if str(precision).lower() == "single" else 0
+    # 'double': FP64, face-by-face polygon form (the reference's); 'single':
+    # FP32 terms with FP64 accumulation; 'fast': FP64 vertex/edge polyhedron form
+    prec = {"double": 0, "single": 1, "fast": 2}.get(str(precision).lower())
+    if prec is None:
+        raise RadiaError("Radia::Error000: precision must be 'double', 'single' or 'fast'")
     need = sorted({p[0] for p in parts})
     vals = {}
     for w in need:

@@ -179,3 +179,42 @@ def test_kernel_launch_counter_advances(cuda, rad):
     h, c = _build(rad, "magnet_array_2x2")
     rad.Fld(h, "b", c["points"])
     assert _native.kernel_launches() > before
+
+
+# ---------------------------------------------------------------------------
+# vertex/edge polyhedron form (fast path): same exact field, fewer transcendentals
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["tet_mesh_150", "mixed_sym"])
+def test_fast_polyhedron_field_matches_oracle(cuda, rad, name):
+    h, c = _build(rad, name)
+    _randomize_m(rad, h, 3)
+    g = model.pack_sources(rad._objs, h, tuple(rad._rand))
+    P = np.array(c["points"])
+    for what in (0, 1, 2):
+        got = _native.field(g, P, what, 2)
+        exp = O.field(g, P, what)
+        if what == 2:
+            assert np.array_equal(got, exp)
+        else:
+            assert rel_err(got, exp) < 1e-10
+
+
+def test_fast_polyhedron_fp32_field(cuda, rad):
+    h, c = _build(rad, "tet_mesh_150")
+    _randomize_m(rad, h, 4)
+    g = model.pack_sources(rad._objs, h, tuple(rad._rand))
+    P = np.array(c["points"])
+    assert rel_err(_native.field(g, P, 0, 1), O.field(g, P, 0)) < 5e-5
+
+
+@pytest.mark.parametrize("name", ["tet_mesh_150", "mixed_sym"])
+def test_fast_polyhedron_assembly_matches_oracle(cuda, rad, name):
+    h, c = _build(rad, name)
+    pack = model.pack_interaction(rad._objs, h, 0, tuple(rad._rand))
+    nat = _native.NativeInteraction(pack, 1 | 16)
+    try:
+        N = nat.matrix(np.float64)
+    finally:
+        nat.free()
+    No = O.assemble(pack)
+    assert np.abs(N - No).max() <= 1e-10 * np.abs(No).max()
