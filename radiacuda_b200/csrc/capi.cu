@@ -266,7 +266,7 @@ int radb200_device_sync(void)
 
 int radb200_field_dev(const RadB200Geom *g, const double *d_pts, int64_t npts, int what, int precision, double *d_out)
 {
-  if (npts < 0 || what < 0 || what > 2 || precision < 0 || precision > 1) { set_error("bad field arguments"); return RADB200_E_ARG; }
+  if (npts < 0 || what < 0 || what > 2 || precision < 0 || precision > 2) { set_error("bad field arguments"); return RADB200_E_ARG; }
   DevGeom dg;
   RB_TRY(dg.upload(g));
   RB_TRY(launch_field(dg.view(precision != 0), d_pts, npts, what, precision == 1 ? 1 : 0, d_out, g_fld_scratch, 0));

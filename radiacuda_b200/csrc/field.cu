@@ -42,8 +42,10 @@ __device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<do
         int in = (fabs(qc.x) < hd.x) && (fabs(qc.y) < hd.y) && (fabs(qc.z) < hd.z);
         if (in) f = mk3<double>(mx, my, mz);
       } else {
-        V3<T> Tt, Ss;
-        int in = cuboid_TS<T>(qc, hd, g.g, Tt, Ss);
+        // cuboids stay FP64 in every precision mode, as in the reference (its
+        // cuboid kernel radgpu_fld.cu:788-882 has no FP32 variant)
+        V3<double> Tt, Ss;
+        int in = cuboid_TS<double>(qc, hd, g.g, Tt, Ss);
         double Tx = Tt.x, Ty = Tt.y, Tz = Tt.z, Sx = Ss.x, Sy = Ss.y, Sz = Ss.z;
         f = mk3<double>(Tx * mx - Sz * my - Sy * mz, -Sz * mx + Ty * my - Sx * mz, -Sy * mx - Sx * my + Tz * mz);
         if (what == 0 && in) { f.x += mx; f.y += my; f.z += mz; }

@@ -1,6 +1,6 @@
 """Small, self-contained launches of the hot kernels for profiling.
 
-    python -m radiacuda_b200.profile_cases field    [--tets N] [--points P] [--fp32]
+    python -m radiacuda_b200.profile_cases field    [--tets N] [--points P] [--precision double|single|fast]
     python -m radiacuda_b200.profile_cases assemble [--tets N]
     python -m radiacuda_b200.profile_cases lu       [--tets N] [--mode 0|1]
     python -m radiacuda_b200.profile_cases relax    [--blocks N]
@@ -34,7 +34,7 @@ def main(argv=None):
     ap.add_argument("--points", type=int, default=20000)
     ap.add_argument("--blocks", type=int, default=16)
     ap.add_argument("--mode", type=int, default=1)
-    ap.add_argument("--fp32", action="store_true")
+    ap.add_argument("--precision", default="double", choices=["double", "single", "fast"])
     a = ap.parse_args(argv)
     from . import _native, model, rad
     MD = _models()
@@ -48,7 +48,7 @@ def main(argv=None):
                 lf.obj.m = rng.normal(size=3)
             P = MD.tet_mesh_points(a.points, ncell=ncell)
             t0 = time.perf_counter()
-            B = rad.Fld(m, "b", P, precision="single" if a.fp32 else "double")
+            B = rad.Fld(m, "b", P, precision=a.precision)
             print("field", P.shape[0], "points", time.perf_counter() - t0, "s", float(np.abs(B).max()))
         elif a.case == "assemble":
             im = rad.RlxPre(m, storage="f32")
