@@ -132,6 +132,11 @@ RADB200_API int radb200_device_sync(void);
  * the FP64 (fp64 != 0) or FP32 pipe of the current device in TFLOP/s, the
  * roofline denominator of the transcendental-bound assembly / field kernels. */
 RADB200_API int radb200_measure_fma_peak(int fp64, double *tflops);
+/* Diagnostics, no counterpart in the reference: runs (once) the self-test of
+ * the tcgen05 TF32 trailing-update kernel of the LU against a CUDA-core GEMM.
+ * state: 0 tensor-core path disabled, 1 / 2 enabled (shared-memory layout
+ * variant of the B operand); err: max relative deviation seen.              */
+RADB200_API int radb200_tc_selftest(int *state, double *err);
 
 /* ---- field evaluation ------------------------------------------------------
  * Replaces radGPU_ComputeField (radgpu_fld.h:183-198) and the reference's

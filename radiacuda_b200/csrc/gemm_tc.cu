@@ -1,13 +1,375 @@
-// gemm_tc.cu -- TF32 tensor-core (tcgen05) trailing update for the blocked LU.
+// gemm_tc.cu -- TF32 tensor-core (tcgen05, TMEM accumulator) trailing update
+// of the blocked LU:   C[m x n] -= A[m x k] * B[k x n],   k <= 128,
+// all FP32 row-major inside the LU matrix (leading dimension ld).
+//
+// One CTA (4 warps) owns a 128 x 256 tile of C:
+//   1. warp 0 allocates 256 TMEM columns (128 lanes x 256 FP32 accumulators);
+//   2. the CTA stages A (128 x k) and B (k x 256) in shared memory in the
+//      canonical no-swizzle UMMA layouts (8-row x 16-byte core matrices),
+//      rounding FP32 -> TF32 (round-to-nearest) on the way;
+//   3. one elected thread issues k/8 tcgen05.mma.kind::tf32 (M=128, N=256,
+//      K=8) and commits them to an mbarrier;
+//   4. every warp reads its 32 TMEM lanes with tcgen05.ld, stages the tile in
+//      shared memory, and the CTA subtracts it from C with coalesced 16-byte
+//      loads / stores.
+// Waits on the mbarrier are bounded: on timeout the CTA raises an error flag,
+// still frees its TMEM and returns (the host then falls back to the CUDA-core
+// GEMM and reports the error).
+//
+// Layouts (byte offsets inside the A / B staging buffers):
+//   A, K-major:  (r/8)*4096 + (k/4)*128 + (r%8)*16 + (k%4)*4
+//                descriptor of MMA step s: start A + 256 s, LBO 128, SBO 4096
+//   B, N-major:  (k/8)*8192 + (n/4)*128 + (k%8)*16 + (n%4)*4
+//                descriptor of MMA step s: start B + 8192 s, SBO 128, LBO 8192
+//   B, K-major (alternative): (n/8)*4096 + (k/4)*128 + (n%8)*16 + (k%4)*4
+// The first use runs a self-test against the CUDA-core GEMM and keeps the
+// tensor-core path only if it agrees to TF32 accuracy.
+#include <math.h>
+#include <stdlib.h>
+
+#include <vector>
+
 #include "internal.cuh"
 
 namespace rb {
 
-int tc_gemm_update_f32(float *A, int ld, int m, int n, int k, const float *L, const float *U, cudaStream_t st, int *used)
+constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 128;
+constexpr int TC_THREADS = 128;
+constexpr int TC_SMEM_A = TC_BM * TC_BK * 4;   // 64 KB
+constexpr int TC_SMEM_B = TC_BK * TC_BN * 4;   // 128 KB
+constexpr int TC_SMEM = TC_SMEM_A + TC_SMEM_B + 1024;
+constexpr long long TC_SPIN_LIMIT = 1ll << 22;  // ~0.3 s of polling; the MMAs of a tile take microseconds
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
-  (void)A; (void)ld; (void)m; (void)n; (void)k; (void)L; (void)U; (void)st;
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ float to_tf32(float x)
+{
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+  return d;
+}
+
+// instruction descriptor: F32 accumulate, TF32 A/B, A K-major, B N- or K-major, M=128, N=256
+__host__ __device__ constexpr uint32_t umma_idesc(int b_mn_major)
+{
+  return (1u << 4) | (2u << 7) | (2u << 10) | (0u << 15) | ((uint32_t)b_mn_major << 16) | ((uint32_t)(TC_BN >> 3) << 17) |
+         ((uint32_t)(TC_BM >> 4) << 24);
+}
+
+// overwrite == 0: C -= A B;  overwrite == 1: C = A B (C may alias the rows of A
+// this CTA reads when n <= 256, or the columns of B it reads when m <= 128:
+// operands are fully staged before the first store).
+template <int B_MN>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *C, int ldc, int m, int n, int k,
+                                                                  const float *A, int lda, const float *B, int ldb,
+                                                                  int *__restrict__ err, int overwrite)
+{
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *sbase = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char *sA = sbase;
+  unsigned char *sB = sbase + TC_SMEM_A;
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int timed_out;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int row0 = blockIdx.y * TC_BM, col0 = blockIdx.x * TC_BN;
+  // once any CTA of this launch (or an earlier one) has timed out, the rest
+  // return at once instead of each spending its own wait limit
+  if (*(volatile int *)err != 0) return;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)), "r"(TC_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    timed_out = 0;
+  }
+  const int ksteps = (k + 7) / 8;
+  const int kpad = ksteps * 8;
+
+  // ---- stage A: rows row0.., k columns; lanes -> (r%8, 4 consecutive k-chunks)
+  for (int it = tid; it < (TC_BM / 8) * (kpad / 4) * 8; it += TC_THREADS) {
+    int rr = it & 7;
+    int rest = it >> 3;
+    int kc = rest % (kpad / 4);
+    int rg = rest / (kpad / 4);
+    int r = rg * 8 + rr, kk = kc * 4;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    int gr = row0 + r;
+    if (gr < m) {
+      const float *src = A + (size_t)gr * lda + kk;
+      if (kk + 3 < k) v = *reinterpret_cast<const float4 *>(src);
+      else {
+        if (kk < k) v.x = src[0];
+        if (kk + 1 < k) v.y = src[1];
+        if (kk + 2 < k) v.z = src[2];
+      }
+    }
+    v.x = to_tf32(v.x); v.y = to_tf32(v.y); v.z = to_tf32(v.z); v.w = to_tf32(v.w);
+    *reinterpret_cast<float4 *>(sA + rg * 4096 + kc * 128 + rr * 16) = v;
+  }
+  // ---- stage B
+  if (B_MN) {
+    // lanes -> (k%8, 4 consecutive n-groups)
+    for (int it = tid; it < (kpad / 8) * (TC_BN / 4) * 8; it += TC_THREADS) {
+      int kr = it & 7;
+      int rest = it >> 3;
+      int ng = rest % (TC_BN / 4);
+      int kg = rest / (TC_BN / 4);
+      int kk = kg * 8 + kr, nn = ng * 4;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      int gc = col0 + nn;
+      if (kk < k) {
+        const float *src = B + (size_t)kk * ldb + gc;
+        if (gc + 3 < n) v = *reinterpret_cast<const float4 *>(src);
+        else {
+          if (gc < n) v.x = src[0];
+          if (gc + 1 < n) v.y = src[1];
+          if (gc + 2 < n) v.z = src[2];
+        }
+      }
+      v.x = to_tf32(v.x); v.y = to_tf32(v.y); v.z = to_tf32(v.z); v.w = to_tf32(v.w);
+      *reinterpret_cast<float4 *>(sB + kg * 8192 + ng * 128 + kr * 16) = v;
+    }
+  } else {
+    // K-major B (transposed gather): lanes -> (n%8, 4 consecutive k-chunks)
+    for (int it = tid; it < (TC_BN / 8) * (kpad / 4) * 8; it += TC_THREADS) {
+      int nr = it & 7;
+      int rest = it >> 3;
+      int kc = rest % (kpad / 4);
+      int ngp = rest / (kpad / 4);
+      int nn = ngp * 8 + nr, kk = kc * 4;
+      int gc = col0 + nn;
+      float vv[4];
+      for (int q = 0; q < 4; q++) vv[q] = (gc < n && kk + q < k) ? B[(size_t)(kk + q) * ldb + gc] : 0.f;
+      float4 v = make_float4(to_tf32(vv[0]), to_tf32(vv[1]), to_tf32(vv[2]), to_tf32(vv[3]));
+      *reinterpret_cast<float4 *>(sB + ngp * 4096 + kc * 128 + nr * 16) = v;
+    }
+  }
+  // make the generic-proxy smem writes visible to the tensor core (async proxy)
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_s;
+
+  if (tid == 0) {
+    const uint32_t idesc = umma_idesc(B_MN);
+    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+    for (int s = 0; s < ksteps; s++) {
+      uint64_t da = umma_desc(a0 + 256u * s, 128u, 4096u);
+      uint64_t db = B_MN ? umma_desc(b0 + 8192u * s, 8192u, 128u) : umma_desc(b0 + 256u * s, 128u, 4096u);
+      uint32_t acc = (s > 0) ? 1u : 0u;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+          "l"(da), "l"(db), "r"(idesc), "r"(acc));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&mbar))
+                 : "memory");
+  }
+  // ---- bounded wait for the MMAs (phase 0)
+  {
+    uint32_t done = 0;
+    long long spins = 0;
+    while (!done) {
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+          : "=r"(done)
+          : "r"(smem_u32(&mbar)), "r"(0u)
+          : "memory");
+      if (!done && ++spins > TC_SPIN_LIMIT) {
+        timed_out = 1;
+        break;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (!timed_out) {
+    // ---- TMEM -> registers -> shared, reusing the A+B staging buffers
+    // (128 x 260 floats = 133,120 bytes <= 196,608; free once the MMAs completed)
+    float *stage = reinterpret_cast<float *>(sA);
+    const int SP = TC_BN + 4;  // padded row pitch (floats)
+    const int r = warp * 32 + lane;
+    for (int c = 0; c < TC_BN; c += 16) {
+      uint32_t v[16];
+      uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+            "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      // the staging rows overlap B only after every warp's MMAs are complete (mbarrier above)
+      for (int q = 0; q < 16; q += 4)
+        *reinterpret_cast<float4 *>(stage + (size_t)r * SP + c + q) =
+            make_float4(__uint_as_float(v[q]), __uint_as_float(v[q + 1]), __uint_as_float(v[q + 2]), __uint_as_float(v[q + 3]));
+    }
+    __syncthreads();
+    // ---- C -= tile, coalesced along rows
+    for (int it = tid; it < TC_BM * (TC_BN / 4); it += TC_THREADS) {
+      int rr = it / (TC_BN / 4), c4 = (it % (TC_BN / 4)) * 4;
+      int gr = row0 + rr, gc = col0 + c4;
+      if (gr >= m) continue;
+      float4 t = *reinterpret_cast<const float4 *>(stage + (size_t)rr * SP + c4);
+      float *dst = C + (size_t)gr * ldc + gc;
+      if (overwrite) {
+        if (gc + 3 < n) *reinterpret_cast<float4 *>(dst) = t;
+        else {
+          if (gc < n) dst[0] = t.x;
+          if (gc + 1 < n) dst[1] = t.y;
+          if (gc + 2 < n) dst[2] = t.z;
+        }
+      } else if (gc + 3 < n) {
+        float4 o = *reinterpret_cast<float4 *>(dst);
+        o.x -= t.x; o.y -= t.y; o.z -= t.z; o.w -= t.w;
+        *reinterpret_cast<float4 *>(dst) = o;
+      } else {
+        if (gc < n) dst[0] -= t.x;
+        if (gc + 1 < n) dst[1] -= t.y;
+        if (gc + 2 < n) dst[2] -= t.z;
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(err, 2);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+}
+
+// CUDA-core reference for the self-test: C -= A B (FP32 inputs rounded to TF32 like the tensor path)
+__global__ void tc_ref_kernel(float *C, int ld, int m, int n, int k, const float *A, const float *B)
+{
+  int r = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m || c >= n) return;
+  float s = 0.f;
+  for (int q = 0; q < k; q++) s = fmaf(to_tf32(A[(size_t)r * ld + q]), to_tf32(B[(size_t)q * ld + c]), s);
+  C[(size_t)r * ld + c] -= s;
+}
+
+static int g_tc_state = -1;   // -1 untested, 0 disabled, 1 N-major B, 2 K-major B
+static double g_tc_err = -1.0;
+static DBuf g_tc_err_flag;
+
+static int launch_tc(int variant, float *C, int ldc, int m, int n, int k, const float *A, int lda, const float *B, int ldb,
+                     cudaStream_t st, int overwrite = 0)
+{
+  dim3 grid((n + TC_BN - 1) / TC_BN, (m + TC_BM - 1) / TC_BM);
+  if (grid.y > 65535) { set_error("tensor-core update grid too large"); return RADB200_E_ARG; }
+  if (variant == 1) {
+    RB_CUDA(cudaFuncSetAttribute(tc_update_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    tc_update_kernel<1><<<grid, TC_THREADS, TC_SMEM, st>>>(C, ldc, m, n, k, A, lda, B, ldb, g_tc_err_flag.as<int>(), overwrite);
+  } else {
+    RB_CUDA(cudaFuncSetAttribute(tc_update_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    tc_update_kernel<0><<<grid, TC_THREADS, TC_SMEM, st>>>(C, ldc, m, n, k, A, lda, B, ldb, g_tc_err_flag.as<int>(), overwrite);
+  }
+  return check_launch("tc_update_kernel");
+}
+
+// Runs both B layouts on a random 300 x 520 x 120 update (ragged on purpose)
+// and keeps the first that matches the CUDA-core reference.
+static int tc_selftest()
+{
+  const int m = 300, n = 520, k = 120, ld = 640;
+  std::vector<float> h((size_t)(m + k) * ld);
+  unsigned s = 12345u;
+  for (auto &x : h) { s = s * 1664525u + 1013904223u; x = (float)((s >> 8) * (1.0 / 16777216.0) - 0.5); }
+  DBuf buf, ref;
+  RB_TRY(buf.alloc(h.size() * 4));
+  RB_TRY(ref.alloc(h.size() * 4));
+  RB_TRY(g_tc_err_flag.alloc(sizeof(int)));
+  float *A = buf.as<float>() + (size_t)k * ld;          // rows k.. : A (m x k) at col 0, C at col k
+  float *Bm = buf.as<float>() + k;                      // rows 0..k-1, cols k.. : B
+  float *C = buf.as<float>() + (size_t)k * ld + k;
+  float *Ar = ref.as<float>() + (size_t)k * ld, *Br = ref.as<float>() + k, *Cr = ref.as<float>() + (size_t)k * ld + k;
+  int nn = n - k;  // C is m x (n-k) inside the ld-wide buffer
+  RB_CUDA(cudaMemcpy(ref.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
+  tc_ref_kernel<<<dim3((nn + 127) / 128, m), 128>>>(Cr, ld, m, nn, k, Ar, Br);
+  RB_TRY(check_launch("tc_ref_kernel"));
+  std::vector<float> cref((size_t)(m + k) * ld), ctc((size_t)(m + k) * ld);
+  RB_CUDA(cudaMemcpy(cref.data(), ref.p, h.size() * 4, cudaMemcpyDeviceToHost));
+  g_tc_state = 0;
+  for (int variant = 1; variant <= 2; variant++) {
+    RB_CUDA(cudaMemcpy(buf.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
+    RB_CUDA(cudaMemset(g_tc_err_flag.p, 0, sizeof(int)));
+    int rc = launch_tc(variant == 1 ? 1 : 0, C, ld, m, nn, k, A, ld, Bm, ld, 0);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (rc != 0 || e != cudaSuccess) {
+      cudaGetLastError();
+      set_error("tensor-core self-test launch failed (variant %d): %s", variant, cudaGetErrorString(e));
+      if (e != cudaSuccess) return RADB200_E_CUDA;  // context may be unusable: stop here
+      continue;
+    }
+    int flag = 0;
+    RB_CUDA(cudaMemcpy(&flag, g_tc_err_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {  // an MMA never completed: leave the tensor-core path off, try nothing else
+      set_error("tensor-core self-test: MMA completion wait timed out (variant %d)", variant);
+      g_tc_state = 0;
+      return 0;
+    }
+    RB_CUDA(cudaMemcpy(ctc.data(), buf.p, h.size() * 4, cudaMemcpyDeviceToHost));
+    double maxd = 0.0, maxr = 0.0;
+    for (size_t i = 0; i < ctc.size(); i++) {
+      maxd = std::max(maxd, (double)fabs(ctc[i] - cref[i]));
+      maxr = std::max(maxr, (double)fabs(cref[i]));
+    }
+    g_tc_err = maxd / maxr;
+    if (flag == 0 && g_tc_err < 1e-4) {
+      g_tc_state = variant;
+      return 0;
+    }
+  }
+  return 0;
+}
+
+int tc_gemm_f32(float *C, int ldc, int m, int n, int k, const float *A, int lda, const float *B, int ldb, cudaStream_t st,
+                int *used, int overwrite)
+{
   *used = 0;
+  if (getenv("RADB200_NO_TC")) return 0;
+  if (k > TC_BK || m <= 0 || n <= 0 || (ldc % 4) || (lda % 4) || (ldb % 4) || ((uintptr_t)C & 15) || ((uintptr_t)A & 15) ||
+      ((uintptr_t)B & 15))
+    return 0;
+  if (g_tc_state < 0) RB_TRY(tc_selftest());
+  if (g_tc_state <= 0) return 0;
+  RB_TRY(g_tc_err_flag.alloc(sizeof(int)));
+  RB_TRY(launch_tc(g_tc_state == 1 ? 1 : 0, C, ldc, m, n, k, A, lda, B, ldb, st, overwrite));
+  *used = 1;
+  return 0;
+}
+
+int tc_error_flag(int *flag)
+{
+  *flag = 0;
+  if (!g_tc_err_flag.p) return 0;
+  RB_CUDA(cudaMemcpy(flag, g_tc_err_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
   return 0;
 }
 
 }  // namespace rb
+
+extern "C" RADB200_API int radb200_tc_selftest(int *state, double *err)
+{
+  if (rb::g_tc_state < 0) RB_TRY(rb::tc_selftest());
+  *state = rb::g_tc_state;
+  *err = rb::g_tc_err;
+  return 0;
+}

@@ -117,6 +117,8 @@ struct Intrc {
   DBuf M, H, Mp, F, part, work;
   // LU factors (row-major [n3 x ld]) and solve state
   DBuf LU32, LU64, lu_scratch;
+  DBuf LUinv;                         // [2][3N x 128] inverses of the diagonal blocks (L, then U)
+  int lu_tc = 0;                      // the factorization ran on the tensor cores
   int lu_mode = -1;                   // factors valid for this mode (-1 none)
   DBuf lastM, lastH;                  // converged state of the last solve
   int last_kind = -1;                 // 0 relax, 1 direct
@@ -154,7 +156,11 @@ int lu_precond_transposed(Intrc &I, double *x, cudaStream_t st);
 
 // TF32 tensor-core trailing update A -= L U (gemm_tc.cu); *used = 0 when the
 // shape is not supported and the caller must fall back to the CUDA-core GEMM.
-int tc_gemm_update_f32(float *A, int ld, int m, int n, int k, const float *L, const float *U, cudaStream_t st, int *used);
+// C[m x n] -= A[m x k] B[k x n] (overwrite != 0: C = A B), FP32 row-major,
+// k <= 128, leading dimensions multiples of 4, 16-byte aligned pointers.
+int tc_gemm_f32(float *C, int ldc, int m, int n, int k, const float *A, int lda, const float *B, int ldb, cudaStream_t st,
+                int *used, int overwrite = 0);
+int tc_error_flag(int *flag);  // 2 when a tensor-core CTA hit its wait limit
 
 // ---- kernels (launch wrappers) ---------------------------------------------
 int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what, int precision,

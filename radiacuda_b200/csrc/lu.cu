@@ -8,12 +8,19 @@
 // positive semi-definite, so A is (close to) positive definite and needs no
 // row exchanges; a vanishing pivot is reported as RADB200_E_NUMERIC.
 //
-//   mode F64  : FP64 factors, FP64 trailing GEMM on the FP64 pipe, then FP64
-//               GMRES refinement (usually converged after the first residual).
-//   mode TF32 : FP32 factors whose trailing updates run on the tcgen05 tensor
-//               cores in TF32 with FP32 accumulation (see gemm_tc.cu), then
-//               right-preconditioned FP64 GMRES on A with the FP64 residual
-//               r = b - A M (FP64 N) back to rtol (GMRES-IR).
+// Panel step k (width nb = 128):
+//   1. one CTA factors the diagonal block in shared memory (FP64) and writes
+//      the inverses of its unit-lower and upper triangles, L_kk^-1 and U_kk^-1;
+//   2. L21 = A21 U_kk^-1 and U12 = L_kk^-1 A12 as GEMMs (out of place, then
+//      copied back), so the triangular solves of the panel also run on the
+//      GEMM engine;
+//   3. trailing update A22 -= L21 U12.
+//   mode F64  : FP64 factors, GEMMs on the FP64 pipe (CUDA cores).
+//   mode TF32 : FP32 factors, GEMMs on the tcgen05 tensor cores in TF32 with
+//               FP32 accumulation (gemm_tc.cu), then right-preconditioned FP64
+//               GMRES on A with the FP64 residual (GMRES-IR).
+// Triangular solves with the factors use the stored diagonal-block inverses:
+// per block one small matvec and one column-panel GEMV.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -23,10 +30,9 @@
 
 namespace rb {
 
-constexpr int LU_NB = 128;  // panel width
+constexpr int LU_NB = 128;  // panel width, also the pitch of the inverse buffers
 
-
-// A = I - X N, into FP64 or FP32 storage (rows/cols beyond n3 become identity)
+// A = I - X N, into FP64 or FP32 storage (columns beyond n3 zero)
 template <typename T, typename NT>
 __global__ void build_A_kernel(const NT *__restrict__ N, const double *__restrict__ mat, int n3, int ld, T *__restrict__ A)
 {
@@ -53,20 +59,7 @@ __global__ void build_rhs_kernel(const double *__restrict__ hext, const double *
     b[3 * e + a] = X[3 * a] * hext[3 * e] + X[3 * a + 1] * hext[3 * e + 1] + X[3 * a + 2] * hext[3 * e + 2] + X[9 + a];
 }
 
-// r = b - (x - X (N x)) where y = N x is given:  r = b - x + X y
-__global__ void residual_kernel(const double *__restrict__ b, const double *__restrict__ x, const double *__restrict__ y,
-                                const double *__restrict__ mat, int n, double *__restrict__ r)
-{
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n) return;
-  const double *X = mat + (size_t)e * RADB200_MAT_STRIDE;
-  for (int a = 0; a < 3; a++) {
-    double xy = X[3 * a] * y[3 * e] + X[3 * a + 1] * y[3 * e + 1] + X[3 * a + 2] * y[3 * e + 2];
-    r[3 * e + a] = b[3 * e + a] - x[3 * e + a] + xy;
-  }
-}
-
-// out = x - X y   (A x with y = N x)
+// out = x - X y   (A x, given y = N x); transpose != 0: out = x - N^T-side handled by caller
 __global__ void apply_A_kernel(const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ mat,
                                int n, double *__restrict__ out)
 {
@@ -77,11 +70,12 @@ __global__ void apply_A_kernel(const double *__restrict__ x, const double *__res
     out[3 * e + a] = x[3 * e + a] - (X[3 * a] * y[3 * e] + X[3 * a + 1] * y[3 * e + 1] + X[3 * a + 2] * y[3 * e + 2]);
 }
 
-// ---- diagonal block factorization (one CTA, unpivoted, in shared memory) ----
+// ---- diagonal block: factor (unpivoted) and invert both triangles ----------
 template <typename T>
-__global__ void __launch_bounds__(256) diag_lu_kernel(T *__restrict__ A, int ld, int k0, int nb, int *__restrict__ err)
+__global__ void __launch_bounds__(256) diag_factor_kernel(T *__restrict__ A, int ld, int k0, int nb, T *__restrict__ Linv,
+                                                          T *__restrict__ Uinv, int *__restrict__ err)
 {
-  extern __shared__ double sblk[];  // nb x nb doubles
+  extern __shared__ double sblk[];  // nb x nb
   for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
     int r = e / nb, c = e % nb;
     sblk[e] = (double)A[(size_t)(k0 + r) * ld + k0 + c];
@@ -91,10 +85,8 @@ __global__ void __launch_bounds__(256) diag_lu_kernel(T *__restrict__ A, int ld,
     double piv = sblk[k * nb + k];
     if (threadIdx.x == 0 && !(fabs(piv) > 1e-300)) err[0] = 1;
     double ip = 1.0 / piv;
-    // scale column below pivot
     for (int r = k + 1 + threadIdx.x; r < nb; r += blockDim.x) sblk[r * nb + k] *= ip;
     __syncthreads();
-    // rank-1 update of the trailing part
     int m = nb - k - 1;
     for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
       int r = k + 1 + e / m, c = k + 1 + e % m;
@@ -106,152 +98,122 @@ __global__ void __launch_bounds__(256) diag_lu_kernel(T *__restrict__ A, int ld,
     int r = e / nb, c = e % nb;
     A[(size_t)(k0 + r) * ld + k0 + c] = (T)sblk[e];
   }
-}
-
-// L panel: rows i >= k0+nb:  A[i, k0:k0+nb] <- A[i, k0:k0+nb] * U_kk^-1  (one warp per row)
-template <typename T>
-__global__ void __launch_bounds__(256) trsm_right_upper_kernel(T *__restrict__ A, int ld, int k0, int nb, int r0, int r1)
-{
-  extern __shared__ double sU[];  // nb x nb upper factor
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    int r = e / nb, c = e % nb;
-    sU[e] = (r <= c) ? (double)A[(size_t)(k0 + r) * ld + k0 + c] : 0.0;
-  }
-  __syncthreads();
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int row = r0 + blockIdx.x * 8 + warp;
-  if (row >= r1) return;
-  T *a = A + (size_t)row * ld + k0;
-  // x U = a, x_c = (a_c - sum_{j<c} x_j U_jc) / U_cc ; lanes hold 4 columns each (nb <= 128)
-  double xv[4];
-  for (int q = 0; q < 4; q++) { int c = lane + 32 * q; xv[q] = (c < nb) ? (double)a[c] : 0.0; }
-  for (int c = 0; c < nb; c++) {
-    int owner = c & 31, q = c >> 5;
-    double xc = __shfl_sync(0xffffffffu, xv[q], owner);
-    xc /= sU[c * nb + c];
-    if (lane == owner) xv[q] = xc;
-    for (int qq = 0; qq < 4; qq++) {
-      int cc = lane + 32 * qq;
-      if (cc > c && cc < nb) xv[qq] -= xc * sU[c * nb + cc];
+  // inverses: threads [0, nb) build column j of L^-1, threads [128, 128+nb) column j of U^-1
+  int j = threadIdx.x & 127;
+  bool lower = threadIdx.x < 128;
+  if (j < nb) {
+    double x[LU_NB];
+    for (int i = 0; i < nb; i++) x[i] = 0.0;
+    if (lower) {
+      x[j] = 1.0;
+      for (int i = j + 1; i < nb; i++) {
+        double s = 0.0;
+        for (int q = j; q < i; q++) s += sblk[i * nb + q] * x[q];
+        x[i] = -s;
+      }
+      for (int i = 0; i < nb; i++) Linv[(size_t)(k0 + i) * LU_NB + j] = (T)x[i];
+    } else {
+      x[j] = 1.0 / sblk[j * nb + j];
+      for (int i = j - 1; i >= 0; i--) {
+        double s = 0.0;
+        for (int q = i + 1; q <= j; q++) s += sblk[i * nb + q] * x[q];
+        x[i] = -s / sblk[i * nb + i];
+      }
+      for (int i = 0; i < nb; i++) Uinv[(size_t)(k0 + i) * LU_NB + j] = (T)x[i];
     }
   }
-  for (int q = 0; q < 4; q++) { int c = lane + 32 * q; if (c < nb) a[c] = (T)xv[q]; }
+  // zero the padding columns of partial last blocks
+  if (nb < LU_NB)
+    for (int e = threadIdx.x; e < nb * (LU_NB - nb); e += blockDim.x) {
+      int r = e / (LU_NB - nb), c = nb + e % (LU_NB - nb);
+      Linv[(size_t)(k0 + r) * LU_NB + c] = T(0);
+      Uinv[(size_t)(k0 + r) * LU_NB + c] = T(0);
+    }
 }
 
-// U panel: cols j >= k0+nb:  A[k0:k0+nb, j] <- L_kk^-1 A[k0:k0+nb, j]  (unit lower; one thread per column)
+// ---- CUDA-core GEMM: C[m x n] (=|-=) A[m x k] B[k x n]; 64x64 tile, k-slices of 16
 template <typename T>
-__global__ void __launch_bounds__(128) trsm_left_lower_kernel(T *__restrict__ A, int ld, int k0, int nb, int c0, int c1)
+__global__ void __launch_bounds__(256) gemm_simt_kernel(T *__restrict__ C, int ldc, int m, int n, int k,
+                                                        const T *__restrict__ A, int lda, const T *__restrict__ B, int ldb,
+                                                        int overwrite)
 {
-  extern __shared__ double sL[];
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    int r = e / nb, c = e % nb;
-    sL[e] = (r > c) ? (double)A[(size_t)(k0 + r) * ld + k0 + c] : 0.0;
-  }
-  __syncthreads();
-  int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= c1) return;
-  T *a = A + (size_t)k0 * ld + col;
-  double x[LU_NB];
-  for (int r = 0; r < nb; r++) x[r] = (double)a[(size_t)r * ld];
-  for (int r = 1; r < nb; r++) {
-    double s = x[r];
-    for (int j = 0; j < r; j++) s -= sL[r * nb + j] * x[j];
-    x[r] = s;
-  }
-  for (int r = 0; r < nb; r++) a[(size_t)r * ld] = (T)x[r];
-}
-
-// Trailing update on CUDA cores: A[m0.., n0..] -= L * U ; L = A[m0.., k0:k0+nb], U = A[k0:k0+nb, n0..]
-// 64x64 tile per CTA, 256 threads, 4x4 outputs per thread, k-slices of 16.
-template <typename T>
-__global__ void __launch_bounds__(256) gemm_update_kernel(T *__restrict__ A, int ld, int m0, int m1, int n0, int n1, int k0, int nb)
-{
-  __shared__ T sL[16][64 + 1];
-  __shared__ T sUt[16][64 + 1];
+  __shared__ T sA[16][64 + 1];
+  __shared__ T sB[16][64 + 1];
   int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  int rb = m0 + blockIdx.y * 64, cb = n0 + blockIdx.x * 64;
+  int rb = blockIdx.y * 64, cb = blockIdx.x * 64;
   T acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; i++)
 #pragma unroll
     for (int j = 0; j < 4; j++) acc[i][j] = 0;
-  for (int kk = 0; kk < nb; kk += 16) {
+  for (int kk = 0; kk < k; kk += 16) {
     for (int e = threadIdx.x; e < 64 * 16; e += 256) {
       int r = e / 16, c = e % 16;
-      int gr = rb + r;
-      sL[c][r] = (gr < m1 && kk + c < nb) ? A[(size_t)gr * ld + k0 + kk + c] : T(0);
+      sA[c][r] = (rb + r < m && kk + c < k) ? A[(size_t)(rb + r) * lda + kk + c] : T(0);
       int kr = e / 64, cc = e % 64;
-      int gc = cb + cc;
-      sUt[kr][cc] = (gc < n1 && kk + kr < nb) ? A[(size_t)(k0 + kk + kr) * ld + gc] : T(0);
+      sB[kr][cc] = (cb + cc < n && kk + kr < k) ? B[(size_t)(kk + kr) * ldb + cb + cc] : T(0);
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < 16; k++) {
-      T l[4], u[4];
+    for (int q = 0; q < 16; q++) {
+      T a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; i++) l[i] = sL[k][ty + 16 * i];
+      for (int i = 0; i < 4; i++) a[i] = sA[q][ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; j++) u[j] = sUt[k][tx + 16 * j];
+      for (int j = 0; j < 4; j++) b[j] = sB[q][tx + 16 * j];
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fma(l[i], u[j], acc[i][j]);
+        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
   }
 #pragma unroll
   for (int i = 0; i < 4; i++) {
     int gr = rb + ty + 16 * i;
-    if (gr >= m1) continue;
+    if (gr >= m) continue;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       int gc = cb + tx + 16 * j;
-      if (gc < n1) A[(size_t)gr * ld + gc] -= acc[i][j];
+      if (gc >= n) continue;
+      T *d = C + (size_t)gr * ldc + gc;
+      if (overwrite) *d = acc[i][j];
+      else *d -= acc[i][j];
     }
   }
 }
 
-// ---- triangular solves with the packed factors (in place on x, FP64) ----
-// forward (unit lower), block step: x[k0:k0+nb] done by one CTA, then rows below updated.
 template <typename T>
-__global__ void __launch_bounds__(128) fwd_diag_kernel(const T *__restrict__ A, int ld, int k0, int nb, double *__restrict__ x)
+static int gemm(T *C, int ldc, int m, int n, int k, const T *A, int lda, const T *B, int ldb, int overwrite, cudaStream_t st,
+                int *tc_used)
 {
-  __shared__ double xs[LU_NB];
-  for (int r = threadIdx.x; r < nb; r += blockDim.x) xs[r] = x[k0 + r];
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    int lane = threadIdx.x;
-    for (int r = 1; r < nb; r++) {
-      double s = 0.0;
-      for (int j = lane; j < r; j += 32) s += (double)A[(size_t)(k0 + r) * ld + k0 + j] * xs[j];
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) xs[r] -= s;
-      __syncwarp();
-    }
+  if (m <= 0 || n <= 0) return 0;
+  if (sizeof(T) == 4) {
+    int used = 0;
+    RB_TRY(tc_gemm_f32((float *)C, ldc, m, n, k, (const float *)A, lda, (const float *)B, ldb, st, &used, overwrite));
+    if (used) { *tc_used = 1; return 0; }
   }
-  __syncthreads();
-  for (int r = threadIdx.x; r < nb; r += blockDim.x) x[k0 + r] = xs[r];
+  dim3 grid((n + 63) / 64, (m + 63) / 64);
+  if (grid.y > 65535) { set_error("GEMM grid too large"); return RADB200_E_ARG; }
+  gemm_simt_kernel<T><<<grid, 256, 0, st>>>(C, ldc, m, n, k, A, lda, B, ldb, overwrite);
+  return check_launch("gemm_simt_kernel");
 }
 
-// backward (upper with diagonal)
+// ---- triangular solves with the factors (in place on x, FP64) ----
+// x[k0:k0+nb] <- Inv_k x[k0:k0+nb]   (Inv = L^-1 or U^-1 of diagonal block k)
 template <typename T>
-__global__ void __launch_bounds__(128) bwd_diag_kernel(const T *__restrict__ A, int ld, int k0, int nb, double *__restrict__ x)
+__global__ void __launch_bounds__(LU_NB) block_matvec_kernel(const T *__restrict__ Inv, int k0, int nb, double *__restrict__ x)
 {
   __shared__ double xs[LU_NB];
-  for (int r = threadIdx.x; r < nb; r += blockDim.x) xs[r] = x[k0 + r];
+  int r = threadIdx.x;
+  if (r < nb) xs[r] = x[k0 + r];
   __syncthreads();
-  if (threadIdx.x < 32) {
-    int lane = threadIdx.x;
-    for (int r = nb - 1; r >= 0; r--) {
-      double s = 0.0;
-      for (int j = r + 1 + lane; j < nb; j += 32) s += (double)A[(size_t)(k0 + r) * ld + k0 + j] * xs[j];
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) xs[r] = (xs[r] - s) / (double)A[(size_t)(k0 + r) * ld + k0 + r];
-      __syncwarp();
-    }
+  if (r < nb) {
+    const T *row = Inv + (size_t)(k0 + r) * LU_NB;
+    double s = 0.0;
+    for (int j = 0; j < nb; j++) s += (double)row[j] * xs[j];
+    x[k0 + r] = s;
   }
-  __syncthreads();
-  for (int r = threadIdx.x; r < nb; r += blockDim.x) x[k0 + r] = xs[r];
 }
 
 // x[rows r0..r1) -= A[rows, k0:k0+nb] x[k0:k0+nb] (warp per row)
@@ -273,47 +235,40 @@ __global__ void __launch_bounds__(256) panel_gemv_kernel(const T *__restrict__ A
 }
 
 template <typename T>
-static int lu_factor(T *A, int n3, int ld, int *d_err, bool use_tc, cudaStream_t st, int *tc_used)
+static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaStream_t st, int *tc_used)
 {
+  const int n3 = I.n3, ld = I.ld;
   const int smax = LU_NB * LU_NB * (int)sizeof(double);
-  RB_CUDA(cudaFuncSetAttribute(diag_lu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-  RB_CUDA(cudaFuncSetAttribute(trsm_right_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-  RB_CUDA(cudaFuncSetAttribute(trsm_left_lower_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  RB_CUDA(cudaFuncSetAttribute(diag_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   for (int k0 = 0; k0 < n3; k0 += LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
-    size_t sm = (size_t)nb * nb * sizeof(double);
-    diag_lu_kernel<T><<<1, 256, sm, st>>>(A, ld, k0, nb, d_err);
-    RB_TRY(check_launch("diag_lu_kernel"));
+    diag_factor_kernel<T><<<1, 256, (size_t)nb * nb * sizeof(double), st>>>(A, ld, k0, nb, Linv, Uinv, d_err);
+    RB_TRY(check_launch("diag_factor_kernel"));
     int rest = k0 + nb;
     if (rest >= n3) break;
     int m = n3 - rest;
-    trsm_right_upper_kernel<T><<<(m + 7) / 8, 256, sm, st>>>(A, ld, k0, nb, rest, n3);
-    RB_TRY(check_launch("trsm_right_upper_kernel"));
-    trsm_left_lower_kernel<T><<<(m + 127) / 128, 128, sm, st>>>(A, ld, k0, nb, rest, n3);
-    RB_TRY(check_launch("trsm_left_lower_kernel"));
-    bool done = false;
-    if (use_tc && sizeof(T) == 4) {
-      int used = 0;
-      RB_TRY(tc_gemm_update_f32((float *)A + (size_t)rest * ld + rest, ld, m, m, nb, (const float *)A + (size_t)rest * ld + k0,
-                                (const float *)A + (size_t)k0 * ld + rest, st, &used));
-      if (used) { done = true; *tc_used = 1; }
-    }
-    if (!done) {
-      dim3 grid((m + 63) / 64, (m + 63) / 64);
-      gemm_update_kernel<T><<<grid, 256, 0, st>>>(A, ld, rest, n3, rest, n3, k0, nb);
-      RB_TRY(check_launch("gemm_update_kernel"));
-    }
+    // L21 = A21 U_kk^-1   (tmp: m x LU_NB)
+    RB_TRY(gemm<T>(tmp, LU_NB, m, nb, nb, A + (size_t)rest * ld + k0, ld, Uinv + (size_t)k0 * LU_NB, LU_NB, 1, st, tc_used));
+    RB_CUDA(cudaMemcpy2DAsync(A + (size_t)rest * ld + k0, ld * sizeof(T), tmp, LU_NB * sizeof(T), nb * sizeof(T), m,
+                              cudaMemcpyDeviceToDevice, st));
+    // U12 = L_kk^-1 A12   (tmp: nb x ld)
+    RB_TRY(gemm<T>(tmp, ld, nb, m, nb, Linv + (size_t)k0 * LU_NB, LU_NB, A + (size_t)k0 * ld + rest, ld, 1, st, tc_used));
+    RB_CUDA(cudaMemcpy2DAsync(A + (size_t)k0 * ld + rest, ld * sizeof(T), tmp, ld * sizeof(T), m * sizeof(T), nb,
+                              cudaMemcpyDeviceToDevice, st));
+    // A22 -= L21 U12
+    RB_TRY(gemm<T>(A + (size_t)rest * ld + rest, ld, m, m, nb, A + (size_t)rest * ld + k0, ld, A + (size_t)k0 * ld + rest, ld,
+                   0, st, tc_used));
   }
   return 0;
 }
 
 template <typename T>
-static int lu_solve(const T *A, int n3, int ld, double *x, cudaStream_t st)
+static int lu_solve(const T *A, const T *Linv, const T *Uinv, int n3, int ld, double *x, cudaStream_t st)
 {
   for (int k0 = 0; k0 < n3; k0 += LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
-    fwd_diag_kernel<T><<<1, 128, 0, st>>>(A, ld, k0, nb, x);
-    RB_TRY(check_launch("fwd_diag_kernel"));
+    block_matvec_kernel<T><<<1, LU_NB, 0, st>>>(Linv, k0, nb, x);
+    RB_TRY(check_launch("block_matvec_kernel"));
     int rest = k0 + nb;
     if (rest < n3) {
       panel_gemv_kernel<T><<<(n3 - rest + 7) / 8, 256, 0, st>>>(A, ld, k0, nb, rest, n3, x);
@@ -323,8 +278,8 @@ static int lu_solve(const T *A, int n3, int ld, double *x, cudaStream_t st)
   int last = ((n3 - 1) / LU_NB) * LU_NB;
   for (int k0 = last; k0 >= 0; k0 -= LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
-    bwd_diag_kernel<T><<<1, 128, 0, st>>>(A, ld, k0, nb, x);
-    RB_TRY(check_launch("bwd_diag_kernel"));
+    block_matvec_kernel<T><<<1, LU_NB, 0, st>>>(Uinv, k0, nb, x);
+    RB_TRY(check_launch("block_matvec_kernel"));
     if (k0 > 0) {
       panel_gemv_kernel<T><<<(k0 + 7) / 8, 256, 0, st>>>(A, ld, k0, nb, 0, k0, x);
       RB_TRY(check_launch("panel_gemv_kernel"));
@@ -335,10 +290,12 @@ static int lu_solve(const T *A, int n3, int ld, double *x, cudaStream_t st)
 
 int lu_precond(Intrc &I, double *x, cudaStream_t st)
 {
-  if (I.lu_mode == RADB200_LU_F64) return lu_solve<double>(I.LU64.as<double>(), I.n3, I.ld, x, st);
-  return lu_solve<float>(I.LU32.as<float>(), I.n3, I.ld, x, st);
+  if (I.lu_mode == RADB200_LU_F64)
+    return lu_solve<double>(I.LU64.as<double>(), I.LUinv.as<double>(), I.LUinv.as<double>() + (size_t)I.n3 * LU_NB, I.n3,
+                            I.ld, x, st);
+  return lu_solve<float>(I.LU32.as<float>(), I.LUinv.as<float>(), I.LUinv.as<float>() + (size_t)I.n3 * LU_NB, I.n3, I.ld,
+                         x, st);
 }
-
 
 struct LinOp : Op {
   Intrc &I;
@@ -353,39 +310,56 @@ struct LinOp : Op {
   int precond(double *v) override { return lu_precond(I, v, 0); }
 };
 
-int direct_solve(Intrc &I, int mode, double rtol, int max_iter, double *status)
+int lu_build(Intrc &I, int mode, double *factor_seconds)
 {
   auto t0 = std::chrono::steady_clock::now();
   const int n3 = I.n3, ld = I.ld;
+  if (I.lu_mode == mode) { *factor_seconds = 0.0; return 0; }
   DBuf err;
   RB_TRY(err.alloc(sizeof(int)));
   RB_CUDA(cudaMemset(err.p, 0, sizeof(int)));
   dim3 bgrid((ld + 255) / 256 > 64 ? 64 : (ld + 255) / 256, n3);
   int tc_used = 0;
-  if (I.lu_mode != mode) {
-    if (mode == RADB200_LU_F64) {
-      I.LU32.release();
-      RB_TRY(I.LU64.alloc((size_t)n3 * ld * sizeof(double)));
-      if (I.N64.p) build_A_kernel<double, double><<<bgrid, 256>>>(I.N64.as<double>(), I.mat.as<double>(), n3, ld, I.LU64.as<double>());
-      else build_A_kernel<double, float><<<bgrid, 256>>>(I.N32.as<float>(), I.mat.as<double>(), n3, ld, I.LU64.as<double>());
-      RB_TRY(check_launch("build_A_kernel"));
-      RB_TRY(lu_factor<double>(I.LU64.as<double>(), n3, ld, err.as<int>(), false, 0, &tc_used));
-    } else {
-      I.LU64.release();
-      RB_TRY(I.LU32.alloc((size_t)n3 * ld * sizeof(float)));
-      if (I.N64.p) build_A_kernel<float, double><<<bgrid, 256>>>(I.N64.as<double>(), I.mat.as<double>(), n3, ld, I.LU32.as<float>());
-      else build_A_kernel<float, float><<<bgrid, 256>>>(I.N32.as<float>(), I.mat.as<double>(), n3, ld, I.LU32.as<float>());
-      RB_TRY(check_launch("build_A_kernel"));
-      RB_TRY(lu_factor<float>(I.LU32.as<float>(), n3, ld, err.as<int>(), true, 0, &tc_used));
-    }
-    int herr = 0;
-    RB_CUDA(cudaMemcpy(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (herr) { I.lu_mode = -1; set_error("LU: vanishing pivot (matrix not factorable without pivoting)"); return RADB200_E_NUMERIC; }
-    I.lu_mode = mode;
+  size_t es = (mode == RADB200_LU_F64) ? sizeof(double) : sizeof(float);
+  RB_TRY(I.LUinv.alloc(2 * (size_t)n3 * LU_NB * es));
+  RB_TRY(I.lu_scratch.alloc((size_t)std::max((size_t)n3 * LU_NB, (size_t)LU_NB * ld) * es));
+  if (mode == RADB200_LU_F64) {
+    I.LU32.release();
+    RB_TRY(I.LU64.alloc((size_t)n3 * ld * sizeof(double)));
+    if (I.N64.p) build_A_kernel<double, double><<<bgrid, 256>>>(I.N64.as<double>(), I.mat.as<double>(), n3, ld, I.LU64.as<double>());
+    else build_A_kernel<double, float><<<bgrid, 256>>>(I.N32.as<float>(), I.mat.as<double>(), n3, ld, I.LU64.as<double>());
+    RB_TRY(check_launch("build_A_kernel"));
+    double *inv = I.LUinv.as<double>();
+    RB_TRY(lu_factor<double>(I, I.LU64.as<double>(), inv, inv + (size_t)n3 * LU_NB, I.lu_scratch.as<double>(), err.as<int>(), 0,
+                             &tc_used));
+  } else {
+    I.LU64.release();
+    RB_TRY(I.LU32.alloc((size_t)n3 * ld * sizeof(float)));
+    if (I.N64.p) build_A_kernel<float, double><<<bgrid, 256>>>(I.N64.as<double>(), I.mat.as<double>(), n3, ld, I.LU32.as<float>());
+    else build_A_kernel<float, float><<<bgrid, 256>>>(I.N32.as<float>(), I.mat.as<double>(), n3, ld, I.LU32.as<float>());
+    RB_TRY(check_launch("build_A_kernel"));
+    float *inv = I.LUinv.as<float>();
+    RB_TRY(lu_factor<float>(I, I.LU32.as<float>(), inv, inv + (size_t)n3 * LU_NB, I.lu_scratch.as<float>(), err.as<int>(), 0,
+                            &tc_used));
   }
+  int herr = 0, tcflag = 0;
+  RB_CUDA(cudaMemcpy(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  RB_TRY(tc_error_flag(&tcflag));
+  if (tcflag) { I.lu_mode = -1; set_error("LU: a tensor-core update timed out waiting for its MMAs"); return RADB200_E_TIMEOUT; }
+  if (herr) { I.lu_mode = -1; set_error("LU: vanishing pivot (matrix not factorable without pivoting)"); return RADB200_E_NUMERIC; }
+  I.lu_mode = mode;
+  I.lu_tc = tc_used;
   RB_CUDA(cudaDeviceSynchronize());
-  auto t1 = std::chrono::steady_clock::now();
-  // rhs and initial solve
+  *factor_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return 0;
+}
+
+int direct_solve(Intrc &I, int mode, double rtol, int max_iter, double *status)
+{
+  auto t0 = std::chrono::steady_clock::now();
+  const int n3 = I.n3, ld = I.ld;
+  double tf = 0.0;
+  RB_TRY(lu_build(I, mode, &tf));
   RB_TRY(I.work.alloc((size_t)4 * ld * sizeof(double)));
   double *b = I.work.as<double>(), *tmp = b + ld;
   RB_CUDA(cudaMemset(I.work.p, 0, (size_t)4 * ld * sizeof(double)));
@@ -398,12 +372,10 @@ int direct_solve(Intrc &I, int mode, double rtol, int max_iter, double *status)
   int its = 0;
   RB_TRY(gmres(op, n3, ld, b, I.M.as<double>(), rtol, max_iter, 30, &relres, &its, 0));
   RB_CUDA(cudaDeviceSynchronize());
-  auto t2 = std::chrono::steady_clock::now();
   status[0] = relres;
   status[1] = its;
-  status[2] = std::chrono::duration<double>(t1 - t0).count();
-  status[3] = std::chrono::duration<double>(t2 - t0).count();
-  (void)tc_used;
+  status[2] = tf;
+  status[3] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return 0;
 }
 
