@@ -88,8 +88,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *C, int 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int row0 = blockIdx.y * TC_BM, col0 = blockIdx.x * TC_BN;
   // once any CTA of this launch (or an earlier one) has timed out, the rest
-  // return at once instead of each spending its own wait limit
-  if (*(volatile int *)err != 0) return;
+  // return at once instead of each spending its own wait limit (the decision
+  // is taken by one thread so the whole CTA leaves together)
+  __shared__ int abort_cta;
+  if (tid == 0) abort_cta = *(volatile int *)err;
+  __syncthreads();
+  if (abort_cta != 0) return;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)), "r"(TC_BN));
