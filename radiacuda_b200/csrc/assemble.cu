@@ -31,8 +31,10 @@ __device__ __forceinline__ void elem_tensor(const GeomView &g, int kind, int idx
     Q[6] = -Ss.y; Q[7] = -Ss.x; Q[8] = Tt.z;
     return;
   }
-  if (g.fast && __ldg(&g.tp.tinfo[idx].y) >= 0) {
-    poly_fast<double, true>(g.tp, idx, q, Q);  // vertex/edge form
+  if (g.fast && __ldg(&g.tp.tinfo[idx].y) >= 0) {  // vertex/edge form
+    int ti = __ldg(g.tetidx + idx);
+    if (ti >= 0) tet_fast<double, true>(g.tetrec + (size_t)ti * TET_REC_TENSOR, q, Q);
+    else poly_fast<double, true>(g.tp, idx, q, Q);
     return;
   }
   const double CH = 1.0 / (4.0 * 3.14159265358979);

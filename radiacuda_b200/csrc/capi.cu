@@ -75,12 +75,60 @@ struct HostTopo {
   std::vector<int4> tinfo, tinfo2, tt;
   std::vector<int2> te;
   std::vector<double> tv, tel, teg, teG, ttm, tfn, tfa;
+  std::vector<int> tetidx;     // per polyhedron: tetrahedron record index or -1
+  std::vector<double> tetrec;  // TET_REC_FIELD or TET_REC_TENSOR doubles per tetrahedron
 };
+
+// Fixed-topology record of a tetrahedron (formulas.cuh, tet_fast) from its
+// deduplicated vertices V[4] and counter-clockwise face loops.
+static void build_tet_record(const std::vector<double> &V, const std::vector<std::vector<int>> &loops, const double *M,
+                             bool tensor, std::vector<double> &out)
+{
+  double rec[TET_REC_TENSOR] = {0};
+  for (int k = 0; k < 12; k++) rec[k] = V[k];
+  for (int e = 0; e < 6; e++) {
+    int a = tet_edge_a(e), b = tet_edge_b(e);
+    double dx = V[3 * b] - V[3 * a], dy = V[3 * b + 1] - V[3 * a + 1], dz = V[3 * b + 2] - V[3 * a + 2];
+    rec[12 + e] = sqrt(dx * dx + dy * dy + dz * dz);
+  }
+  for (int f = 0; f < 4; f++) {
+    // the loop of face f is the one without vertex f
+    const std::vector<int> *L = nullptr;
+    for (auto &lp : loops)
+      if (lp[0] != f && lp[1] != f && lp[2] != f) L = &lp;
+    const double *p0 = &V[3 * (*L)[0]], *p1 = &V[3 * (*L)[1]], *p2 = &V[3 * (*L)[2]];
+    double u[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]}, w[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+    double m[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+    double mn = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    double n[3] = {m[0] / mn, m[1] / mn, m[2] / mn};
+    double sigma = M[0] * n[0] + M[1] * n[1] + M[2] * n[2];
+    for (int c = 0; c < 3; c++) {
+      rec[18 + 3 * f + c] = m[c];
+      rec[30 + 3 * f + c] = tensor ? n[c] : sigma * n[c];
+    }
+    for (int j = 0; j < 3; j++) {  // directed edges of the counter-clockwise loop
+      int a = (*L)[j], b = (*L)[(j + 1) % 3];
+      double t[3] = {V[3 * b] - V[3 * a], V[3 * b + 1] - V[3 * a + 1], V[3 * b + 2] - V[3 * a + 2]};
+      double tl = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+      for (int c = 0; c < 3; c++) t[c] /= tl;
+      double nu[3] = {t[1] * n[2] - t[2] * n[1], t[2] * n[0] - t[0] * n[2], t[0] * n[1] - t[1] * n[0]};
+      int e = tet_pair(std::min(a, b), std::max(a, b));
+      if (tensor) {
+        for (int r = 0; r < 3; r++)
+          for (int c = 0; c < 3; c++) rec[42 + 9 * e + 3 * r + c] += nu[r] * n[c];
+      } else {
+        for (int c = 0; c < 3; c++) rec[42 + 3 * e + c] += sigma * nu[c];
+      }
+    }
+  }
+  out.insert(out.end(), rec, rec + (tensor ? TET_REC_TENSOR : TET_REC_FIELD));
+}
 
 static void build_topo(const RadB200Geom *G, bool tensor, HostTopo &h)
 {
   h.tinfo.resize(G->n_poly);
   h.tinfo2.resize(G->n_poly);
+  h.tetidx.assign(G->n_poly, -1);
   for (int p = 0; p < G->n_poly; p++) {
     int f0 = G->poly_info[4 * p], nf = G->poly_info[4 * p + 1];
     const double *M = G->poly + (size_t)p * RADB200_POLY_STRIDE + 3;
@@ -111,6 +159,10 @@ static void build_topo(const RadB200Geom *G, bool tensor, HostTopo &h)
       }
     }
     int nv = (int)(V.size() / 3);
+    if (nv == 4 && nf == 4 && loops[0].size() == 3 && loops[1].size() == 3 && loops[2].size() == 3 && loops[3].size() == 3) {
+      h.tetidx[p] = (int)(h.tetrec.size() / (tensor ? TET_REC_TENSOR : TET_REC_FIELD));
+      build_tet_record(V, loops, M, tensor, h.tetrec);
+    }
     if (nv > POLY_NV_FAST) {  // too many vertices for the register form: reference form only
       h.tinfo[p] = make_int4(v0, -1, e0, 0);
       h.tinfo2[p] = make_int4(t0, 0, ff0, 0);
@@ -186,6 +238,9 @@ int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs)
     RB_TRY(ttm.upload(h.ttm.data(), h.ttm.size() * sizeof(double)));
     RB_TRY(tfn.upload(h.tfn.data(), h.tfn.size() * sizeof(double)));
     RB_TRY(tfa.upload(h.tfa.data(), h.tfa.size() * sizeof(double)));
+    RB_TRY(tetidx.upload(h.tetidx.data(), h.tetidx.size() * sizeof(int)));
+    RB_TRY(tetrec.upload(h.tetrec.data(), h.tetrec.size() * sizeof(double)));
+    all_tets = std::all_of(h.tetidx.begin(), h.tetidx.end(), [](int t) { return t >= 0; }) ? 1 : 0;
   }
   RB_TRY(trf.upload(G->trf, (size_t)G->n_trf * RADB200_TRF_STRIDE * sizeof(double)));
   RB_TRY(rec.upload(G->rec, (size_t)G->n_rec * RADB200_REC_STRIDE * sizeof(double)));
@@ -199,14 +254,19 @@ int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs)
   RB_TRY(bkg.upload(G->bkg, (size_t)G->n_bkg * 3 * sizeof(double)));
   // unit table: one entry per (source, image); cuboids, polyhedra, arcs, backgrounds
   std::vector<int4> u;
+  ustart[0] = 0;
   for (int i = 0; i < G->n_rec; i++)
     for (int t = 0; t < G->rec_img[2 * i + 1]; t++) u.push_back(make_int4(0, i, G->rec_img[2 * i] + t, 0));
+  ustart[1] = (int)u.size();
   for (int i = 0; i < G->n_poly; i++)
     for (int t = 0; t < G->poly_info[4 * i + 3]; t++) u.push_back(make_int4(1, i, G->poly_info[4 * i + 2] + t, 0));
+  ustart[2] = (int)u.size();
   for (int i = 0; i < G->n_arc; i++)
     for (int t = 0; t < G->arc_img[2 * i + 1]; t++) u.push_back(make_int4(2, i, G->arc_img[2 * i] + t, 0));
+  ustart[3] = (int)u.size();
   for (int i = 0; i < G->n_bkg; i++)
     for (int t = 0; t < G->bkg_img[2 * i + 1]; t++) u.push_back(make_int4(3, i, G->bkg_img[2 * i] + t, 0));
+  ustart[4] = (int)u.size();
   n_units = (int)u.size();
   RB_TRY(units.upload(u.data(), u.size() * sizeof(int4)));
   n_rec = G->n_rec;
@@ -222,10 +282,14 @@ GeomView DevGeom::view(int fast) const
   v.poly = poly.as<double>(); v.poly_info = poly_info.as<int>(); v.face = face.as<double>();
   v.face_vtx = face_vtx.as<int>(); v.vtx2d = vtx2d.as<double>(); v.arc = arc.as<double>();
   v.bkg = bkg.as<double>(); v.units = units.as<int4>(); v.n_units = n_units; v.g = g;
+  for (int k = 0; k < 5; k++) v.ustart[k] = ustart[k];
   v.tp.tinfo = tinfo.as<int4>(); v.tp.tinfo2 = tinfo2.as<int4>(); v.tp.tv = tv.as<double>();
   v.tp.te = te.as<int2>(); v.tp.tel = tel.as<double>(); v.tp.teg = teg.as<double>(); v.tp.teG = teG.as<double>();
   v.tp.tt = tt.as<int4>(); v.tp.ttm = ttm.as<double>(); v.tp.tfn = tfn.as<double>(); v.tp.tfa = tfa.as<double>();
   v.fast = (fast && tinfo.p) ? 1 : 0;
+  v.tetidx = tetidx.as<int>();
+  v.tetrec = tetrec.as<double>();
+  v.all_tets = all_tets;
   return v;
 }
 

@@ -19,7 +19,12 @@
 
 namespace rb {
 
-template <typename T>
+// KIND: 0 cuboid, 1 polyhedron (face-by-face form), 2 polyhedron (vertex/edge
+// form where available), 3 arc current, 4 background.  One kernel is compiled
+// per kind so each gets the register budget of its own formula.
+enum { UK_REC = 0, UK_POLY = 1, UK_POLY_FAST = 2, UK_ARC = 3, UK_BKG = 4, UK_TET = 5 };
+
+template <typename T, int KIND>
 __device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<double> P, int what)
 {
   const double *Tr = g.trf + (size_t)u.z * RADB200_TRF_STRIDE;
@@ -29,7 +34,7 @@ __device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<do
                              __ldg(Tr + 3) * dx + __ldg(Tr + 4) * dy + __ldg(Tr + 5) * dz,
                              __ldg(Tr + 6) * dx + __ldg(Tr + 7) * dy + __ldg(Tr + 8) * dz);
   V3<double> f = mk3<double>(0, 0, 0);
-  if (u.x == 0) {
+  if (KIND == UK_REC) {
     const double *r = g.rec + (size_t)u.y * RADB200_REC_STRIDE;
     double jx = __ldg(r + 9), jy = __ldg(r + 10), jz = __ldg(r + 11);
     V3<double> qc = mk3<double>(q.x - __ldg(r + 0), q.y - __ldg(r + 1), q.z - __ldg(r + 2));
@@ -51,17 +56,28 @@ __device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<do
         if (what == 0 && in) { f.x += mx; f.y += my; f.z += mz; }
       }
     }
-  } else if (u.x == 1 && g.fast && __ldg(&g.tp.tinfo[u.y].y) >= 0) {
-    // vertex/edge form (formulas.cuh, poly_fast)
+  } else if (KIND == UK_TET) {
+    // every polyhedron is a tetrahedron: fixed-topology vertex/edge form only
     const double *pr = g.poly + (size_t)u.y * RADB200_POLY_STRIDE;
     double h[3];
-    int in = poly_fast<T, false>(g.tp, u.y, q, h);
+    int in = tet_fast<T, false>(g.tetrec + (size_t)__ldg(g.tetidx + u.y) * TET_REC_FIELD, q, h);
     if (what == 2) f = in ? mk3<double>(__ldg(pr + 3), __ldg(pr + 4), __ldg(pr + 5)) : mk3<double>(0, 0, 0);
     else {
       f = mk3<double>(h[0], h[1], h[2]);
       if (what == 0 && in) { f.x += __ldg(pr + 3); f.y += __ldg(pr + 4); f.z += __ldg(pr + 5); }
     }
-  } else if (u.x == 1) {
+  } else if (KIND == UK_POLY_FAST && __ldg(&g.tp.tinfo[u.y].y) >= 0) {
+    // vertex/edge form (formulas.cuh: tet_fast for tetrahedra, poly_fast otherwise)
+    const double *pr = g.poly + (size_t)u.y * RADB200_POLY_STRIDE;
+    double h[3];
+    int ti = __ldg(g.tetidx + u.y);
+    int in = (ti >= 0) ? tet_fast<T, false>(g.tetrec + (size_t)ti * TET_REC_FIELD, q, h) : poly_fast<T, false>(g.tp, u.y, q, h);
+    if (what == 2) f = in ? mk3<double>(__ldg(pr + 3), __ldg(pr + 4), __ldg(pr + 5)) : mk3<double>(0, 0, 0);
+    else {
+      f = mk3<double>(h[0], h[1], h[2]);
+      if (what == 0 && in) { f.x += __ldg(pr + 3); f.y += __ldg(pr + 4); f.z += __ldg(pr + 5); }
+    }
+  } else if (KIND == UK_POLY || KIND == UK_POLY_FAST) {
     const double *pr = g.poly + (size_t)u.y * RADB200_POLY_STRIDE;
     double mx = __ldg(pr + 3), my = __ldg(pr + 4), mz = __ldg(pr + 5);
     int f0 = __ldg(g.poly_info + 4 * u.y), nf = __ldg(g.poly_info + 4 * u.y + 1);
@@ -100,7 +116,7 @@ __device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<do
       f = mk3<double>(hx, hy, hz);
       if (what == 0 && inside) { f.x += mx; f.y += my; f.z += mz; }
     }
-  } else if (u.x == 2) {
+  } else if (KIND == UK_ARC) {
     if (what != 2) f = arc_field(g.arc + (size_t)u.y * RADB200_ARC_STRIDE, q);
   } else {
     if (what != 2) {
@@ -114,71 +130,100 @@ __device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<do
                      __ldg(F + 6) * f.x + __ldg(F + 7) * f.y + __ldg(F + 8) * f.z);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(128) field_kernel(GeomView g, const double *__restrict__ pts, int64_t npts,
-                                                    int what, double *__restrict__ out, int chunk)
+// Units [ub, ue) of one kind; gridDim.y splits them into chunks.  With one
+// chunk the result goes to out directly (accumulate: out += result), else to
+// the chunk's slice of the partial buffer.
+template <typename T, int KIND>
+__global__ void __launch_bounds__(128) field_kernel(GeomView g, const double *__restrict__ pts, int64_t npts, int what,
+                                                    double *__restrict__ out, int ub, int ue, int chunk, int accumulate)
 {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int u0 = blockIdx.y * chunk, u1 = min(g.n_units, u0 + chunk);
+  int u0 = ub + blockIdx.y * chunk, u1 = min(ue, u0 + chunk);
   bool active = i < npts;
   V3<double> P = mk3<double>(0, 0, 0);
   if (active) P = mk3<double>(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
   double ax = 0, ay = 0, az = 0;
   for (int u = u0; u < u1; u++) {
     int4 un = __ldg(g.units + u);
-    V3<double> f = eval_unit<T>(g, un, P, what);
+    V3<double> f = eval_unit<T, KIND>(g, un, P, what);
     ax += f.x; ay += f.y; az += f.z;
   }
   if (active) {
     double *o = out + ((size_t)blockIdx.y * npts + i) * 3;
-    o[0] = ax; o[1] = ay; o[2] = az;
+    if (accumulate) { o[0] += ax; o[1] += ay; o[2] += az; }
+    else { o[0] = ax; o[1] = ay; o[2] = az; }
   }
 }
 
-// out[i] = sum_c partial[c][i], fixed order c = 0..nc-1
-__global__ void chunk_reduce_kernel(const double *__restrict__ part, int nc, int64_t n3, double *__restrict__ out)
+// out[i] (=|+=) sum_c partial[c][i], fixed order c = 0..nc-1
+__global__ void chunk_reduce_kernel(const double *__restrict__ part, int nc, int64_t n3, double *__restrict__ out, int accumulate)
 {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n3) return;
-  double s = 0;
+  double s = accumulate ? out[i] : 0.0;
   for (int c = 0; c < nc; c++) s += part[(size_t)c * n3 + i];
   out[i] = s;
+}
+
+template <typename T, int KIND>
+static int launch_kind(const GeomView &g, const double *d_pts, int64_t npts, int what, double *d_out, int ub, int ue,
+                       int accumulate, DBuf &scratch, cudaStream_t st)
+{
+  const int TPB = 128;
+  int64_t nblk = (npts + TPB - 1) / TPB;
+  int nu = ue - ub;
+  // split the unit range when the points alone give fewer than ~8 CTAs per SM
+  int nchunk = 1;
+  const int64_t target = 148 * 8;
+  if (nblk < target) nchunk = (int)((target + nblk - 1) / nblk);
+  if (nchunk > nu) nchunk = nu;
+  if (nchunk > 65535) nchunk = 65535;
+  int chunk = (nu + nchunk - 1) / nchunk;
+  nchunk = (nu + chunk - 1) / chunk;
+  dim3 grid((unsigned)nblk, (unsigned)nchunk);
+  if (nchunk == 1) {
+    field_kernel<T, KIND><<<grid, TPB, 0, st>>>(g, d_pts, npts, what, d_out, ub, ue, chunk, accumulate);
+    return check_launch("field_kernel");
+  }
+  RB_TRY(scratch.alloc((size_t)nchunk * npts * 3 * sizeof(double)));
+  field_kernel<T, KIND><<<grid, TPB, 0, st>>>(g, d_pts, npts, what, scratch.as<double>(), ub, ue, chunk, 0);
+  RB_TRY(check_launch("field_kernel"));
+  int64_t n3 = npts * 3;
+  chunk_reduce_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(scratch.as<double>(), nchunk, n3, d_out, accumulate);
+  return check_launch("chunk_reduce_kernel");
 }
 
 int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what, int precision, double *d_out,
                  DBuf &scratch, cudaStream_t st)
 {
   if (npts <= 0) return 0;
+  if ((npts + 127) / 128 > INT32_MAX) { set_error("too many points"); return RADB200_E_ARG; }
   if (g.n_units == 0) {
     RB_CUDA(cudaMemsetAsync(d_out, 0, (size_t)npts * 3 * sizeof(double), st));
     return 0;
   }
-  const int TPB = 128;
-  int64_t nblk = (npts + TPB - 1) / TPB;
-  if (nblk > INT32_MAX) { set_error("too many points"); return RADB200_E_ARG; }
-  // split the unit list when the points alone give fewer than ~8 CTAs per SM
-  int nchunk = 1;
-  const int64_t target = 148 * 8;
-  if (nblk < target) nchunk = (int)((target + nblk - 1) / nblk);
-  if (nchunk > g.n_units) nchunk = g.n_units;
-  if (nchunk > 65535) nchunk = 65535;
-  int chunk = (g.n_units + nchunk - 1) / nchunk;
-  nchunk = (g.n_units + chunk - 1) / chunk;
-  double *dst = d_out;
-  if (nchunk > 1) {
-    RB_TRY(scratch.alloc((size_t)nchunk * npts * 3 * sizeof(double)));
-    dst = scratch.as<double>();
-  }
-  dim3 grid((unsigned)nblk, (unsigned)nchunk);
-  if (precision == 1)
-    field_kernel<float><<<grid, TPB, 0, st>>>(g, d_pts, npts, what, dst, chunk);
-  else
-    field_kernel<double><<<grid, TPB, 0, st>>>(g, d_pts, npts, what, dst, chunk);
-  RB_TRY(check_launch("field_kernel"));
-  if (nchunk > 1) {
-    int64_t n3 = npts * 3;
-    chunk_reduce_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(dst, nchunk, n3, d_out);
-    RB_TRY(check_launch("chunk_reduce_kernel"));
+  // units are ordered by kind (cuboids, polyhedra, arcs, backgrounds): one launch per kind present
+  int acc = 0;
+  for (int kind = 0; kind < 4; kind++) {
+    int ub = g.ustart[kind], ue = g.ustart[kind + 1];
+    if (ue <= ub) continue;
+    int rc;
+    if (kind == 0)
+      rc = launch_kind<double, UK_REC>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
+    else if (kind == 1 && g.fast && g.all_tets)
+      rc = (precision == 1) ? launch_kind<float, UK_TET>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st)
+                            : launch_kind<double, UK_TET>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
+    else if (kind == 1 && g.fast)
+      rc = (precision == 1) ? launch_kind<float, UK_POLY_FAST>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st)
+                            : launch_kind<double, UK_POLY_FAST>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
+    else if (kind == 1)
+      rc = launch_kind<double, UK_POLY>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
+    else if (kind == 2)
+      rc = launch_kind<double, UK_ARC>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
+    else
+      rc = launch_kind<double, UK_BKG>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
+    RB_TRY(rc);
+    acc = 1;
   }
   return 0;
 }

@@ -486,4 +486,85 @@ __device__ __forceinline__ int poly_fast(const TopoView &tp, int p, V3<double> q
   return omega_tot < -6.283185307179586;
 }
 
+// ---------------------------------------------------------------------------
+// Tetrahedron, vertex/edge form with a fixed topology: edges (01 02 03 12 13
+// 23), faces opposite each vertex, the face cross products m_t oriented
+// outward on the host.  No index selection in the inner loop, everything
+// unrolled.  Record (object frame), TET_REC_FIELD doubles:
+//   [0,12) vertices  [12,18) edge lengths  [18,30) m_t  [30,42) a_f = sigma_f n_f
+//   [42,60) g_e = sum_f sigma_f nu_{e,f}
+// TET_REC_TENSOR doubles: [0,30) as above, [30,42) n_f, [42,96) G_e (3x3 each).
+constexpr int TET_REC_FIELD = 60, TET_REC_TENSOR = 96;
+__host__ __device__ constexpr int tet_edge_a(int e) { return e < 3 ? 0 : (e < 5 ? 1 : 2); }
+__host__ __device__ constexpr int tet_edge_b(int e) { return e == 0 ? 1 : e == 1 ? 2 : e == 2 ? 3 : e == 3 ? 2 : 3; }
+// face f (opposite vertex f) = triangle (a, b, c)
+__host__ __device__ constexpr int tet_face_a(int f) { return f == 0 ? 1 : 0; }
+__host__ __device__ constexpr int tet_face_b(int f) { return f == 0 ? 2 : (f == 1 ? 2 : 1); }
+__host__ __device__ constexpr int tet_face_c(int f) { return f == 3 ? 2 : 3; }
+// index of the vertex pair (i < j) in the edge list
+__host__ __device__ constexpr int tet_pair(int i, int j) { return i == 0 ? j - 1 : (i == 1 ? j + 1 : 5); }
+
+template <typename T, bool TENSOR>
+__device__ __forceinline__ int tet_fast(const double *__restrict__ rec, V3<double> q, double *out)
+{
+  const double C = 1.0 / (4.0 * 3.141592653589793238);
+  T rx[4], ry[4], rz[4], R[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    rx[k] = T(__ldg(rec + 3 * k) - q.x);
+    ry[k] = T(__ldg(rec + 3 * k + 1) - q.y);
+    rz[k] = T(__ldg(rec + 3 * k + 2) - q.z);
+    R[k] = sqrtT(rx[k] * rx[k] + ry[k] * ry[k] + rz[k] * rz[k]);
+  }
+  T d[6];  // r_i . r_j per edge
+#pragma unroll
+  for (int e = 0; e < 6; e++) {
+    const int a = tet_edge_a(e), b = tet_edge_b(e);
+    d[e] = rx[a] * rx[b] + ry[a] * ry[b] + rz[a] * rz[b];
+  }
+  double acc[TENSOR ? 9 : 3];
+#pragma unroll
+  for (int k = 0; k < (TENSOR ? 9 : 3); k++) acc[k] = 0.0;
+#pragma unroll
+  for (int e = 0; e < 6; e++) {
+    const int a = tet_edge_a(e), b = tet_edge_b(e);
+    T l = T(__ldg(rec + 12 + e));
+    T D;
+    if (d[e] >= T(0)) D = R[a] * R[b] + d[e];
+    else {
+      T cx = ry[a] * rz[b] - rz[a] * ry[b], cy = rz[a] * rx[b] - rx[a] * rz[b], cz = rx[a] * ry[b] - ry[a] * rx[b];
+      D = (cx * cx + cy * cy + cz * cz) / (R[a] * R[b] - d[e]);
+    }
+    double L = (double)log1pT<T>(l * (R[a] + R[b] + l) / D);
+    if (TENSOR) {
+#pragma unroll
+      for (int k = 0; k < 9; k++) acc[k] += L * __ldg(rec + 42 + 9 * e + k);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; k++) acc[k] += L * __ldg(rec + 42 + 3 * e + k);
+    }
+  }
+  double omega_tot = 0.0;
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const int a = tet_face_a(f), b = tet_face_b(f), c = tet_face_c(f);
+    T num = rx[a] * T(__ldg(rec + 18 + 3 * f)) + ry[a] * T(__ldg(rec + 19 + 3 * f)) + rz[a] * T(__ldg(rec + 20 + 3 * f));
+    T den = R[a] * R[b] * R[c] + d[tet_pair(a, b)] * R[c] + d[tet_pair(a, c)] * R[b] + d[tet_pair(b, c)] * R[a];
+    double om = 2.0 * (double)atan2T(-num, den);
+    omega_tot += om;
+    if (TENSOR) {
+      double n0 = __ldg(rec + 30 + 3 * f), n1 = __ldg(rec + 31 + 3 * f), n2 = __ldg(rec + 32 + 3 * f);
+      acc[0] += om * n0 * n0; acc[1] += om * n0 * n1; acc[2] += om * n0 * n2;
+      acc[3] += om * n1 * n0; acc[4] += om * n1 * n1; acc[5] += om * n1 * n2;
+      acc[6] += om * n2 * n0; acc[7] += om * n2 * n1; acc[8] += om * n2 * n2;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; k++) acc[k] += om * __ldg(rec + 30 + 3 * f + k);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < (TENSOR ? 9 : 3); k++) out[k] = C * acc[k];
+  return omega_tot < -6.283185307179586;
+}
+
 }  // namespace rb

@@ -82,10 +82,14 @@ struct GeomView {
   const double *vtx2d;
   const double *arc;
   const double *bkg;
-  const int4 *units;  // {kind, source, transform, 0}
+  const int4 *units;  // {kind, source, transform, 0}, ordered by kind
   int n_units;
+  int ustart[5];      // first unit of each kind (cuboid, polyhedron, arc, background), end
   Guard g;
   TopoView tp;        // vertex/edge form of the polyhedra (tinfo.y < 0: not available)
+  const int *tetidx;  // per polyhedron: tetrahedron record or -1
+  const double *tetrec;
+  int all_tets;       // every polyhedron has a tetrahedron record
   int fast;           // 1: evaluate polyhedra in the vertex/edge form
 };
 
@@ -93,7 +97,10 @@ struct DevGeom {
   DBuf trf, rec, rec_img, poly, poly_info, face, face_vtx, vtx2d, arc, bkg, units;
   // polyhedron topology (vertex/edge form), see TopoView in formulas.cuh
   DBuf tinfo, tinfo2, tv, te, tel, teg, teG, tt, ttm, tfn, tfa;
+  DBuf tetidx, tetrec;  // fixed-topology tetrahedron records (tet_fast)
   int n_units = 0, n_rec = 0, n_poly = 0;
+  int ustart[5] = {0, 0, 0, 0, 0};
+  int all_tets = 0;
   Guard g{0, 0, 0};
   int upload(const RadB200Geom *G, bool tensor_coeffs = false);
   GeomView view(int fast = 0) const;

@@ -183,6 +183,26 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(T *__restrict__ C, int l
   }
 }
 
+// dst[r][c] = src[r][c] for r < rows, c < cols (row-major, leading dimensions in elements)
+template <typename T>
+__global__ void copy2d_kernel(T *__restrict__ dst, int ldd, const T *__restrict__ src, int lds, int rows, int cols)
+{
+  int64_t tot = (int64_t)rows * cols;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    int r = (int)(i / cols), c = (int)(i % cols);
+    dst[(size_t)r * ldd + c] = src[(size_t)r * lds + c];
+  }
+}
+
+template <typename T>
+static int copy2d(T *dst, int ldd, const T *src, int lds, int rows, int cols, cudaStream_t st)
+{
+  int64_t tot = (int64_t)rows * cols;
+  int nb = (int)std::min<int64_t>((tot + 255) / 256, 148 * 16);
+  copy2d_kernel<T><<<std::max(nb, 1), 256, 0, st>>>(dst, ldd, src, lds, rows, cols);
+  return check_launch("copy2d_kernel");
+}
+
 template <typename T>
 static int gemm(T *C, int ldc, int m, int n, int k, const T *A, int lda, const T *B, int ldb, int overwrite, cudaStream_t st,
                 int *tc_used)
@@ -240,25 +260,42 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
   const int n3 = I.n3, ld = I.ld;
   const int smax = LU_NB * LU_NB * (int)sizeof(double);
   RB_CUDA(cudaFuncSetAttribute(diag_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  // RADB200_LU_TIMING=1 prints the time of each phase (synchronizes per phase)
+  const bool timing = getenv("RADB200_LU_TIMING") != nullptr;
+  double tph[4] = {0, 0, 0, 0};
+  auto t_last = std::chrono::steady_clock::now();
+  auto phase = [&](int p) -> int {
+    if (!timing) return 0;
+    RB_CUDA(cudaStreamSynchronize(st));
+    auto t = std::chrono::steady_clock::now();
+    tph[p] += std::chrono::duration<double>(t - t_last).count();
+    t_last = t;
+    return 0;
+  };
   for (int k0 = 0; k0 < n3; k0 += LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
     diag_factor_kernel<T><<<1, 256, (size_t)nb * nb * sizeof(double), st>>>(A, ld, k0, nb, Linv, Uinv, d_err);
     RB_TRY(check_launch("diag_factor_kernel"));
+    RB_TRY(phase(0));
     int rest = k0 + nb;
     if (rest >= n3) break;
     int m = n3 - rest;
     // L21 = A21 U_kk^-1   (tmp: m x LU_NB)
     RB_TRY(gemm<T>(tmp, LU_NB, m, nb, nb, A + (size_t)rest * ld + k0, ld, Uinv + (size_t)k0 * LU_NB, LU_NB, 1, st, tc_used));
-    RB_CUDA(cudaMemcpy2DAsync(A + (size_t)rest * ld + k0, ld * sizeof(T), tmp, LU_NB * sizeof(T), nb * sizeof(T), m,
-                              cudaMemcpyDeviceToDevice, st));
+    RB_TRY(copy2d<T>(A + (size_t)rest * ld + k0, ld, tmp, LU_NB, m, nb, st));
+    RB_TRY(phase(1));
     // U12 = L_kk^-1 A12   (tmp: nb x ld)
     RB_TRY(gemm<T>(tmp, ld, nb, m, nb, Linv + (size_t)k0 * LU_NB, LU_NB, A + (size_t)k0 * ld + rest, ld, 1, st, tc_used));
-    RB_CUDA(cudaMemcpy2DAsync(A + (size_t)k0 * ld + rest, ld * sizeof(T), tmp, ld * sizeof(T), m * sizeof(T), nb,
-                              cudaMemcpyDeviceToDevice, st));
+    RB_TRY(copy2d<T>(A + (size_t)k0 * ld + rest, ld, tmp, ld, nb, m, st));
+    RB_TRY(phase(2));
     // A22 -= L21 U12
     RB_TRY(gemm<T>(A + (size_t)rest * ld + rest, ld, m, m, nb, A + (size_t)rest * ld + k0, ld, A + (size_t)k0 * ld + rest, ld,
                    0, st, tc_used));
+    RB_TRY(phase(3));
   }
+  if (timing)
+    fprintf(stderr, "[radb200 LU n=%d %s] diag %.3f s, L panel %.3f s, U panel %.3f s, trailing %.3f s\n", n3,
+            sizeof(T) == 4 ? "fp32/tf32" : "fp64", tph[0], tph[1], tph[2], tph[3]);
   return 0;
 }
 
