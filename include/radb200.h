@@ -147,6 +147,20 @@ RADB200_API int radb200_tc_selftest(int *state, double *err);
  * call copies them to and from the device.                                   */
 RADB200_API int radb200_field(const RadB200Geom *g, const double *pts, int64_t npts,
                   int what, int precision, double *out);
+/* No counterpart in the reference: field evaluation for callers that cannot
+ * allocate device memory (code running while another part of the process
+ * captures a CUDA graph, real-time loops that must stay off the allocator,
+ * hosts that hand the library fixed device arenas).  EVERY array is in device
+ * memory: the pointer fields of *g, pts and out; the struct itself and its
+ * counts are on the host.  FP64, face-by-face polyhedron form.  The call
+ * allocates nothing: its only scratch is a static 3 MiB device array that
+ * every GPU loading the library keeps until exit (its address is looked up
+ * on the first call on each device; make that first call outside any stream
+ * capture).  At most 16,384 points per call; larger counts are rejected with
+ * RADB200_E_ARG.  Calls that overlap on the GPU share the scratch and race:
+ * serialize them.  Synchronizes stream 0 before returning.                   */
+RADB200_API int radb200_field_noalloc(const RadB200Geom *g, const double *d_pts, int64_t npts,
+                                      int what, double *d_out);
 /* Same, with pts/out already in device memory (cudaStream 0 ordering).      */
 RADB200_API int radb200_field_dev(const RadB200Geom *g, const double *d_pts, int64_t npts,
                       int what, int precision, double *d_out);
