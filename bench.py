@@ -233,6 +233,51 @@ def run_ours(args, rank, world):
     return res
 
 
+def adjoint_ratio(reps=3):
+    """Second half of the metric: wall time of one full adjoint gradient over
+    one forward solve, through radiacuda_b200.adjoint.FieldProblem (the public
+    API: host parameters in, host field / gradients out), on
+      planar undulator: 2 x 40 blocks 50x10x5 mm, anisotropic MatLin, 2x2x2
+        subdivision (640 elements), B at 4,000 on-axis points, FP64 direct solve;
+      hybrid undulator: 80 NdFeB blocks + 80 saturating iron poles (4x4x4),
+        about 6,000 elements, mirror plane (2 images), B at 1e5 points,
+        Newton-Krylov relaxation.
+    Forward = assembly + solve + field; adjoint = field VJP + transposed solve
+    + derivative contractions.  Median of `reps` after one warm-up."""
+    import torch
+
+    from radiacuda_b200 import adjoint as A
+    from radiacuda_b200 import rad
+    import models as MD
+
+    out = {}
+    cases = [("undulator_640", lambda: MD.undulator(rad, nper_row=40, div=2)[0], MD.undulator_points(4000, 40)),
+             ("hybrid_6k", lambda: MD.hybrid_undulator(rad)[0], MD.hybrid_points(100_000))]
+    for name, build, pts in cases:
+        h = build()
+        prob = A.FieldProblem(h, pts, "b", prec=1e-12)
+        W = np.random.default_rng(1).normal(size=pts.shape)
+        tf, tb = [], []
+        for r in range(reps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            prob.forward()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            prob.backward(W)
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            if r:
+                tf.append(t1 - t0)
+                tb.append(t2 - t1)
+        f, b = float(np.median(tf)), float(np.median(tb))
+        out[name] = {"n_elements": int(prob.n), "n_points": int(pts.shape[0]), "forward_s": round(f, 4),
+                     "adjoint_s": round(b, 4), "adjoint_over_forward": round(b / f, 3),
+                     "adjoint_residual": float(prob.last_status["adjoint"][0]),
+                     "adjoint_iterations": int(prob.last_status["adjoint"][1])}
+    return out
+
+
 # FP64 operations of one triangular face term of radTPolygon::B_comp as
 # restated in csrc/formulas.cuh, counting an add/mul/compare as 1, an FMA as
 # 2 and each elementary function by the cost of a standard implementation:
@@ -334,6 +379,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     res = run_ours(args, rank, world)
+    if not args.profile:
+        res["adjoint"] = adjoint_ratio()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = reference_sample()
         res["cpu_baseline"] = cb if cb is not None else {"value": None, "unavailable": "oracle/_ref missing"}

@@ -232,23 +232,34 @@ RADB200_API int radb200_direct_solve(int64_t handle, int mode, double rtol, int 
 RADB200_API int radb200_adjoint_solve(int64_t handle, const double *dLdM, double rtol,
                           int max_iter, double *lambda_out, double *status);
 
-/* Sensitivities of a scalar loss L(M) through the converged relaxation, with
- * respect to the per-element remanence Mr [3N] (dL/dMr = D_r^T lambda, where
- * D_r = dM/dMr = I for every law here), and the centre of each RECTANGULAR
- * element (dL/dc [3N], from lambda^T (dN/dc) M recomputed on the fly by
- * differentiating the block formulas; images included).                      */
-RADB200_API int radb200_adjoint_grad(int64_t handle, const double *lambda,
-                         double *dL_dMr, double *dL_dc);
+/* Sensitivities of a scalar loss through the converged solve, given lambda
+ * from radb200_adjoint_solve.  Every output is per element, may be NULL:
+ *   dL_dMr  [3N]  w.r.t. the remanence Mr of each element's material (element
+ *                 frame) with the susceptibility tensor held fixed: lambda;
+ *   dL_dchi [9N]  w.r.t. the 3x3 susceptibility tensor of linear elements,
+ *                 lambda_e H_e^T (H at the converged state); chaining it
+ *                 through chi(Mr) = chi_perp I + (chi_par - chi_perp) L L^T,
+ *                 L = Mr/|Mr| (radmater.h:292-303) gives the easy-axis term;
+ *   dL_dc   [3N]  w.r.t. the centre of each RECTANGULAR element (object
+ *                 frame of the element), from lambda^T D (dN/dc) M + the
+ *                 gradient of H_ext at the centres; zero for polyhedra;
+ *   dL_dd   [3N]  w.r.t. the dimensions (full widths) of each rectangular
+ *                 element, from lambda^T D (dN/dd) M; zero for polyhedra.
+ * dN/dc and dN/dd are the analytic derivatives of the cuboid tensor,
+ * recomputed pair by pair (images included), never stored.  Terms of the
+ * loss that depend on the parameters directly (a field loss at fixed points)
+ * come from radb200_field_vjp and are added by the caller.                   */
+RADB200_API int radb200_adjoint_grad(int64_t handle, const double *lambda, double *dL_dMr, double *dL_dchi,
+                                     double *dL_dc, double *dL_dd);
 
-/* Field-operator part of the adjoint: for a loss on field values at points,
- * given W = dL/dF [npts*3] (F = B or H at pts), returns
- *   g_M [3N]  = (dF/dM)^T W       (the field operator's transpose applied to W)
- *   g_c [3N]  = d(W.F)/dc_e       (rectangular element centres, M held fixed)
- * evaluated for the current magnetization M [3N] of the relaxable elements
- * of this interaction.                                                       */
-RADB200_API int radb200_field_vjp(int64_t handle, const double *M, const double *pts,
-                      int64_t npts, int what, const double *W,
-                      double *g_M, double *g_c);
+/* Field-operator part of the adjoint.  F = B (what 0) or H (what 1) at pts
+ * [npts*3] from the relaxable elements of this interaction magnetized by M
+ * [3N] (element frames).  Given W = dL/dF [npts*3], returns (any may be NULL)
+ *   g_M [3N]  = (dF/dM)^T W;
+ *   g_c [3N]  = d(W.F)/d(centre) of each rectangular element, M fixed;
+ *   g_d [3N]  = d(W.F)/d(dimensions) of each rectangular element, M fixed.  */
+RADB200_API int radb200_field_vjp(int64_t handle, const double *M, const double *pts, int64_t npts, int what,
+                                  const double *W, double *g_M, double *g_c, double *g_d);
 
 #ifdef __cplusplus
 }

@@ -42,8 +42,8 @@ def lib():
         L.radb200_relax.argtypes = [_i64, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, _dp, _dp, _dp]
         L.radb200_direct_solve.argtypes = [_i64, C.c_int, C.c_double, C.c_int, _dp, _dp]
         L.radb200_adjoint_solve.argtypes = [_i64, _dp, C.c_double, C.c_int, _dp, _dp]
-        L.radb200_adjoint_grad.argtypes = [_i64, _dp, _dp, _dp]
-        L.radb200_field_vjp.argtypes = [_i64, _dp, _dp, _i64, C.c_int, _dp, _dp, _dp]
+        L.radb200_adjoint_grad.argtypes = [_i64, _dp, _dp, _dp, _dp, _dp]
+        L.radb200_field_vjp.argtypes = [_i64, _dp, _dp, _i64, C.c_int, _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -138,19 +138,21 @@ class NativeInteraction:
               "radb200_adjoint_solve")
         return lam, st
 
-    def adjoint_grad(self, lam: np.ndarray):
+    def adjoint_grad(self, lam: np.ndarray, want=("Mr", "chi", "c", "d")):
+        """Per-element sensitivities through the converged solve (radb200_adjoint_grad)."""
         lam = np.ascontiguousarray(lam, dtype=np.float64)
-        gMr = np.zeros(3 * self.n)
-        gc = np.zeros(3 * self.n)
-        check(lib().radb200_adjoint_grad(self.handle, _p(lam), _p(gMr), _p(gc)), "radb200_adjoint_grad")
-        return gMr, gc
+        out = {k: np.zeros(9 * self.n if k == "chi" else 3 * self.n) for k in want}
+        check(lib().radb200_adjoint_grad(self.handle, _p(lam), *[(_p(out[k]) if k in out else None)
+                                                                  for k in ("Mr", "chi", "c", "d")]),
+              "radb200_adjoint_grad")
+        return out
 
     def field_vjp(self, M: np.ndarray, pts: np.ndarray, what: int, W: np.ndarray):
+        """(dF/dM)^T W and the centre / dimension gradients of W.F at fixed M."""
         M = np.ascontiguousarray(M, dtype=np.float64)
         P = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
         W = np.ascontiguousarray(W, dtype=np.float64).reshape(-1, 3)
-        gM = np.zeros(3 * self.n)
-        gc = np.zeros(3 * self.n)
-        check(lib().radb200_field_vjp(self.handle, _p(M), _p(P), P.shape[0], what, _p(W), _p(gM), _p(gc)),
+        gM, gc, gd = np.zeros(3 * self.n), np.zeros(3 * self.n), np.zeros(3 * self.n)
+        check(lib().radb200_field_vjp(self.handle, _p(M), _p(P), P.shape[0], what, _p(W), _p(gM), _p(gc), _p(gd)),
               "radb200_field_vjp")
-        return gM, gc
+        return gM, gc, gd

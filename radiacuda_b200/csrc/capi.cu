@@ -310,8 +310,9 @@ int relax_newton(Intrc &I, double prec, int max_iter, double *status);
 int relax_reset(Intrc &I);
 int direct_solve(Intrc &I, int mode, double rtol, int max_iter, double *status);
 int adjoint_solve(Intrc &I, const double *dLdM, double rtol, int max_iter, double *lambda, double *status);
-int adjoint_grad(Intrc &I, const double *lambda, double *dMr, double *dc);
-int field_vjp(Intrc &I, const double *M, const double *pts, int64_t npts, int what, const double *W, double *gM, double *gc);
+int adjoint_grad(Intrc &I, const double *lambda, double *dMr, double *dchi, double *dc, double *dd);
+int field_vjp(Intrc &I, const double *M, const double *pts, int64_t npts, int what, const double *W, double *gM, double *gc,
+              double *gd);
 
 }  // namespace rb
 
@@ -378,6 +379,8 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   I->fast = fast;
   // observation points and row transforms from each element's main image
   std::vector<double> obs(3 * (size_t)n), rowT(9 * (size_t)n);
+  I->h_obsJ.assign(9 * (size_t)n, 0.0);
+  I->h_elem_src.assign(r->elem_src, r->elem_src + 2 * (size_t)n);
   for (int e = 0; e < n; e++) {
     int k = r->elem_src[2 * e], idx = r->elem_src[2 * e + 1];
     int t0;
@@ -388,7 +391,10 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
     double s = T[21];
     for (int a = 0; a < 3; a++) {
       obs[3 * e + a] = (T[12 + 3 * a] * c[0] + T[13 + 3 * a] * c[1] + T[14 + 3 * a] * c[2]) / s + T[9 + a];
-      for (int b = 0; b < 3; b++) rowT[9 * e + 3 * a + b] = s * T[3 * a + b];
+      for (int b = 0; b < 3; b++) {
+        rowT[9 * e + 3 * a + b] = s * T[3 * a + b];
+        I->h_obsJ[9 * e + 3 * a + b] = T[12 + 3 * a + b] / s;
+      }
     }
   }
   RB_TRY(I->obs.upload(obs.data(), obs.size() * sizeof(double)));
@@ -410,8 +416,9 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   RB_TRY(I->hext.alloc(vb));
   RB_CUDA(cudaMemset(I->hext.p, 0, vb));
   if (ext && (ext->n_rec + ext->n_poly + ext->n_arc + ext->n_bkg) > 0) {
-    DevGeom xg;
+    DevGeom &xg = I->xgeom;
     RB_TRY(xg.upload(ext));
+    I->has_ext = 1;
     DBuf tmp, scratch;
     RB_TRY(tmp.alloc(3 * (size_t)n * sizeof(double)));
     RB_TRY(launch_field(xg.view(fast), I->obs.as<double>(), n, 1, 0, tmp.as<double>(), scratch, 0));
@@ -526,25 +533,28 @@ int radb200_adjoint_solve(int64_t handle, const double *dLdM, double rtol, int m
 {
   Intrc *I = find_intrc(handle);
   if (!I) return RADB200_E_HANDLE;
-  if (!dLdM || !lambda_out || !status) { set_error("bad adjoint arguments"); return RADB200_E_ARG; }
+  if (!dLdM || !lambda_out || !status || !(rtol > 0) || max_iter < 1) { set_error("bad adjoint arguments"); return RADB200_E_ARG; }
+  if (I->last_kind < 0) { set_error("adjoint: no converged solve on this interaction"); return RADB200_E_ARG; }
   return adjoint_solve(*I, dLdM, rtol, max_iter, lambda_out, status);
 }
 
-int radb200_adjoint_grad(int64_t handle, const double *lambda, double *dL_dMr, double *dL_dc)
+int radb200_adjoint_grad(int64_t handle, const double *lambda, double *dL_dMr, double *dL_dchi, double *dL_dc,
+                         double *dL_dd)
 {
   Intrc *I = find_intrc(handle);
   if (!I) return RADB200_E_HANDLE;
   if (!lambda) { set_error("bad adjoint arguments"); return RADB200_E_ARG; }
-  return adjoint_grad(*I, lambda, dL_dMr, dL_dc);
+  if (I->last_kind < 0) { set_error("adjoint: no converged solve on this interaction"); return RADB200_E_ARG; }
+  return adjoint_grad(*I, lambda, dL_dMr, dL_dchi, dL_dc, dL_dd);
 }
 
 int radb200_field_vjp(int64_t handle, const double *M, const double *pts, int64_t npts, int what, const double *W,
-                      double *g_M, double *g_c)
+                      double *g_M, double *g_c, double *g_d)
 {
   Intrc *I = find_intrc(handle);
   if (!I) return RADB200_E_HANDLE;
   if (!M || !pts || !W || npts < 0 || what < 0 || what > 1) { set_error("bad field_vjp arguments"); return RADB200_E_ARG; }
-  return field_vjp(*I, M, pts, npts, what, W, g_M, g_c);
+  return field_vjp(*I, M, pts, npts, what, W, g_M, g_c, g_d);
 }
 
 }  // extern "C"

@@ -129,6 +129,12 @@ struct Intrc {
   int lu_mode = -1;                   // factors valid for this mode (-1 none)
   DBuf lastM, lastH;                  // converged state of the last solve
   int last_kind = -1;                 // 0 relax, 1 direct
+  // adjoint: external sources (kept for the gradient of H_ext at the centres),
+  // element kinds and d(obs_e)/d(centre_e) of each element's main image
+  DevGeom xgeom;
+  int has_ext = 0;
+  std::vector<int> h_elem_src;        // [2n]
+  std::vector<double> h_obsJ;         // [9n] row-major
 };
 
 // ---- small vector helpers (relax.cu) ---------------------------------------

@@ -61,6 +61,9 @@ int gmres(Op &op, int n3, int ld, const double *b, double *x, double rtol, int m
   DBuf Vb, wb, rb_;
   RB_TRY(Vb.alloc((size_t)(restart + 1) * ld * sizeof(double)));
   RB_TRY(wb.alloc((size_t)2 * ld * sizeof(double)));
+  // the matvec reads whole padded rows (ld), so the padding must hold zeros
+  RB_CUDA(cudaMemset(Vb.p, 0, (size_t)(restart + 1) * ld * sizeof(double)));
+  RB_CUDA(cudaMemset(wb.p, 0, (size_t)2 * ld * sizeof(double)));
   std::vector<double *> V(restart + 1);
   for (int k = 0; k <= restart; k++) V[k] = Vb.as<double>() + (size_t)k * ld;
   double *w = wb.as<double>(), *z = w + ld;

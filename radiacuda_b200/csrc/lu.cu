@@ -254,6 +254,66 @@ __global__ void __launch_bounds__(256) panel_gemv_kernel(const T *__restrict__ A
   if (lane == 0) x[row] -= s;
 }
 
+// ---- transposed solves, A^T = U^T L^T (adjoint) ----
+// x[k0:k0+nb] <- Inv_k^T x[k0:k0+nb]
+template <typename T>
+__global__ void __launch_bounds__(LU_NB) block_matvec_t_kernel(const T *__restrict__ Inv, int k0, int nb, double *__restrict__ x)
+{
+  __shared__ double xs[LU_NB];
+  int r = threadIdx.x;
+  if (r < nb) xs[r] = x[k0 + r];
+  __syncthreads();
+  if (r < nb) {
+    double s = 0.0;
+    for (int j = 0; j < nb; j++) s += (double)Inv[(size_t)(k0 + j) * LU_NB + r] * xs[j];
+    x[k0 + r] = s;
+  }
+}
+
+// x[c0..c1) -= A[k0:k0+nb, c0..c1)^T x[k0:k0+nb] (thread per column, coalesced rows)
+template <typename T>
+__global__ void __launch_bounds__(256) panel_gemv_t_kernel(const T *__restrict__ A, int ld, int k0, int nb, int c0, int c1,
+                                                           double *__restrict__ x)
+{
+  __shared__ double xs[LU_NB];
+  for (int r = threadIdx.x; r < nb; r += blockDim.x) xs[r] = x[k0 + r];
+  __syncthreads();
+  int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= c1) return;
+  const T *a = A + (size_t)k0 * ld + c;
+  double s = 0.0;
+  for (int r = 0; r < nb; r++) s += (double)a[(size_t)r * ld] * xs[r];
+  x[c] -= s;
+}
+
+template <typename T>
+static int lu_solve_t(const T *A, const T *Linv, const T *Uinv, int n3, int ld, double *x, cudaStream_t st)
+{
+  // U^T y = x, forward over the block rows of U
+  for (int k0 = 0; k0 < n3; k0 += LU_NB) {
+    int nb = std::min(LU_NB, n3 - k0);
+    block_matvec_t_kernel<T><<<1, LU_NB, 0, st>>>(Uinv, k0, nb, x);
+    RB_TRY(check_launch("block_matvec_t_kernel"));
+    int rest = k0 + nb;
+    if (rest < n3) {
+      panel_gemv_t_kernel<T><<<(n3 - rest + 255) / 256, 256, 0, st>>>(A, ld, k0, nb, rest, n3, x);
+      RB_TRY(check_launch("panel_gemv_t_kernel"));
+    }
+  }
+  // L^T z = y, backward over the block rows of L
+  int last = ((n3 - 1) / LU_NB) * LU_NB;
+  for (int k0 = last; k0 >= 0; k0 -= LU_NB) {
+    int nb = std::min(LU_NB, n3 - k0);
+    block_matvec_t_kernel<T><<<1, LU_NB, 0, st>>>(Linv, k0, nb, x);
+    RB_TRY(check_launch("block_matvec_t_kernel"));
+    if (k0 > 0) {
+      panel_gemv_t_kernel<T><<<(k0 + 255) / 256, 256, 0, st>>>(A, ld, k0, nb, 0, k0, x);
+      RB_TRY(check_launch("panel_gemv_t_kernel"));
+    }
+  }
+  return 0;
+}
+
 template <typename T>
 static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaStream_t st, int *tc_used)
 {
@@ -332,6 +392,19 @@ int lu_precond(Intrc &I, double *x, cudaStream_t st)
                             I.ld, x, st);
   return lu_solve<float>(I.LU32.as<float>(), I.LUinv.as<float>(), I.LUinv.as<float>() + (size_t)I.n3 * LU_NB, I.n3, I.ld,
                          x, st);
+}
+
+// x <- A^-T x with the kept factors (the adjoint's preconditioner)
+int lu_precond_transposed(Intrc &I, double *x, cudaStream_t st)
+{
+  if (I.lu_mode == RADB200_LU_F64)
+    return lu_solve_t<double>(I.LU64.as<double>(), I.LUinv.as<double>(), I.LUinv.as<double>() + (size_t)I.n3 * LU_NB, I.n3,
+                              I.ld, x, st);
+  if (I.lu_mode == RADB200_LU_TF32)
+    return lu_solve_t<float>(I.LU32.as<float>(), I.LUinv.as<float>(), I.LUinv.as<float>() + (size_t)I.n3 * LU_NB, I.n3,
+                             I.ld, x, st);
+  set_error("no LU factors on this interaction");
+  return RADB200_E_ARG;
 }
 
 struct LinOp : Op {

@@ -216,6 +216,75 @@ def undulator_points(n=4000, nper_row=40):
 
 
 # ---------------------------------------------------------------------------
+# hybrid undulator: NdFeB blocks (magnetized along +-z) alternating with
+# saturating iron poles along z, upper half modelled, the lower half by the
+# mirror plane y = 0 (2 images per element)
+# ---------------------------------------------------------------------------
+HYB_POLE = (40.0, 20.0, 4.0)    # x, y, z widths of a pole
+HYB_BLOCK = (50.0, 25.0, 6.0)   # of a block; period = 2 (pole + block) = 20 mm
+
+
+def hybrid_undulator(R, n_pairs=80, pole_div=(4, 4, 4), block_div=(2, 2, 3), gap=10.0, mr=1.25, seed=6,
+                     pole_dz=None, block_mr=None):
+    """n_pairs blocks alternating with n_pairs poles.  pole_dz[k] changes the
+    z width of pole k (centre fixed); block_mr[k] replaces block k's remanence
+    vector.  Returns (model, pole handles, block handles, pole centres)."""
+    reset(R)
+    rng = np.random.default_rng(seed)
+    pz, bz = HYB_POLE[2], HYB_BLOCK[2]
+    step = pz + bz
+    z0 = -0.5 * n_pairs * step
+    poles, blocks, pc = [], [], []
+    for k in range(n_pairs):
+        zp = z0 + k * step + 0.5 * pz
+        zb = zp + 0.5 * (pz + bz)
+        dz = pz + (0.0 if pole_dz is None else pole_dz[k])
+        p = R.ObjRecMag([0.0, 0.5 * gap + 0.5 * HYB_POLE[1], zp], [HYB_POLE[0], HYB_POLE[1], dz], [0, 0, 0])
+        if pole_div != (1, 1, 1):
+            R.ObjDivMag(p, list(pole_div))
+        poles.append(p)
+        pc.append([0.0, 0.5 * gap + 0.5 * HYB_POLE[1], zp])
+        if block_mr is not None:
+            m = np.asarray(block_mr[k], float)
+        else:
+            m = np.array([0.0, 0.0, mr * (1 if k % 2 == 0 else -1)]) * (1.0 + 0.01 * rng.uniform(-1, 1))
+        b = R.ObjRecMag([0.0, 0.5 * gap + 0.5 + 0.5 * HYB_BLOCK[1], zb], list(HYB_BLOCK), m.tolist())
+        R.MatApl(b, R.MatLin([0.05, 0.15], m.tolist()))
+        if block_div != (1, 1, 1):
+            R.ObjDivMag(b, list(block_div))
+        blocks.append(b)
+    gp = R.ObjCnt(poles)
+    R.MatApl(gp, R.MatSatIsoFrm([2000, 1.5], [100, 0.4], [10, 0.2]))
+    g = R.ObjCnt([gp] + blocks)
+    R.TrfZerPara(g, [0, 0, 0], [0, 1, 0])
+    return g, poles, blocks, np.array(pc)
+
+
+def hybrid_points(n=100_000, n_pairs=80, seed=9):
+    """Points in the gap over the length of the device (off every face plane)."""
+    rng = np.random.default_rng(seed)
+    L = n_pairs * (HYB_POLE[2] + HYB_BLOCK[2])
+    return np.stack([rng.uniform(-15, 15, n) + 0.0137, rng.uniform(-4, 4, n) + 0.0071,
+                     rng.uniform(-0.5 * L, 0.5 * L, n) + 0.0517], axis=1)
+
+
+# ---------------------------------------------------------------------------
+# small models for the adjoint tests: linear anisotropic blocks with images,
+# a rotated block, a coil and a background field; and a small hybrid
+# ---------------------------------------------------------------------------
+def adjoint_linear(R):
+    g = sym_blocks(R, div=2)
+    coil = R.ObjRaceTrk([20.0, 20.0, 25.0], [3, 9], [10, 14], 6, 4, 2.0, "man", "z")
+    bk = R.ObjBckg([0.05, -0.02, 0.1])
+    return R.ObjCnt([g, coil, bk])
+
+
+def adjoint_points(n=160, seed=31):
+    rng = np.random.default_rng(seed)
+    return rng.uniform([-45, -15, -25], [45, 55, 25], size=(n, 3)) + np.array([0.0137, 0.0071, 0.0053])
+
+
+# ---------------------------------------------------------------------------
 # mixed cuboids + tetrahedra with a symmetry, saturating material and a coil
 # ---------------------------------------------------------------------------
 def mixed_sym(R, seed=3):
