@@ -225,3 +225,73 @@ def test_autograd_undulator_block_gradients_match_central_differences(cuda, rad)
                 got = float((mr_blk.grad if which == "mr" else dc_blk.grad)[b, a])
                 scale = float((mr_blk.grad if which == "mr" else dc_blk.grad).abs().max())
                 assert abs(got - fd) <= 1e-5 * scale, (which, b, a, got, fd)
+
+
+# ---------------------------------------------------------------------------
+# pinned to the reference: finite differences of the reference CPU Radia
+# (tests/golden/adjoint_fd.json, made by tests/golden/make_adjoint_golden.py)
+# ---------------------------------------------------------------------------
+def _golden_fd():
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "adjoint_fd.json")) as f:
+        return json.load(f)
+
+
+def block_gradients(pack, blocks, rad, g):
+    """Per-block d/dMr (through M and the easy-axis chi(Mr), radmater.h:292-303)
+    and d/dcentre from per-element gradients g (dict Mr, chi, c)."""
+    leaf_block = {}
+    for b, hb in enumerate(blocks):
+        for lf in model.collect_leaves(rad._objs, hb):
+            leaf_block[lf.handle] = b
+    nb = len(blocks)
+    gmr, gc = np.zeros((nb, 3)), np.zeros((nb, 3))
+    for e, lf in enumerate(pack.leaves):
+        b = leaf_block[lf.handle]
+        mr = pack.mat[e, 9:12]
+        kpar, kperp = lf.obj.mat.ksi
+        amr = np.linalg.norm(mr)
+        L = mr / amr
+        dL = (np.eye(3) - np.outer(L, L)) / amr  # column a: dL/dmr_a
+        gchi = g["chi"][9 * e:9 * e + 9].reshape(3, 3)
+        for a in range(3):
+            dchi = (kpar - kperp) * (np.outer(dL[:, a], L) + np.outer(L, dL[:, a]))
+            gmr[b, a] += g["Mr"][3 * e + a] + np.sum(gchi * dchi)
+        gc[b] += g["c"][3 * e:3 * e + 3]
+    return gmr, gc
+
+
+def _check_against_golden(G, gmr, gc):
+    for kind, got in (("mr", gmr), ("c", gc)):
+        ref = G["grad_" + kind]
+        scale = max(abs(v) for v in ref.values())
+        for key, v in ref.items():
+            b, a = map(int, key.split(","))
+            assert abs(got[b, a] - v) <= 5e-5 * scale, (kind, key, got[b, a], v)
+
+
+def test_oracle_adjoint_matches_reference_finite_differences(rad):
+    G = _golden_fd()
+    h, blocks = MD.undulator(rad, nper_row=G["nper_row"], div=G["div"])
+    pack = _pack(rad, h)
+    pts = MD.undulator_points(n=G["n_points"], nper_row=G["nper_row"])
+    W = np.random.default_rng(G["w_seed"]).normal(size=pts.shape)
+    M, L = oracle_forward(pack, pts, W)
+    assert abs(L - G["loss"]) <= 1e-6 * abs(G["loss"])
+    _check_against_golden(G, *block_gradients(pack, blocks, rad, AO.gradients(pack, M, pts, W)))
+
+
+@pytest.mark.gpu
+def test_device_adjoint_matches_reference_finite_differences(cuda, rad):
+    from radiacuda_b200 import adjoint as A
+    G = _golden_fd()
+    h, blocks = MD.undulator(rad, nper_row=G["nper_row"], div=G["div"])
+    pts = MD.undulator_points(n=G["n_points"], nper_row=G["nper_row"])
+    W = np.random.default_rng(G["w_seed"]).normal(size=pts.shape)
+    prob = A.FieldProblem(h, pts, "b")
+    L = float(np.sum(prob.forward() * W))
+    assert abs(L - G["loss"]) <= 1e-6 * abs(G["loss"])
+    g = prob.backward(W)
+    ge = dict(Mr=g["mr"].reshape(-1), chi=g["chi"].reshape(-1), c=g["centre"].reshape(-1))
+    _check_against_golden(G, *block_gradients(prob.pack, blocks, rad, ge))
