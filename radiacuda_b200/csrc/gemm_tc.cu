@@ -2,16 +2,16 @@
 // of the blocked LU:   C[m x n] -= A[m x k] * B[k x n],   k <= 128,
 // all FP32 row-major inside the LU matrix (leading dimension ld).
 //
-// One CTA (4 warps) owns a 128 x 256 tile of C:
-//   1. warp 0 allocates 256 TMEM columns (128 lanes x 256 FP32 accumulators);
-//   2. the CTA stages A (128 x k) and B (k x 256) in shared memory in the
-//      canonical no-swizzle UMMA layouts (8-row x 16-byte core matrices),
-//      rounding FP32 -> TF32 (round-to-nearest) on the way;
-//   3. one elected thread issues k/8 tcgen05.mma.kind::tf32 (M=128, N=256,
-//      K=8) and commits them to an mbarrier;
-//   4. every warp reads its 32 TMEM lanes with tcgen05.ld, stages the tile in
-//      shared memory, and the CTA subtracts it from C with coalesced 16-byte
-//      loads / stores.
+// Persistent CTAs of 8 warps loop over 128 x 256 tiles of C (one CTA per SM,
+// 192 KB of staged operands):
+//   1. cp.async brings A (128 x k) and B^T (256 x k) into shared memory in the
+//      canonical no-swizzle UMMA layouts (8-row x 16-byte core matrices) with
+//      many copies in flight; each thread then rounds its own chunks to TF32
+//      (round to nearest);
+//   2. one elected thread issues k/8 tcgen05.mma.kind::tf32 (M=128, N=256,
+//      K=8) into 256 TMEM columns and commits them to an mbarrier, while every
+//      thread loads the 128 C values of its row segment;
+//   3. each thread reads its accumulators with tcgen05.ld and stores C - AB.
 // Waits on the mbarrier are bounded: on timeout the CTA raises an error flag,
 // still frees its TMEM and returns (the host then falls back to the CUDA-core
 // GEMM and reports the error).
@@ -19,9 +19,10 @@
 // Layouts (byte offsets inside the A / B staging buffers):
 //   A, K-major:  (r/8)*4096 + (k/4)*128 + (r%8)*16 + (k%4)*4
 //                descriptor of MMA step s: start A + 256 s, LBO 128, SBO 4096
-//   B, N-major:  (k/8)*8192 + (n/4)*128 + (k%8)*16 + (n%4)*4
-//                descriptor of MMA step s: start B + 8192 s, SBO 128, LBO 8192
-//   B, K-major (alternative): (n/8)*4096 + (k/4)*128 + (n%8)*16 + (k%4)*4
+//   B^T, K-major: (n/8)*4096 + (k/4)*128 + (n%8)*16 + (k%4)*4, same descriptors
+//   (B arrives row-major k x n and is transposed to n x 128 in global memory
+//   first: the k*n*8 bytes of the transpose are small against the m*n*8 of C;
+//   the MMA reads tf32 operands K-major only)
 // The first use runs a self-test against the CUDA-core GEMM and keeps the
 // tensor-core path only if it agrees to TF32 accuracy.
 #include <math.h>
@@ -34,7 +35,7 @@
 namespace rb {
 
 constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 128;
-constexpr int TC_THREADS = 128;
+constexpr int TC_THREADS = 256;
 constexpr int TC_SMEM_A = TC_BM * TC_BK * 4;   // 64 KB
 constexpr int TC_SMEM_B = TC_BK * TC_BN * 4;   // 128 KB
 constexpr int TC_SMEM = TC_SMEM_A + TC_SMEM_B + 1024;
@@ -70,12 +71,17 @@ __host__ __device__ constexpr uint32_t umma_idesc(int b_mn_major)
          ((uint32_t)(TC_BM >> 4) << 24);
 }
 
-// overwrite == 0: C -= A B;  overwrite == 1: C = A B (C may alias the rows of A
-// this CTA reads when n <= 256, or the columns of B it reads when m <= 128:
-// operands are fully staged before the first store).
-template <int B_MN>
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *C, int ldc, int m, int n, int k,
-                                                                  const float *A, int lda, const float *B, int ldb,
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
+// overwrite == 0: C -= A B;  overwrite == 1: C = A B.  C must not alias A or B.
+// Bt = B^T (n x ldbt, K contiguous).  Persistent: CTA b handles tiles b,
+// b + gridDim.x, ... (n-tiles fastest, so neighbouring CTAs share A rows in L2).
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restrict__ C, int ldc, int m, int n, int k,
+                                                                  const float *__restrict__ A, int lda,
+                                                                  const float *__restrict__ Bt, int ldbt,
                                                                   int *__restrict__ err, int overwrite)
 {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -85,15 +91,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *C, int 
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_base_s;
   __shared__ int timed_out;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int row0 = blockIdx.y * TC_BM, col0 = blockIdx.x * TC_BN;
-  // once any CTA of this launch (or an earlier one) has timed out, the rest
-  // return at once instead of each spending its own wait limit (the decision
-  // is taken by one thread so the whole CTA leaves together)
   __shared__ int abort_cta;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles_n = (n + TC_BN - 1) / TC_BN, tiles_m = (m + TC_BM - 1) / TC_BM;
+  const int ntiles = tiles_n * tiles_m;
+  // once any CTA of this launch (or an earlier one) has timed out, the rest
+  // return at once (decided by one thread so the whole CTA leaves together)
   if (tid == 0) abort_cta = *(volatile int *)err;
   __syncthreads();
-  if (abort_cta != 0) return;
+  if (abort_cta != 0 || (int)blockIdx.x >= ntiles) return;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)), "r"(TC_BN));
@@ -104,156 +110,150 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *C, int 
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     timed_out = 0;
   }
-  const int ksteps = (k + 7) / 8;
-  const int kpad = ksteps * 8;
-
-  // ---- stage A: rows row0.., k columns; lanes -> (r%8, 4 consecutive k-chunks)
-  for (int it = tid; it < (TC_BM / 8) * (kpad / 4) * 8; it += TC_THREADS) {
-    int rr = it & 7;
-    int rest = it >> 3;
-    int kc = rest % (kpad / 4);
-    int rg = rest / (kpad / 4);
-    int r = rg * 8 + rr, kk = kc * 4;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    int gr = row0 + r;
-    if (gr < m) {
-      const float *src = A + (size_t)gr * lda + kk;
-      if (kk + 3 < k) v = *reinterpret_cast<const float4 *>(src);
-      else {
-        if (kk < k) v.x = src[0];
-        if (kk + 1 < k) v.y = src[1];
-        if (kk + 2 < k) v.z = src[2];
-      }
-    }
-    v.x = to_tf32(v.x); v.y = to_tf32(v.y); v.z = to_tf32(v.z); v.w = to_tf32(v.w);
-    *reinterpret_cast<float4 *>(sA + rg * 4096 + kc * 128 + rr * 16) = v;
-  }
-  // ---- stage B
-  if (B_MN) {
-    // lanes -> (k%8, 4 consecutive n-groups)
-    for (int it = tid; it < (kpad / 8) * (TC_BN / 4) * 8; it += TC_THREADS) {
-      int kr = it & 7;
-      int rest = it >> 3;
-      int ng = rest % (TC_BN / 4);
-      int kg = rest / (TC_BN / 4);
-      int kk = kg * 8 + kr, nn = ng * 4;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      int gc = col0 + nn;
-      if (kk < k) {
-        const float *src = B + (size_t)kk * ldb + gc;
-        if (gc + 3 < n) v = *reinterpret_cast<const float4 *>(src);
-        else {
-          if (gc < n) v.x = src[0];
-          if (gc + 1 < n) v.y = src[1];
-          if (gc + 2 < n) v.z = src[2];
-        }
-      }
-      v.x = to_tf32(v.x); v.y = to_tf32(v.y); v.z = to_tf32(v.z); v.w = to_tf32(v.w);
-      *reinterpret_cast<float4 *>(sB + kg * 8192 + ng * 128 + kr * 16) = v;
-    }
-  } else {
-    // K-major B (transposed gather): lanes -> (n%8, 4 consecutive k-chunks)
-    for (int it = tid; it < (TC_BN / 8) * (kpad / 4) * 8; it += TC_THREADS) {
-      int nr = it & 7;
-      int rest = it >> 3;
-      int kc = rest % (kpad / 4);
-      int ngp = rest / (kpad / 4);
-      int nn = ngp * 8 + nr, kk = kc * 4;
-      int gc = col0 + nn;
-      float vv[4];
-      for (int q = 0; q < 4; q++) vv[q] = (gc < n && kk + q < k) ? B[(size_t)(kk + q) * ldb + gc] : 0.f;
-      float4 v = make_float4(to_tf32(vv[0]), to_tf32(vv[1]), to_tf32(vv[2]), to_tf32(vv[3]));
-      *reinterpret_cast<float4 *>(sB + ngp * 4096 + kc * 128 + nr * 16) = v;
-    }
-  }
-  // make the generic-proxy smem writes visible to the tensor core (async proxy)
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base_s;
+  const int ksteps = (k + 7) / 8;
+  const int kpad = ksteps * 8;
+  const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+  const int na = (TC_BM / 8) * (kpad / 4) * 8;   // 16-byte chunks of A
+  const int nbb = (TC_BN / 8) * (kpad / 4) * 8;  // of B^T
+  uint32_t phase = 0;
 
-  if (tid == 0) {
-    const uint32_t idesc = umma_idesc(B_MN);
-    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-    for (int s = 0; s < ksteps; s++) {
-      uint64_t da = umma_desc(a0 + 256u * s, 128u, 4096u);
-      uint64_t db = B_MN ? umma_desc(b0 + 8192u * s, 8192u, 128u) : umma_desc(b0 + 256u * s, 128u, 4096u);
-      uint32_t acc = (s > 0) ? 1u : 0u;
-      asm volatile(
-          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-          "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-          "l"(da), "l"(db), "r"(idesc), "r"(acc));
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int row0 = (tile / tiles_n) * TC_BM, col0 = (tile % tiles_n) * TC_BN;
+    // ---- 1. stage A and B^T (K-major core matrices): lanes -> (row % 8, 4 consecutive k-chunks)
+    for (int it = tid; it < na; it += TC_THREADS) {
+      int rr = it & 7, rest = it >> 3;
+      int kc = rest % (kpad / 4), rg = rest / (kpad / 4);
+      int gr = row0 + rg * 8 + rr, kk = kc * 4;
+      uint32_t bytes = (gr < m && kk < k) ? (uint32_t)(min(4, k - kk) * 4) : 0u;
+      const float *src = bytes ? A + (size_t)gr * lda + kk : A;
+      cp_async16(a0 + rg * 4096 + kc * 128 + rr * 16, src, bytes);
     }
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&mbar))
-                 : "memory");
-  }
-  // ---- bounded wait for the MMAs (phase 0)
-  {
-    uint32_t done = 0;
-    long long spins = 0;
-    while (!done) {
-      asm volatile(
-          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-          : "=r"(done)
-          : "r"(smem_u32(&mbar)), "r"(0u)
-          : "memory");
-      if (!done && ++spins > TC_SPIN_LIMIT) {
-        timed_out = 1;
-        break;
+    for (int it = tid; it < nbb; it += TC_THREADS) {
+      int nr = it & 7, rest = it >> 3;
+      int kc = rest % (kpad / 4), ngp = rest / (kpad / 4);
+      int gc = col0 + ngp * 8 + nr, kk = kc * 4;
+      uint32_t bytes = (gc < n && kk < k) ? (uint32_t)(min(4, k - kk) * 4) : 0u;
+      const float *src = bytes ? Bt + (size_t)gc * ldbt + kk : Bt;
+      cp_async16(b0 + ngp * 4096 + kc * 128 + nr * 16, src, bytes);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    // round this thread's own chunks to TF32 (visible to it after wait_all)
+    for (int it = tid; it < na; it += TC_THREADS) {
+      int rr = it & 7, rest = it >> 3;
+      int kc = rest % (kpad / 4), rg = rest / (kpad / 4);
+      float4 *p = reinterpret_cast<float4 *>(sA + rg * 4096 + kc * 128 + rr * 16);
+      float4 v = *p;
+      *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
+    }
+    for (int it = tid; it < nbb; it += TC_THREADS) {
+      int nr = it & 7, rest = it >> 3;
+      int kc = rest % (kpad / 4), ngp = rest / (kpad / 4);
+      float4 *p = reinterpret_cast<float4 *>(sB + ngp * 4096 + kc * 128 + nr * 16);
+      float4 v = *p;
+      *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
+    }
+    // generic-proxy smem writes -> visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    // ---- 2. MMAs (one thread)
+    if (tid == 0) {
+      const uint32_t idesc = umma_idesc(0);
+      for (int s = 0; s < ksteps; s++) {
+        uint64_t da = umma_desc(a0 + 256u * s, 128u, 4096u);
+        uint64_t db = umma_desc(b0 + 256u * s, 128u, 4096u);
+        uint32_t acc = (s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(da), "l"(db), "r"(idesc), "r"(acc));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&mbar))
+                   : "memory");
+    }
+
+    // ---- meanwhile: this thread's C values (row r, 128 columns)
+    const int q = warp & 3, hc = warp >> 2;
+    const int r = q * 32 + lane;
+    const int gr = row0 + r, gcb = col0 + hc * 128;
+    float4 cv[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      int gc = gcb + 4 * j;
+      cv[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (!overwrite && gr < m) {
+        const float *src = C + (size_t)gr * ldc + gc;
+        if (gc + 3 < n) cv[j] = *reinterpret_cast<const float4 *>(src);
+        else if (gc < n) {
+          cv[j].x = src[0];
+          if (gc + 1 < n) cv[j].y = src[1];
+          if (gc + 2 < n) cv[j].z = src[2];
+        }
       }
     }
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (!timed_out) {
-    // ---- TMEM -> registers -> shared, reusing the A+B staging buffers
-    // (128 x 260 floats = 133,120 bytes <= 196,608; free once the MMAs completed)
-    float *stage = reinterpret_cast<float *>(sA);
-    const int SP = TC_BN + 4;  // padded row pitch (floats)
-    const int r = warp * 32 + lane;
-    for (int c = 0; c < TC_BN; c += 16) {
+
+    // ---- bounded wait for the MMAs of this tile
+    {
+      uint32_t done = 0;
+      long long spins = 0;
+      while (!done) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_u32(&mbar)), "r"(phase)
+            : "memory");
+        if (!done && ++spins > TC_SPIN_LIMIT) {
+          timed_out = 1;
+          break;
+        }
+      }
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (timed_out) break;
+
+    // ---- 3. epilogue: TMEM -> registers -> C (warp w: TMEM lanes 32 (w % 4), columns 128 (w / 4))
+#pragma unroll
+    for (int cb = 0; cb < 128; cb += 16) {
       uint32_t v[16];
-      uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
+      uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(hc * 128 + cb);
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
           : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
             "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      // the staging rows overlap B only after every warp's MMAs are complete (mbarrier above)
-      for (int q = 0; q < 16; q += 4)
-        *reinterpret_cast<float4 *>(stage + (size_t)r * SP + c + q) =
-            make_float4(__uint_as_float(v[q]), __uint_as_float(v[q + 1]), __uint_as_float(v[q + 2]), __uint_as_float(v[q + 3]));
-    }
-    __syncthreads();
-    // ---- C -= tile, coalesced along rows
-    for (int it = tid; it < TC_BM * (TC_BN / 4); it += TC_THREADS) {
-      int rr = it / (TC_BN / 4), c4 = (it % (TC_BN / 4)) * 4;
-      int gr = row0 + rr, gc = col0 + c4;
-      if (gr >= m) continue;
-      float4 t = *reinterpret_cast<const float4 *>(stage + (size_t)rr * SP + c4);
-      float *dst = C + (size_t)gr * ldc + gc;
-      if (overwrite) {
-        if (gc + 3 < n) *reinterpret_cast<float4 *>(dst) = t;
-        else {
-          if (gc < n) dst[0] = t.x;
-          if (gc + 1 < n) dst[1] = t.y;
-          if (gc + 2 < n) dst[2] = t.z;
+      if (gr < m) {
+#pragma unroll
+        for (int j4 = 0; j4 < 4; j4++) {
+          const int j = cb / 4 + j4;
+          const int gc = gcb + 4 * j;
+          float4 t = make_float4(__uint_as_float(v[4 * j4]), __uint_as_float(v[4 * j4 + 1]), __uint_as_float(v[4 * j4 + 2]),
+                                 __uint_as_float(v[4 * j4 + 3]));
+          float4 o = overwrite ? t : make_float4(cv[j].x - t.x, cv[j].y - t.y, cv[j].z - t.z, cv[j].w - t.w);
+          float *dst = C + (size_t)gr * ldc + gc;
+          if (gc + 3 < n) *reinterpret_cast<float4 *>(dst) = o;
+          else if (gc < n) {
+            dst[0] = o.x;
+            if (gc + 1 < n) dst[1] = o.y;
+            if (gc + 2 < n) dst[2] = o.z;
+          }
         }
-      } else if (gc + 3 < n) {
-        float4 o = *reinterpret_cast<float4 *>(dst);
-        o.x -= t.x; o.y -= t.y; o.z -= t.z; o.w -= t.w;
-        *reinterpret_cast<float4 *>(dst) = o;
-      } else {
-        if (gc < n) dst[0] -= t.x;
-        if (gc + 1 < n) dst[1] -= t.y;
-        if (gc + 2 < n) dst[2] -= t.z;
       }
     }
-  } else if (tid == 0) {
-    atomicExch(err, 2);
+    // TMEM reads and smem uses of this tile complete before the next tile's copies / MMAs
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
+  if (timed_out && tid == 0) atomicExch(err, 2);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
@@ -269,27 +269,54 @@ __global__ void tc_ref_kernel(float *C, int ld, int m, int n, int k, const float
   C[(size_t)r * ld + c] -= s;
 }
 
-static int g_tc_state = -1;   // -1 untested, 0 disabled, 1 N-major B, 2 K-major B
+static int g_tc_state = -1;   // -1 untested, 0 disabled, 1 enabled
 static double g_tc_err = -1.0;
 static DBuf g_tc_err_flag;
 
-static int launch_tc(int variant, float *C, int ldc, int m, int n, int k, const float *A, int lda, const float *B, int ldb,
-                     cudaStream_t st, int overwrite = 0)
+// Bt[c][r] = B[r][c] for r < k, c < n (32 x 32 tiles through shared memory)
+__global__ void tc_transpose_kernel(const float *__restrict__ B, int ldb, int k, int n, float *__restrict__ Bt, int ldbt)
 {
-  dim3 grid((n + TC_BN - 1) / TC_BN, (m + TC_BM - 1) / TC_BM);
-  if (grid.y > 65535) { set_error("tensor-core update grid too large"); return RADB200_E_ARG; }
-  if (variant == 1) {
-    RB_CUDA(cudaFuncSetAttribute(tc_update_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-    tc_update_kernel<1><<<grid, TC_THREADS, TC_SMEM, st>>>(C, ldc, m, n, k, A, lda, B, ldb, g_tc_err_flag.as<int>(), overwrite);
-  } else {
-    RB_CUDA(cudaFuncSetAttribute(tc_update_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-    tc_update_kernel<0><<<grid, TC_THREADS, TC_SMEM, st>>>(C, ldc, m, n, k, A, lda, B, ldb, g_tc_err_flag.as<int>(), overwrite);
+  __shared__ float t[32][33];
+  int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    int r = r0 + i, c = c0 + threadIdx.x;
+    if (r < k && c < n) t[i][threadIdx.x] = B[(size_t)r * ldb + c];
   }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    int c = c0 + i, r = r0 + threadIdx.x;
+    if (r < k && c < n) Bt[(size_t)c * ldbt + r] = t[threadIdx.x][i];
+  }
+}
+
+static DBuf g_tc_bt;   // B^T scratch, [n x TC_BK] floats
+
+// max_ctas > 0 caps the persistent grid (the self-test uses it to make every
+// CTA loop over several tiles)
+static int launch_tc(float *C, int ldc, int m, int n, int k, const float *A, int lda, const float *B, int ldb,
+                     cudaStream_t st, int overwrite = 0, int max_ctas = 0)
+{
+  long long tiles = (long long)((n + TC_BN - 1) / TC_BN) * ((m + TC_BM - 1) / TC_BM);
+  if (tiles > (1ll << 30) || k > TC_BK) { set_error("tensor-core update shape out of range"); return RADB200_E_ARG; }
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    RB_CUDA(cudaGetDevice(&dev));
+    RB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  }
+  RB_TRY(g_tc_bt.alloc((size_t)n * TC_BK * sizeof(float)));
+  tc_transpose_kernel<<<dim3((n + 31) / 32, (k + 31) / 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, g_tc_bt.as<float>(), TC_BK);
+  RB_TRY(check_launch("tc_transpose_kernel"));
+  int grid = (int)std::min<long long>(tiles, max_ctas > 0 ? max_ctas : nsm);
+  RB_CUDA(cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+  tc_update_kernel<<<grid, TC_THREADS, TC_SMEM, st>>>(C, ldc, m, n, k, A, lda, g_tc_bt.as<float>(), TC_BK,
+                                                      g_tc_err_flag.as<int>(), overwrite);
   return check_launch("tc_update_kernel");
 }
 
-// Runs both B layouts on a random 300 x 520 x 120 update (ragged on purpose)
-// and keeps the first that matches the CUDA-core reference.
+// Runs a random 300 x 400 x 120 update (ragged in m, n and k on purpose) on
+// 2 CTAs, so each CTA loops over 3 tiles, and keeps the tensor-core path only
+// if it matches the CUDA-core reference.
 static int tc_selftest()
 {
   const int m = 300, n = 520, k = 120, ld = 640;
@@ -311,10 +338,10 @@ static int tc_selftest()
   std::vector<float> cref((size_t)(m + k) * ld), ctc((size_t)(m + k) * ld);
   RB_CUDA(cudaMemcpy(cref.data(), ref.p, h.size() * 4, cudaMemcpyDeviceToHost));
   g_tc_state = 0;
-  for (int variant = 1; variant <= 2; variant++) {
+  for (int variant = 1; variant <= 1; variant++) {
     RB_CUDA(cudaMemcpy(buf.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
     RB_CUDA(cudaMemset(g_tc_err_flag.p, 0, sizeof(int)));
-    int rc = launch_tc(variant == 1 ? 1 : 0, C, ld, m, nn, k, A, ld, Bm, ld, 0);
+    int rc = launch_tc(C, ld, m, nn, k, A, ld, Bm, ld, 0, 0, 2);
     cudaError_t e = cudaDeviceSynchronize();
     if (rc != 0 || e != cudaSuccess) {
       cudaGetLastError();
@@ -355,7 +382,7 @@ int tc_gemm_f32(float *C, int ldc, int m, int n, int k, const float *A, int lda,
   if (g_tc_state < 0) RB_TRY(tc_selftest());
   if (g_tc_state <= 0) return 0;
   RB_TRY(g_tc_err_flag.alloc(sizeof(int)));
-  RB_TRY(launch_tc(g_tc_state == 1 ? 1 : 0, C, ldc, m, n, k, A, lda, B, ldb, st, overwrite));
+  RB_TRY(launch_tc(C, ldc, m, n, k, A, lda, B, ldb, st, overwrite));
   *used = 1;
   return 0;
 }
