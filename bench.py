@@ -93,6 +93,16 @@ class Clocks:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(e)}
 
 
+def max_over_ranks(value, device):
+    """The job's step time under N replicas: the slowest rank's device time
+    (all-reduce MAX over the default process group; NCCL on GPUs, gloo on CPU)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -145,12 +155,15 @@ def run_ours(args, rank, world):
         return st.copy()
 
     # plain FP64 GPU path once: the error reference and the speed comparator
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    step(0, 1, 0)
-    torch.cuda.synchronize()
-    t_plain = time.perf_counter() - t0
-    B_plain = d_B.cpu().numpy().copy()
+    # (--no-plain skips it, for launch-list captures of the mixed step alone)
+    t_plain, B_plain = float("nan"), None
+    if not args.no_plain:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step(0, 1, 0)
+        torch.cuda.synchronize()
+        t_plain = time.perf_counter() - t0
+        B_plain = d_B.cpu().numpy().copy()
 
     launches0 = _native.kernel_launches()
     for _ in range(args.warmup):
@@ -158,7 +171,7 @@ def run_ours(args, rank, world):
         step(1, MIXED_FAST, 2)
     torch.cuda.synchronize()
     B_mixed = d_B.cpu().numpy().copy()
-    err = float(np.abs(B_mixed - B_plain).max() / np.abs(B_plain).max())
+    err = float(np.abs(B_mixed - B_plain).max() / np.abs(B_plain).max()) if B_plain is not None else None
 
     times, t_asm, t_solve, t_fld = [], [], [], []
     clocks = Clocks(os.path.join(ROOT, "gpurun_out", f"bench_clocks_r{rank}.csv") if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
@@ -168,6 +181,8 @@ def run_ours(args, rank, world):
         dist.barrier()
     torch.cuda.synchronize()
     launches_before = _native.kernel_launches()
+    L.radb200_update_stats.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.radb200_update_timing(1)
     with clocks:
         for _ in range(args.steps):
             flush.fill_(2.0)
@@ -179,13 +194,13 @@ def run_ours(args, rank, world):
             t_fld.append(ev[2].elapsed_time(ev[3]) / 1e3)
             times.append(ev[0].elapsed_time(ev[3]) / 1e3)
     launches = (_native.kernel_launches() - launches_before) // max(args.steps, 1)
+    upd_n, upd_s, upd_b = C.c_int64(0), C.c_double(0), C.c_double(0)
+    L.radb200_update_stats(C.byref(upd_n), C.byref(upd_s), C.byref(upd_b))
+    L.radb200_update_timing(0)
     torch.cuda.synchronize()
     t_step = float(np.mean(times))
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([t_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_step = float(t.item())
+        t_step = max_over_ranks(t_step, dev)
 
     # end to end through the public API with host buffers (rad.RlxPre/RlxAuto/Fld)
     Ph = torch.from_numpy(P).pin_memory().numpy()
@@ -199,11 +214,27 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         e2e.append(time.perf_counter() - t0)
         rad.UtiDel(im)
-    e2e_err = float(np.abs(np.asarray(Bh) - B_plain).max() / np.abs(B_plain).max()) if e2e else None
+    e2e_err = float(np.abs(np.asarray(Bh) - B_plain).max() / np.abs(B_plain).max()) if (e2e and B_plain is not None) else None
     if not e2e:
         e2e = [float("nan")]
 
-    # roofline of the dominant kernel: the field evaluation (FP64 pipe)
+    # roofline of the LU trailing update (TF32 tcgen05, bounded by its C
+    # read-modify-write in HBM): algorithmic bytes per launch / event-timed
+    # launch duration, against the measured copy bandwidth
+    peaks = _peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    upd_gbs = upd_b.value / max(upd_s.value, 1e-30) / 1e9
+    upd_bytes_per_launch = upd_b.value / max(upd_n.value, 1)
+    roof_upd = {"kernel": "tc_update_kernel (LU trailing update A22 -= L21 U12)", "bound": "hbm",
+                "achieved": round(upd_gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(upd_gbs / hbm, 4),
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "traffic": round(TC_TRAFFIC_OVER_ALGORITHMIC * upd_bytes_per_launch),
+                "traffic_note": "ncu dram bytes / algorithmic bytes of the same kernel on a 9,000^2 LU, "
+                                "scaled to the launches of this step",
+                "launches_per_step": int(upd_n.value // max(args.steps, 1)),
+                "seconds_per_step": round(upd_s.value / max(args.steps, 1), 4),
+                "algorithmic": "8 m^2 + 8 m k bytes per launch (FP32 C read + written, panels read once)"}
+    # the field kernel (FP64 pipe, transcendental-bound) against the measured FP64 FMA peak
     n_faces = src["face"].shape[0]
     ops_per_face = FIELD_OPS_PER_TRIANGLE
     fld_s = float(np.mean(t_fld))
@@ -223,7 +254,8 @@ def run_ours(args, rank, world):
                 "h2d_bytes_per_step": int(P.nbytes + sum(a.nbytes for a in src.values()) + sum(a.nbytes for a in pack.elems.values())),
                 "d2h_bytes_per_step": int(P.nbytes + n3 * 8)},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": "field_kernel<double>", "bound": "fp64", "achieved": round(achieved, 3),
+        "roofline": roof_upd,
+        "roofline_field": {"kernel": "field_kernel<double, tetrahedron>", "bound": "fp64 pipe", "achieved": round(achieved, 3),
                      "peak": round(fp64_peak.value, 3), "unit": "TFLOP/s", "frac": round(achieved / fp64_peak.value, 4),
                      "peak_source": "measured FP64 FMA loop (radb200_measure_fma_peak) on this GPU",
                      "algorithmic": f"{ops_per_face} FP64 ops per (point, triangular face)",
@@ -276,6 +308,12 @@ def adjoint_ratio(reps=3):
                      "adjoint_residual": float(prob.last_status["adjoint"][0]),
                      "adjoint_iterations": int(prob.last_status["adjoint"][1])}
     return out
+
+
+# dram__bytes_read.sum + dram__bytes_write.sum over the algorithmic bytes of the
+# trailing-update kernel, from the ncu capture summarised in
+# profiles/tc_update_kernel_lu9000.md
+TC_TRAFFIC_OVER_ALGORITHMIC = 1.0
 
 
 # FP64 operations of one triangular face term of radTPolygon::B_comp as
@@ -345,6 +383,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison step (profiling runs)")
     ap.add_argument("--profile", action="store_true",
                     help="launch-list run: skip the end-to-end and CPU-baseline legs (keeps the launch count small)")
     args = ap.parse_args()

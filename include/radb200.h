@@ -128,6 +128,13 @@ RADB200_API int radb200_version(void);                      /* 100 * major + min
 /* Number of this library's kernels launched since load (all entry points). */
 RADB200_API int64_t radb200_kernel_launches(void);
 RADB200_API int radb200_device_sync(void);
+/* Profiling hook, no counterpart in the reference: CUDA-event timing of the
+ * dense LU's trailing updates on their own stream.  radb200_update_timing(1)
+ * starts collecting (and clears), 0 stops; radb200_update_stats returns the
+ * launches timed, their summed device seconds and algorithmic bytes (C read
+ * and written, panels read once) since then.                                */
+RADB200_API int radb200_update_timing(int on);
+RADB200_API int radb200_update_stats(int64_t *launches, double *seconds, double *bytes);
 /* Diagnostics, no counterpart in the reference: measured FMA throughput of
  * the FP64 (fp64 != 0) or FP32 pipe of the current device in TFLOP/s, the
  * roofline denominator of the transcendental-bound assembly / field kernels. */
@@ -227,8 +234,12 @@ RADB200_API int radb200_direct_solve(int64_t handle, int mode, double rtol, int 
  * Given the converged magnetization of the last solve and dL/dM [3N] (each
  * element's frame), solves the transposed system (I - D N)^T lambda = dL/dM
  * with D = dM/dH at the converged state (radmater.cpp:206-277) and returns
- * lambda [3N].  Uses the LU factors when the last solve was direct (linear),
- * otherwise GMRES on the transposed operator.                                */
+ * lambda [3N], by FP64 GMRES on the transposed operator preconditioned with
+ * A^T = U^T L^T: the kept factors of the direct solve (linear materials), or
+ * otherwise a factorization of A = I - D N (TF32 tensor cores above 3,072
+ * unknowns), kept until the next solve.  status: [4] = final relative
+ * residual, GMRES iterations, 1 if LU-preconditioned (0: block-Jacobi split
+ * after a factorization breakdown), seconds.                                */
 RADB200_API int radb200_adjoint_solve(int64_t handle, const double *dLdM, double rtol,
                           int max_iter, double *lambda_out, double *status);
 

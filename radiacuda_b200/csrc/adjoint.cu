@@ -348,6 +348,18 @@ __global__ void adj_finish_kernel(const double *__restrict__ part, int nchunk, i
   for (int a = 0; a < 3; a++) out[3 * e + a] = v[3 * e + a] - y[a];
 }
 
+// X_e = D_e = dM/dH at H_e, in the layout of a material record's chi slots
+__global__ void adj_dmat_kernel(const double *__restrict__ H, const int *__restrict__ kind, const double *__restrict__ mat,
+                                int n, double *__restrict__ X)
+{
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  double D[9];
+  mat_D(kind[e], mat + (size_t)e * RADB200_MAT_STRIDE, mk3<double>(H[3 * e], H[3 * e + 1], H[3 * e + 2]), D);
+  for (int k = 0; k < 9; k++) X[(size_t)e * RADB200_MAT_STRIDE + k] = D[k];
+  for (int k = 9; k < RADB200_MAT_STRIDE; k++) X[(size_t)e * RADB200_MAT_STRIDE + k] = 0.0;
+}
+
 // u_e = rowT_e^T D_e^T lambda_e (lab-frame weight of element e's field row)
 __global__ void adj_weight_kernel(const double *__restrict__ lambda, const double *__restrict__ H,
                                   const int *__restrict__ kind, const double *__restrict__ mat,
@@ -417,7 +429,8 @@ int adjoint_solve(Intrc &I, const double *dLdM, double rtol, int max_iter, doubl
 {
   auto t0 = std::chrono::steady_clock::now();
   const int n = I.n, n3 = I.n3, ld = I.ld;
-  const int use_lu = (all_linear(I) && I.last_kind == 1 && I.lu_mode >= 0) ? 1 : 0;
+  // factors of the forward matrix itself after a direct (linear) solve
+  int use_lu = (all_linear(I) && I.last_kind == 1 && I.lu_mode >= 0 && !I.lu_of_d) ? 1 : 0;
   DBuf buf, coef, part;
   RB_TRY(buf.alloc((size_t)4 * ld * sizeof(double)));
   RB_CUDA(cudaMemset(buf.p, 0, (size_t)4 * ld * sizeof(double)));
@@ -426,6 +439,23 @@ int adjoint_solve(Intrc &I, const double *dLdM, double rtol, int max_iter, doubl
   RB_TRY(converged_H(I, H));
   RB_TRY(coef.alloc((size_t)n * 27 * sizeof(double)));
   int nb = (n + 127) / 128;
+  double tfac = 0.0;
+  if (!use_lu) {
+    // factor A = I - D N at the converged state (TF32 tensor cores with FP64
+    // refinement for large systems) and precondition the transposed GMRES with
+    // A^T = U^T L^T; kept until the next solve.  If the unpivoted factorization
+    // breaks down, the block-Jacobi split of the operator is used instead.
+    if (I.lu_of_d && I.lu_solve_id == I.solve_id && I.lu_mode >= 0) {
+      use_lu = 1;
+    } else {
+      DBuf X;
+      RB_TRY(X.alloc((size_t)n * RADB200_MAT_STRIDE * sizeof(double)));
+      adj_dmat_kernel<<<nb, 128>>>(H, I.mat_kind.as<int>(), I.mat.as<double>(), n, X.as<double>());
+      RB_TRY(check_launch("adj_dmat_kernel"));
+      const int mode = n3 >= 3072 ? RADB200_LU_TF32 : RADB200_LU_F64;
+      if (lu_build_x(I, mode, X.as<double>(), 1, &tfac) == 0) use_lu = 1;
+    }
+  }
   if (I.N64.p)
     adj_prep_kernel<double><<<nb, 128>>>(I.N64.as<double>(), ld, n, H, I.mat_kind.as<int>(), I.mat.as<double>(), use_lu,
                                          coef.as<double>());

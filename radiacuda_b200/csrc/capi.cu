@@ -135,17 +135,30 @@ static void build_topo(const RadB200Geom *G, bool tensor, HostTopo &h)
     int v0 = (int)(h.tv.size() / 3), e0 = (int)h.tel.size(), t0 = (int)h.tt.size(), ff0 = (int)(h.tfn.size() / 3);
     std::vector<double> V;  // local vertices
     std::vector<std::vector<int>> loops(nf);
-    double scale = 0.0;
+    // every face's vertices back in 3-D: P = R^T (x, y, coordZ)
+    std::vector<double> Pall;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (int k = 0; k < nf; k++) {
       const double *R = G->face + (size_t)(f0 + k) * RADB200_FACE_STRIDE;
       int a0 = G->face_vtx[2 * (f0 + k)], na = G->face_vtx[2 * (f0 + k) + 1];
       for (int j = 0; j < na; j++) {
         double x = G->vtx2d[2 * (size_t)(a0 + j)], y = G->vtx2d[2 * (size_t)(a0 + j) + 1], z = R[9];
         double P[3] = {x * R[0] + y * R[3] + z * R[6], x * R[1] + y * R[4] + z * R[7], x * R[2] + y * R[5] + z * R[8]};
-        scale = std::max(scale, std::max(fabs(P[0]), std::max(fabs(P[1]), fabs(P[2]))));
+        for (int c = 0; c < 3; c++) { lo[c] = std::min(lo[c], P[c]); hi[c] = std::max(hi[c], P[c]); }
+        Pall.insert(Pall.end(), P, P + 3);
+      }
+    }
+    // copies of one vertex seen from different face frames differ by rounding
+    // of the frames (up to ~1e-7 of the size for sliver faces): merge within
+    // 1e-6 of the polyhedron's extent
+    double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    const double tol = 1e-6 * ext;
+    for (int k = 0, idx = 0; k < nf; k++) {
+      int na = G->face_vtx[2 * (f0 + k) + 1];
+      for (int j = 0; j < na; j++, idx++) {
+        const double *P = &Pall[3 * (size_t)idx];
         int found = -1;
         for (size_t q = 0; q < V.size() / 3; q++) {
-          double tol = 1e-10 * (1.0 + scale);
           if (fabs(V[3 * q] - P[0]) <= tol && fabs(V[3 * q + 1] - P[1]) <= tol && fabs(V[3 * q + 2] - P[2]) <= tol) {
             found = (int)q;
             break;
@@ -499,6 +512,7 @@ int radb200_relax(int64_t handle, int method, double prec, int max_iter, int res
   Intrc *I = find_intrc(handle);
   if (!I) return RADB200_E_HANDLE;
   if (!M_io || !status || max_iter < 0 || !(prec > 0) || method < 0 || method > 1) { set_error("bad relax arguments"); return RADB200_E_ARG; }
+  I->solve_id++;
   if (reset) RB_TRY(relax_reset(*I));
   else {
     RB_CUDA(cudaMemcpy(I->M.p, M_io, I->n3 * sizeof(double), cudaMemcpyHostToDevice));
@@ -521,6 +535,7 @@ int radb200_direct_solve(int64_t handle, int mode, double rtol, int max_iter, do
   if (!M_out || !status || mode < 0 || mode > 1) { set_error("bad direct-solve arguments"); return RADB200_E_ARG; }
   for (int e = 0; e < I->n; e++)
     if (I->h_mat_kind[e] != RADB200_MAT_LINEAR) { set_error("direct solve needs linear materials"); return RADB200_E_UNSUPPORTED; }
+  I->solve_id++;
   RB_TRY(direct_solve(*I, mode, rtol, max_iter, status));
   RB_CUDA(cudaMemcpy(M_out, I->M.p, I->n3 * sizeof(double), cudaMemcpyDeviceToHost));
   RB_TRY(I->lastM.alloc(I->ld * sizeof(double)));

@@ -11,7 +11,9 @@
 //   2. one elected thread issues k/8 tcgen05.mma.kind::tf32 (M=128, N=256,
 //      K=8) into 256 TMEM columns and commits them to an mbarrier, while every
 //      thread loads the 128 C values of its row segment;
-//   3. each thread reads its accumulators with tcgen05.ld and stores C - AB.
+//   3. each thread reads its accumulators with tcgen05.ld and stores C - AB,
+//      while the next tile's operand copies (issued once the MMAs completed)
+//      are in flight.
 // Waits on the mbarrier are bounded: on timeout the CTA raises an error flag,
 // still frees its TMEM and returns (the host then falls back to the CUDA-core
 // GEMM and reports the error).
@@ -76,6 +78,53 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 
+// 16-byte cp.async of the A (rows row0..) and B^T (rows col0..) chunks this
+// thread owns, in the K-major core-matrix layout; lanes -> (row % 8, 4
+// consecutive k-chunks), so global reads are 64-byte runs and shared writes
+// are bank-conflict free.
+__device__ __forceinline__ void tc_issue_operands(uint32_t a0, uint32_t b0, const float *__restrict__ A, int lda,
+                                                  const float *__restrict__ Bt, int ldbt, int m, int n, int k, int kpad,
+                                                  int row0, int col0, int tid)
+{
+  const int na = (TC_BM / 8) * (kpad / 4) * 8, nbb = (TC_BN / 8) * (kpad / 4) * 8;
+  for (int it = tid; it < na; it += TC_THREADS) {
+    int rr = it & 7, rest = it >> 3;
+    int kc = rest % (kpad / 4), rg = rest / (kpad / 4);
+    int gr = row0 + rg * 8 + rr, kk = kc * 4;
+    uint32_t bytes = (gr < m && kk < k) ? (uint32_t)(min(4, k - kk) * 4) : 0u;
+    const float *src = bytes ? A + (size_t)gr * lda + kk : A;
+    cp_async16(a0 + rg * 4096 + kc * 128 + rr * 16, src, bytes);
+  }
+  for (int it = tid; it < nbb; it += TC_THREADS) {
+    int nr = it & 7, rest = it >> 3;
+    int kc = rest % (kpad / 4), ngp = rest / (kpad / 4);
+    int gc = col0 + ngp * 8 + nr, kk = kc * 4;
+    uint32_t bytes = (gc < n && kk < k) ? (uint32_t)(min(4, k - kk) * 4) : 0u;
+    const float *src = bytes ? Bt + (size_t)gc * ldbt + kk : Bt;
+    cp_async16(b0 + ngp * 4096 + kc * 128 + nr * 16, src, bytes);
+  }
+}
+
+// round the chunks this thread copied to TF32 (visible to it after wait_all)
+__device__ __forceinline__ void tc_round_operands(unsigned char *sA, unsigned char *sB, int kpad, int tid)
+{
+  const int na = (TC_BM / 8) * (kpad / 4) * 8, nbb = (TC_BN / 8) * (kpad / 4) * 8;
+  for (int it = tid; it < na; it += TC_THREADS) {
+    int rr = it & 7, rest = it >> 3;
+    int kc = rest % (kpad / 4), rg = rest / (kpad / 4);
+    float4 *p = reinterpret_cast<float4 *>(sA + rg * 4096 + kc * 128 + rr * 16);
+    float4 v = *p;
+    *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
+  }
+  for (int it = tid; it < nbb; it += TC_THREADS) {
+    int nr = it & 7, rest = it >> 3;
+    int kc = rest % (kpad / 4), ngp = rest / (kpad / 4);
+    float4 *p = reinterpret_cast<float4 *>(sB + ngp * 4096 + kc * 128 + nr * 16);
+    float4 v = *p;
+    *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
+  }
+}
+
 // overwrite == 0: C -= A B;  overwrite == 1: C = A B.  C must not alias A or B.
 // Bt = B^T (n x ldbt, K contiguous).  Persistent: CTA b handles tiles b,
 // b + gridDim.x, ... (n-tiles fastest, so neighbouring CTAs share A rows in L2).
@@ -117,45 +166,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
   const int ksteps = (k + 7) / 8;
   const int kpad = ksteps * 8;
   const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-  const int na = (TC_BM / 8) * (kpad / 4) * 8;   // 16-byte chunks of A
-  const int nbb = (TC_BN / 8) * (kpad / 4) * 8;  // of B^T
   uint32_t phase = 0;
+  // operands of the first tile; later tiles' operands are issued as soon as the
+  // previous tile's MMAs are complete, so they arrive during its epilogue
+  if ((int)blockIdx.x < ntiles)
+    tc_issue_operands(a0, b0, A, lda, Bt, ldbt, m, n, k, kpad, ((int)blockIdx.x / tiles_n) * TC_BM,
+                      ((int)blockIdx.x % tiles_n) * TC_BN, tid);
 
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int row0 = (tile / tiles_n) * TC_BM, col0 = (tile % tiles_n) * TC_BN;
-    // ---- 1. stage A and B^T (K-major core matrices): lanes -> (row % 8, 4 consecutive k-chunks)
-    for (int it = tid; it < na; it += TC_THREADS) {
-      int rr = it & 7, rest = it >> 3;
-      int kc = rest % (kpad / 4), rg = rest / (kpad / 4);
-      int gr = row0 + rg * 8 + rr, kk = kc * 4;
-      uint32_t bytes = (gr < m && kk < k) ? (uint32_t)(min(4, k - kk) * 4) : 0u;
-      const float *src = bytes ? A + (size_t)gr * lda + kk : A;
-      cp_async16(a0 + rg * 4096 + kc * 128 + rr * 16, src, bytes);
-    }
-    for (int it = tid; it < nbb; it += TC_THREADS) {
-      int nr = it & 7, rest = it >> 3;
-      int kc = rest % (kpad / 4), ngp = rest / (kpad / 4);
-      int gc = col0 + ngp * 8 + nr, kk = kc * 4;
-      uint32_t bytes = (gc < n && kk < k) ? (uint32_t)(min(4, k - kk) * 4) : 0u;
-      const float *src = bytes ? Bt + (size_t)gc * ldbt + kk : Bt;
-      cp_async16(b0 + ngp * 4096 + kc * 128 + nr * 16, src, bytes);
-    }
+    const int next = tile + (int)gridDim.x;
+    // ---- 1. this tile's operands: wait for the copies, round to TF32
     asm volatile("cp.async.wait_all;" ::: "memory");
-    // round this thread's own chunks to TF32 (visible to it after wait_all)
-    for (int it = tid; it < na; it += TC_THREADS) {
-      int rr = it & 7, rest = it >> 3;
-      int kc = rest % (kpad / 4), rg = rest / (kpad / 4);
-      float4 *p = reinterpret_cast<float4 *>(sA + rg * 4096 + kc * 128 + rr * 16);
-      float4 v = *p;
-      *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
-    }
-    for (int it = tid; it < nbb; it += TC_THREADS) {
-      int nr = it & 7, rest = it >> 3;
-      int kc = rest % (kpad / 4), ngp = rest / (kpad / 4);
-      float4 *p = reinterpret_cast<float4 *>(sB + ngp * 4096 + kc * 128 + nr * 16);
-      float4 v = *p;
-      *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
-    }
+    tc_round_operands(sA, sB, kpad, tid);
     // generic-proxy smem writes -> visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -218,6 +241,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
     if (timed_out) break;
+    // the MMAs no longer read shared memory: fetch the next tile's operands now
+    if (next < ntiles)
+      tc_issue_operands(a0, b0, A, lda, Bt, ldbt, m, n, k, kpad, (next / tiles_n) * TC_BM, (next % tiles_n) * TC_BN, tid);
 
     // ---- 3. epilogue: TMEM -> registers -> C (warp w: TMEM lanes 32 (w % 4), columns 128 (w / 4))
 #pragma unroll

@@ -127,6 +127,9 @@ struct Intrc {
   DBuf LUinv;                         // [2][3N x 128] inverses of the diagonal blocks (L, then U)
   int lu_tc = 0;                      // the factorization ran on the tensor cores
   int lu_mode = -1;                   // factors valid for this mode (-1 none)
+  int lu_of_d = 0;                    // 1: the factors are of I - D N at the converged state of solve lu_solve_id
+  int lu_solve_id = -1;
+  int solve_id = 0;                   // counts relaxations / direct solves on this interaction
   DBuf lastM, lastH;                  // converged state of the last solve
   int last_kind = -1;                 // 0 relax, 1 direct
   // adjoint: external sources (kept for the gradient of H_ext at the centres),
@@ -166,6 +169,9 @@ int gmres(Op &op, int n3, int ld, const double *b, double *x, double rtol, int m
 int lu_precond(Intrc &I, double *x, cudaStream_t st);
 int relax_jacobi(Intrc &I, double prec, int max_iter, double omega0, double *status);
 int lu_precond_transposed(Intrc &I, double *x, cudaStream_t st);
+// factor A = I - X N with X [n x RADB200_MAT_STRIDE] (3x3 in the first 9
+// slots) into the interaction's LU buffers; of_d marks factors of I - D N
+int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_seconds);
 
 // TF32 tensor-core trailing update A -= L U (gemm_tc.cu); *used = 0 when the
 // shape is not supported and the caller must fall back to the CUDA-core GEMM.

@@ -71,64 +71,85 @@ __global__ void apply_A_kernel(const double *__restrict__ x, const double *__res
 }
 
 // ---- diagonal block: factor (unpivoted) and invert both triangles ----------
+// The block lives in shared memory at row pitch nb + 1 (so that threads
+// reading different rows at one column hit different banks).
+//   factor:  for k: scale column k below the pivot, rank-1 update of the
+//            trailing block (warp per row, lanes across columns);
+//   invert:  in place, L^-1 column by column from the right (unit lower,
+//            Linv[i][j] = -(L[i][j] + sum_{j<q<i} Linv[i][q] L[q][j])) by
+//            threads 0..127, and U^-1 column by column from the left
+//            (Uinv[i][j] = -sum_{i<=q<j} Uinv[i][q] U[q][j] / U[j][j]) by
+//            threads 128..255, each column copied aside first.
 template <typename T>
 __global__ void __launch_bounds__(256) diag_factor_kernel(T *__restrict__ A, int ld, int k0, int nb, T *__restrict__ Linv,
                                                           T *__restrict__ Uinv, int *__restrict__ err)
 {
-  extern __shared__ double sblk[];  // nb x nb
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    int r = e / nb, c = e % nb;
-    sblk[e] = (double)A[(size_t)(k0 + r) * ld + k0 + c];
+  extern __shared__ double sblk[];  // nb x (nb + 1)
+  __shared__ double colL[LU_NB], colU[LU_NB];
+  const int P = nb + 1;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int e = tid; e < nb * nb; e += blockDim.x) {
+    int r = e / nb, c = e - r * nb;
+    sblk[r * P + c] = (double)A[(size_t)(k0 + r) * ld + k0 + c];
   }
   __syncthreads();
   for (int k = 0; k < nb; k++) {
-    double piv = sblk[k * nb + k];
-    if (threadIdx.x == 0 && !(fabs(piv) > 1e-300)) err[0] = 1;
-    double ip = 1.0 / piv;
-    for (int r = k + 1 + threadIdx.x; r < nb; r += blockDim.x) sblk[r * nb + k] *= ip;
-    __syncthreads();
-    int m = nb - k - 1;
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      int r = k + 1 + e / m, c = k + 1 + e % m;
-      sblk[r * nb + c] -= sblk[r * nb + k] * sblk[k * nb + c];
+    const double piv = sblk[k * P + k];
+    if (tid == 0 && !(fabs(piv) > 1e-300)) err[0] = 1;
+    const double ip = 1.0 / piv;
+    for (int r = k + 1 + warp; r < nb; r += 8) {
+      const double l = sblk[r * P + k] * ip;
+      __syncwarp();
+      for (int c = k + 1 + lane; c < nb; c += 32) sblk[r * P + c] -= l * sblk[k * P + c];
+      if (lane == 0) sblk[r * P + k] = l;
     }
     __syncthreads();
   }
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    int r = e / nb, c = e % nb;
-    A[(size_t)(k0 + r) * ld + k0 + c] = (T)sblk[e];
+  for (int e = tid; e < nb * nb; e += blockDim.x) {
+    int r = e / nb, c = e - r * nb;
+    A[(size_t)(k0 + r) * ld + k0 + c] = (T)sblk[r * P + c];
   }
-  // inverses: threads [0, nb) build column j of L^-1, threads [128, 128+nb) column j of U^-1
-  int j = threadIdx.x & 127;
-  bool lower = threadIdx.x < 128;
-  if (j < nb) {
-    double x[LU_NB];
-    for (int i = 0; i < nb; i++) x[i] = 0.0;
+  __syncthreads();
+  const bool lower = tid < 128;
+  const int t = tid & 127;
+  for (int s = 0; s < nb; s++) {
+    const int jl = nb - 1 - s, ju = s;
     if (lower) {
-      x[j] = 1.0;
-      for (int i = j + 1; i < nb; i++) {
-        double s = 0.0;
-        for (int q = j; q < i; q++) s += sblk[i * nb + q] * x[q];
-        x[i] = -s;
+      if (t > jl && t < nb) colL[t] = sblk[t * P + jl];
+    } else if (t <= ju) {
+      colU[t] = sblk[t * P + ju];
+    }
+    __syncthreads();
+    if (lower) {
+      const int i = t;
+      if (i > jl && i < nb) {
+        double acc = colL[i];
+        for (int q = jl + 1; q < i; q++) acc += sblk[i * P + q] * colL[q];
+        sblk[i * P + jl] = -acc;
       }
-      for (int i = 0; i < nb; i++) Linv[(size_t)(k0 + i) * LU_NB + j] = (T)x[i];
     } else {
-      x[j] = 1.0 / sblk[j * nb + j];
-      for (int i = j - 1; i >= 0; i--) {
-        double s = 0.0;
-        for (int q = i + 1; q <= j; q++) s += sblk[i * nb + q] * x[q];
-        x[i] = -s / sblk[i * nb + i];
+      const int i = t;
+      const double d = 1.0 / colU[ju];
+      if (i < ju) {
+        double acc = 0.0;
+        for (int q = i; q < ju; q++) acc += sblk[i * P + q] * colU[q];
+        sblk[i * P + ju] = -acc * d;
+      } else if (i == ju) {
+        sblk[i * P + ju] = d;
       }
-      for (int i = 0; i < nb; i++) Uinv[(size_t)(k0 + i) * LU_NB + j] = (T)x[i];
     }
+    __syncthreads();
   }
-  // zero the padding columns of partial last blocks
-  if (nb < LU_NB)
-    for (int e = threadIdx.x; e < nb * (LU_NB - nb); e += blockDim.x) {
-      int r = e / (LU_NB - nb), c = nb + e % (LU_NB - nb);
-      Linv[(size_t)(k0 + r) * LU_NB + c] = T(0);
-      Uinv[(size_t)(k0 + r) * LU_NB + c] = T(0);
+  for (int e = tid; e < nb * LU_NB; e += blockDim.x) {
+    int i = e / LU_NB, j = e - i * LU_NB;
+    double l = 0.0, u = 0.0;
+    if (j < nb) {
+      l = (i > j) ? sblk[i * P + j] : (i == j ? 1.0 : 0.0);
+      u = (i <= j) ? sblk[i * P + j] : 0.0;
     }
+    Linv[(size_t)(k0 + i) * LU_NB + j] = (T)l;
+    Uinv[(size_t)(k0 + i) * LU_NB + j] = (T)u;
+  }
 }
 
 // ---- CUDA-core GEMM: C[m x n] (=|-=) A[m x k] B[k x n]; 64x64 tile, k-slices of 16
@@ -220,37 +241,58 @@ static int gemm(T *C, int ldc, int m, int n, int k, const T *A, int lda, const T
 }
 
 // ---- triangular solves with the factors (in place on x, FP64) ----
-// x[k0:k0+nb] <- Inv_k x[k0:k0+nb]   (Inv = L^-1 or U^-1 of diagonal block k)
+// dot of a 128-wide row (16-byte aligned, zero beyond nb) with xs, across a warp
+__device__ __forceinline__ double row128_dot(const float *row, const double *xs, int lane)
+{
+  float4 v = __ldg(reinterpret_cast<const float4 *>(row) + lane);
+  const double *xp = xs + 4 * lane;
+  return (double)v.x * xp[0] + (double)v.y * xp[1] + (double)v.z * xp[2] + (double)v.w * xp[3];
+}
+__device__ __forceinline__ double row128_dot(const double *row, const double *xs, int lane)
+{
+  double2 v0 = __ldg(reinterpret_cast<const double2 *>(row) + lane);
+  double2 v1 = __ldg(reinterpret_cast<const double2 *>(row) + 32 + lane);
+  return v0.x * xs[2 * lane] + v0.y * xs[2 * lane + 1] + v1.x * xs[64 + 2 * lane] + v1.y * xs[64 + 2 * lane + 1];
+}
+__device__ __forceinline__ double warp_sum(double s)
+{
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// x[k0:k0+nb] <- Inv_k x[k0:k0+nb]   (Inv = L^-1 or U^-1 of diagonal block k,
+// pitch 128 with zero columns beyond nb); warp per row
 template <typename T>
-__global__ void __launch_bounds__(LU_NB) block_matvec_kernel(const T *__restrict__ Inv, int k0, int nb, double *__restrict__ x)
+__global__ void __launch_bounds__(256) block_matvec_kernel(const T *__restrict__ Inv, int k0, int nb, double *__restrict__ x)
 {
   __shared__ double xs[LU_NB];
-  int r = threadIdx.x;
-  if (r < nb) xs[r] = x[k0 + r];
+  if (threadIdx.x < LU_NB) xs[threadIdx.x] = threadIdx.x < nb ? x[k0 + threadIdx.x] : 0.0;
   __syncthreads();
-  if (r < nb) {
-    const T *row = Inv + (size_t)(k0 + r) * LU_NB;
-    double s = 0.0;
-    for (int j = 0; j < nb; j++) s += (double)row[j] * xs[j];
-    x[k0 + r] = s;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r = warp; r < nb; r += 8) {
+    double s = warp_sum(row128_dot(Inv + (size_t)(k0 + r) * LU_NB, xs, lane));
+    if (lane == 0) x[k0 + r] = s;
   }
 }
 
-// x[rows r0..r1) -= A[rows, k0:k0+nb] x[k0:k0+nb] (warp per row)
+// x[rows r0..r1) -= A[rows, k0:k0+nb] x[k0:k0+nb] (warp per row, 16-byte loads
+// when the panel is a full 128 wide)
 template <typename T>
 __global__ void __launch_bounds__(256) panel_gemv_kernel(const T *__restrict__ A, int ld, int k0, int nb, int r0, int r1,
                                                          double *__restrict__ x)
 {
   __shared__ double xs[LU_NB];
-  for (int r = threadIdx.x; r < nb; r += blockDim.x) xs[r] = x[k0 + r];
+  for (int r = threadIdx.x; r < LU_NB; r += blockDim.x) xs[r] = r < nb ? x[k0 + r] : 0.0;
   __syncthreads();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int row = r0 + blockIdx.x * 8 + warp;
   if (row >= r1) return;
   const T *a = A + (size_t)row * ld + k0;
   double s = 0.0;
-  for (int j = lane; j < nb; j += 32) s += (double)a[j] * xs[j];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (nb == LU_NB) s = row128_dot(a, xs, lane);
+  else
+    for (int j = lane; j < nb; j += 32) s += (double)a[j] * xs[j];
+  s = warp_sum(s);
   if (lane == 0) x[row] -= s;
 }
 
@@ -314,11 +356,33 @@ static int lu_solve_t(const T *A, const T *Linv, const T *Uinv, int n3, int ld, 
   return 0;
 }
 
+// Optional CUDA-event timing of the trailing updates (A22 -= L21 U12) on the
+// stream they are launched on: radb200_update_timing(1) starts collecting,
+// radb200_update_stats() returns launches, summed device time and algorithmic
+// bytes (C read + written, panels read once) since then.
+struct UpdEvents {
+  std::vector<cudaEvent_t> ev;
+  int used = 0;
+  int grow()
+  {
+    if (2 * used + 2 <= (int)ev.size()) return 0;
+    for (int q = 0; q < 512; q++) {
+      cudaEvent_t e;
+      RB_CUDA(cudaEventCreate(&e));
+      ev.push_back(e);
+    }
+    return 0;
+  }
+};
+static int g_update_timing = 0;
+static UpdEvents g_upd_ev;
+static double g_upd_bytes = 0.0;
+
 template <typename T>
 static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaStream_t st, int *tc_used)
 {
   const int n3 = I.n3, ld = I.ld;
-  const int smax = LU_NB * LU_NB * (int)sizeof(double);
+  const int smax = LU_NB * (LU_NB + 1) * (int)sizeof(double);
   RB_CUDA(cudaFuncSetAttribute(diag_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   // RADB200_LU_TIMING=1 prints the time of each phase (synchronizes per phase)
   const bool timing = getenv("RADB200_LU_TIMING") != nullptr;
@@ -334,7 +398,7 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
   };
   for (int k0 = 0; k0 < n3; k0 += LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
-    diag_factor_kernel<T><<<1, 256, (size_t)nb * nb * sizeof(double), st>>>(A, ld, k0, nb, Linv, Uinv, d_err);
+    diag_factor_kernel<T><<<1, 256, (size_t)nb * (nb + 1) * sizeof(double), st>>>(A, ld, k0, nb, Linv, Uinv, d_err);
     RB_TRY(check_launch("diag_factor_kernel"));
     RB_TRY(phase(0));
     int rest = k0 + nb;
@@ -349,8 +413,18 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
     RB_TRY(copy2d<T>(A + (size_t)k0 * ld + rest, ld, tmp, ld, nb, m, st));
     RB_TRY(phase(2));
     // A22 -= L21 U12
+    if (g_update_timing) {
+      RB_TRY(g_upd_ev.grow());
+      RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used], st));
+    }
     RB_TRY(gemm<T>(A + (size_t)rest * ld + rest, ld, m, m, nb, A + (size_t)rest * ld + k0, ld, A + (size_t)k0 * ld + rest, ld,
                    0, st, tc_used));
+    if (g_update_timing) {
+      RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used + 1], st));
+      g_upd_ev.used++;
+      // algorithmic bytes: C read + written, the L and U panels read once
+      g_upd_bytes += (double)sizeof(T) * (2.0 * m * m + 2.0 * m * nb);
+    }
     RB_TRY(phase(3));
   }
   if (timing)
@@ -364,7 +438,7 @@ static int lu_solve(const T *A, const T *Linv, const T *Uinv, int n3, int ld, do
 {
   for (int k0 = 0; k0 < n3; k0 += LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
-    block_matvec_kernel<T><<<1, LU_NB, 0, st>>>(Linv, k0, nb, x);
+    block_matvec_kernel<T><<<1, 256, 0, st>>>(Linv, k0, nb, x);
     RB_TRY(check_launch("block_matvec_kernel"));
     int rest = k0 + nb;
     if (rest < n3) {
@@ -375,7 +449,7 @@ static int lu_solve(const T *A, const T *Linv, const T *Uinv, int n3, int ld, do
   int last = ((n3 - 1) / LU_NB) * LU_NB;
   for (int k0 = last; k0 >= 0; k0 -= LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
-    block_matvec_kernel<T><<<1, LU_NB, 0, st>>>(Uinv, k0, nb, x);
+    block_matvec_kernel<T><<<1, 256, 0, st>>>(Uinv, k0, nb, x);
     RB_TRY(check_launch("block_matvec_kernel"));
     if (k0 > 0) {
       panel_gemv_kernel<T><<<(k0 + 7) / 8, 256, 0, st>>>(A, ld, k0, nb, 0, k0, x);
@@ -422,9 +496,15 @@ struct LinOp : Op {
 
 int lu_build(Intrc &I, int mode, double *factor_seconds)
 {
+  if (I.lu_mode == mode && !I.lu_of_d) { *factor_seconds = 0.0; return 0; }
+  return lu_build_x(I, mode, I.mat.as<double>(), 0, factor_seconds);
+}
+
+int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_seconds)
+{
   auto t0 = std::chrono::steady_clock::now();
   const int n3 = I.n3, ld = I.ld;
-  if (I.lu_mode == mode) { *factor_seconds = 0.0; return 0; }
+  I.lu_mode = -1;
   DBuf err;
   RB_TRY(err.alloc(sizeof(int)));
   RB_CUDA(cudaMemset(err.p, 0, sizeof(int)));
@@ -436,8 +516,8 @@ int lu_build(Intrc &I, int mode, double *factor_seconds)
   if (mode == RADB200_LU_F64) {
     I.LU32.release();
     RB_TRY(I.LU64.alloc((size_t)n3 * ld * sizeof(double)));
-    if (I.N64.p) build_A_kernel<double, double><<<bgrid, 256>>>(I.N64.as<double>(), I.mat.as<double>(), n3, ld, I.LU64.as<double>());
-    else build_A_kernel<double, float><<<bgrid, 256>>>(I.N32.as<float>(), I.mat.as<double>(), n3, ld, I.LU64.as<double>());
+    if (I.N64.p) build_A_kernel<double, double><<<bgrid, 256>>>(I.N64.as<double>(), X, n3, ld, I.LU64.as<double>());
+    else build_A_kernel<double, float><<<bgrid, 256>>>(I.N32.as<float>(), X, n3, ld, I.LU64.as<double>());
     RB_TRY(check_launch("build_A_kernel"));
     double *inv = I.LUinv.as<double>();
     RB_TRY(lu_factor<double>(I, I.LU64.as<double>(), inv, inv + (size_t)n3 * LU_NB, I.lu_scratch.as<double>(), err.as<int>(), 0,
@@ -445,8 +525,8 @@ int lu_build(Intrc &I, int mode, double *factor_seconds)
   } else {
     I.LU64.release();
     RB_TRY(I.LU32.alloc((size_t)n3 * ld * sizeof(float)));
-    if (I.N64.p) build_A_kernel<float, double><<<bgrid, 256>>>(I.N64.as<double>(), I.mat.as<double>(), n3, ld, I.LU32.as<float>());
-    else build_A_kernel<float, float><<<bgrid, 256>>>(I.N32.as<float>(), I.mat.as<double>(), n3, ld, I.LU32.as<float>());
+    if (I.N64.p) build_A_kernel<float, double><<<bgrid, 256>>>(I.N64.as<double>(), X, n3, ld, I.LU32.as<float>());
+    else build_A_kernel<float, float><<<bgrid, 256>>>(I.N32.as<float>(), X, n3, ld, I.LU32.as<float>());
     RB_TRY(check_launch("build_A_kernel"));
     float *inv = I.LUinv.as<float>();
     RB_TRY(lu_factor<float>(I, I.LU32.as<float>(), inv, inv + (size_t)n3 * LU_NB, I.lu_scratch.as<float>(), err.as<int>(), 0,
@@ -458,6 +538,8 @@ int lu_build(Intrc &I, int mode, double *factor_seconds)
   if (tcflag) { I.lu_mode = -1; set_error("LU: a tensor-core update timed out waiting for its MMAs"); return RADB200_E_TIMEOUT; }
   if (herr) { I.lu_mode = -1; set_error("LU: vanishing pivot (matrix not factorable without pivoting)"); return RADB200_E_NUMERIC; }
   I.lu_mode = mode;
+  I.lu_of_d = of_d;
+  I.lu_solve_id = I.solve_id;
   I.lu_tc = tc_used;
   RB_CUDA(cudaDeviceSynchronize());
   *factor_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -490,3 +572,26 @@ int direct_solve(Intrc &I, int mode, double rtol, int max_iter, double *status)
 }
 
 }  // namespace rb
+
+extern "C" RADB200_API int radb200_update_timing(int on)
+{
+  rb::g_update_timing = on;
+  rb::g_upd_ev.used = 0;
+  rb::g_upd_bytes = 0.0;
+  return 0;
+}
+
+extern "C" RADB200_API int radb200_update_stats(int64_t *launches, double *seconds, double *bytes)
+{
+  RB_CUDA(cudaDeviceSynchronize());
+  double ms_total = 0.0;
+  for (int i = 0; i < rb::g_upd_ev.used; i++) {
+    float ms = 0.f;
+    RB_CUDA(cudaEventElapsedTime(&ms, rb::g_upd_ev.ev[2 * i], rb::g_upd_ev.ev[2 * i + 1]));
+    ms_total += ms;
+  }
+  *launches = rb::g_upd_ev.used;
+  *seconds = 1e-3 * ms_total;
+  *bytes = rb::g_upd_bytes;
+  return 0;
+}
