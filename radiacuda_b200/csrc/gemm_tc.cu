@@ -1,32 +1,33 @@
-// gemm_tc.cu -- TF32 tensor-core (tcgen05, TMEM accumulator) trailing update
-// of the blocked LU:   C[m x n] -= A[m x k] * B[k x n],   k <= 128,
-// all FP32 row-major inside the LU matrix (leading dimension ld).
+// gemm_tc.cu -- TF32 tensor-core (tcgen05, TMEM accumulator) GEMM updates of
+// the blocked LU:   C[m x n] -= A[m x k] * B[k x n]   (or C = A B),
+// all FP32 row-major inside the LU matrix (leading dimension ld), any k.
 //
 // Persistent CTAs of 8 warps loop over 128 x 256 tiles of C (one CTA per SM,
 // 192 KB of staged operands):
-//   1. cp.async brings A (128 x k) and B^T (256 x k) into shared memory in the
-//      canonical no-swizzle UMMA layouts (8-row x 16-byte core matrices) with
-//      many copies in flight; each thread then rounds its own chunks to TF32
-//      (round to nearest);
-//   2. one elected thread issues k/8 tcgen05.mma.kind::tf32 (M=128, N=256,
-//      K=8) into 256 TMEM columns and commits them to an mbarrier, while every
-//      thread loads the 128 C values of its row segment;
-//   3. each thread reads its accumulators with tcgen05.ld and stores C - AB,
-//      while the next tile's operand copies (issued once the MMAs completed)
-//      are in flight.
+//   1. K runs in chunks of 64 through two shared-memory stages: cp.async
+//      brings chunk g+1 of A (128 x 64) and B^T (256 x 64) into one stage,
+//      in the canonical no-swizzle UMMA layout (8-row x 16-byte core
+//      matrices), while the tensor core works on chunk g in the other; each
+//      thread rounds the chunks it copied to TF32 (round to nearest);
+//   2. one elected thread issues 8 tcgen05.mma.kind::tf32 (M=128, N=256,
+//      K=8) per chunk into 256 TMEM columns and commits them to an mbarrier;
+//      at a tile's first chunk every thread loads the 128 C values of its row
+//      segment, which stay in registers through the K loop;
+//   3. after the last chunk each thread reads its accumulators with
+//      tcgen05.ld and stores C - AB, while the next tile's first chunk lands.
 // Waits on the mbarrier are bounded: on timeout the CTA raises an error flag,
-// still frees its TMEM and returns (the host then falls back to the CUDA-core
-// GEMM and reports the error).
+// waits for its own copies, frees its TMEM and returns (the host then falls
+// back to the CUDA-core GEMM and reports the error).
 //
-// Layouts (byte offsets inside the A / B staging buffers):
-//   A, K-major:  (r/8)*4096 + (k/4)*128 + (r%8)*16 + (k%4)*4
-//                descriptor of MMA step s: start A + 256 s, LBO 128, SBO 4096
-//   B^T, K-major: (n/8)*4096 + (k/4)*128 + (n%8)*16 + (k%4)*4, same descriptors
-//   (B arrives row-major k x n and is transposed to n x 128 in global memory
-//   first: the k*n*8 bytes of the transpose are small against the m*n*8 of C;
-//   the MMA reads tf32 operands K-major only)
-// The first use runs a self-test against the CUDA-core GEMM and keeps the
-// tensor-core path only if it agrees to TF32 accuracy.
+// Layouts (byte offsets inside one stage's A / B^T buffers, chunk-local k):
+//   (row/8)*2048 + (k/4)*128 + (row%8)*16 + (k%4)*4, both operands K-major
+//   descriptor of MMA step s: start + 256 s, LBO 128 (next k group),
+//   SBO 2048 (next 8 rows).  B arrives row-major k x n and is transposed to
+//   n x k in global memory first (k*n*8 bytes, small against the m*n*8 of C;
+//   the MMA reads tf32 operands K-major only).
+// The first use runs a self-test against the CUDA-core GEMM (ragged m, n, k,
+// several tiles and chunks per CTA) and keeps the tensor-core path only if it
+// agrees to TF32 accuracy.
 #include <math.h>
 #include <stdlib.h>
 
@@ -36,11 +37,13 @@
 
 namespace rb {
 
-constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 128;
+constexpr int TC_BM = 128, TC_BN = 256;
+constexpr int TC_KC = 64;                       // K chunk per pipeline stage
 constexpr int TC_THREADS = 256;
-constexpr int TC_SMEM_A = TC_BM * TC_BK * 4;   // 64 KB
-constexpr int TC_SMEM_B = TC_BK * TC_BN * 4;   // 128 KB
-constexpr int TC_SMEM = TC_SMEM_A + TC_SMEM_B + 1024;
+constexpr int TC_STAGE_A = TC_BM * TC_KC * 4;   // 32 KB
+constexpr int TC_STAGE_B = TC_BN * TC_KC * 4;   // 64 KB
+constexpr int TC_STAGE = TC_STAGE_A + TC_STAGE_B;
+constexpr int TC_SMEM = 2 * TC_STAGE + 1024;      // two stages + alignment slack
 constexpr long long TC_SPIN_LIMIT = 1ll << 22;  // ~0.3 s of polling; the MMAs of a tile take microseconds
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -78,48 +81,54 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 
-// 16-byte cp.async of the A (rows row0..) and B^T (rows col0..) chunks this
-// thread owns, in the K-major core-matrix layout; lanes -> (row % 8, 4
-// consecutive k-chunks), so global reads are 64-byte runs and shared writes
-// are bank-conflict free.
-__device__ __forceinline__ void tc_issue_operands(uint32_t a0, uint32_t b0, const float *__restrict__ A, int lda,
-                                                  const float *__restrict__ Bt, int ldbt, int m, int n, int k, int kpad,
-                                                  int row0, int col0, int tid)
+// 16-byte cp.async of this thread's share of K chunk [k0, k0 + 64) of A
+// (rows row0..) and B^T (rows col0..) into one stage, in the K-major
+// core-matrix layout: offset (row / 8) * 2048 + (k / 4) * 128 + (row % 8) * 16.
+// Lanes -> (row % 8, 4 consecutive k-groups): global reads are 64-byte runs,
+// shared writes bank-conflict free.  Zero-filled past m, n and k.
+__device__ __forceinline__ void tc_issue_chunk(uint32_t sa, uint32_t sb, const float *__restrict__ A, int lda,
+                                               const float *__restrict__ Bt, int ldbt, int m, int n, int k, int k0,
+                                               int row0, int col0, int tid)
 {
-  const int na = (TC_BM / 8) * (kpad / 4) * 8, nbb = (TC_BN / 8) * (kpad / 4) * 8;
-  for (int it = tid; it < na; it += TC_THREADS) {
+  constexpr int NA = (TC_BM / 8) * (TC_KC / 4) * 8, NB = (TC_BN / 8) * (TC_KC / 4) * 8;
+#pragma unroll 4
+  for (int it = tid; it < NA; it += TC_THREADS) {
     int rr = it & 7, rest = it >> 3;
-    int kc = rest % (kpad / 4), rg = rest / (kpad / 4);
-    int gr = row0 + rg * 8 + rr, kk = kc * 4;
+    int kc = rest & (TC_KC / 4 - 1), rg = rest / (TC_KC / 4);
+    int gr = row0 + rg * 8 + rr, kk = k0 + kc * 4;
     uint32_t bytes = (gr < m && kk < k) ? (uint32_t)(min(4, k - kk) * 4) : 0u;
     const float *src = bytes ? A + (size_t)gr * lda + kk : A;
-    cp_async16(a0 + rg * 4096 + kc * 128 + rr * 16, src, bytes);
+    cp_async16(sa + rg * 2048 + kc * 128 + rr * 16, src, bytes);
   }
-  for (int it = tid; it < nbb; it += TC_THREADS) {
+#pragma unroll 4
+  for (int it = tid; it < NB; it += TC_THREADS) {
     int nr = it & 7, rest = it >> 3;
-    int kc = rest % (kpad / 4), ngp = rest / (kpad / 4);
-    int gc = col0 + ngp * 8 + nr, kk = kc * 4;
+    int kc = rest & (TC_KC / 4 - 1), ngp = rest / (TC_KC / 4);
+    int gc = col0 + ngp * 8 + nr, kk = k0 + kc * 4;
     uint32_t bytes = (gc < n && kk < k) ? (uint32_t)(min(4, k - kk) * 4) : 0u;
     const float *src = bytes ? Bt + (size_t)gc * ldbt + kk : Bt;
-    cp_async16(b0 + ngp * 4096 + kc * 128 + nr * 16, src, bytes);
+    cp_async16(sb + ngp * 2048 + kc * 128 + nr * 16, src, bytes);
   }
 }
 
-// round the chunks this thread copied to TF32 (visible to it after wait_all)
-__device__ __forceinline__ void tc_round_operands(unsigned char *sA, unsigned char *sB, int kpad, int tid)
+// round the chunks this thread copied into stage (sa, sb) to TF32 (visible to
+// it after cp.async.wait_all)
+__device__ __forceinline__ void tc_round_chunk(unsigned char *sa, unsigned char *sb, int tid)
 {
-  const int na = (TC_BM / 8) * (kpad / 4) * 8, nbb = (TC_BN / 8) * (kpad / 4) * 8;
-  for (int it = tid; it < na; it += TC_THREADS) {
+  constexpr int NA = (TC_BM / 8) * (TC_KC / 4) * 8, NB = (TC_BN / 8) * (TC_KC / 4) * 8;
+#pragma unroll 4
+  for (int it = tid; it < NA; it += TC_THREADS) {
     int rr = it & 7, rest = it >> 3;
-    int kc = rest % (kpad / 4), rg = rest / (kpad / 4);
-    float4 *p = reinterpret_cast<float4 *>(sA + rg * 4096 + kc * 128 + rr * 16);
+    int kc = rest & (TC_KC / 4 - 1), rg = rest / (TC_KC / 4);
+    float4 *p = reinterpret_cast<float4 *>(sa + rg * 2048 + kc * 128 + rr * 16);
     float4 v = *p;
     *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
   }
-  for (int it = tid; it < nbb; it += TC_THREADS) {
+#pragma unroll 4
+  for (int it = tid; it < NB; it += TC_THREADS) {
     int nr = it & 7, rest = it >> 3;
-    int kc = rest % (kpad / 4), ngp = rest / (kpad / 4);
-    float4 *p = reinterpret_cast<float4 *>(sB + ngp * 4096 + kc * 128 + nr * 16);
+    int kc = rest & (TC_KC / 4 - 1), ngp = rest / (TC_KC / 4);
+    float4 *p = reinterpret_cast<float4 *>(sb + ngp * 2048 + kc * 128 + nr * 16);
     float4 v = *p;
     *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
   }
@@ -128,6 +137,10 @@ __device__ __forceinline__ void tc_round_operands(unsigned char *sA, unsigned ch
 // overwrite == 0: C -= A B;  overwrite == 1: C = A B.  C must not alias A or B.
 // Bt = B^T (n x ldbt, K contiguous).  Persistent: CTA b handles tiles b,
 // b + gridDim.x, ... (n-tiles fastest, so neighbouring CTAs share A rows in L2).
+// Every tile runs ceil(k / 64) chunks through a two-stage pipeline: chunk g+1
+// is copied into the other stage while the MMAs of chunk g run; the tile's C
+// values are loaded into registers at its first chunk and consumed at its
+// last, so their latency hides behind the whole K loop.
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restrict__ C, int ldc, int m, int n, int k,
                                                                   const float *__restrict__ A, int lda,
                                                                   const float *__restrict__ Bt, int ldbt,
@@ -135,8 +148,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
 {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *sbase = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char *sA = sbase;
-  unsigned char *sB = sbase + TC_SMEM_A;
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_base_s;
   __shared__ int timed_out;
@@ -144,11 +155,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tiles_n = (n + TC_BN - 1) / TC_BN, tiles_m = (m + TC_BM - 1) / TC_BM;
   const int ntiles = tiles_n * tiles_m;
+  const int nch = (k + TC_KC - 1) / TC_KC;
   // once any CTA of this launch (or an earlier one) has timed out, the rest
   // return at once (decided by one thread so the whole CTA leaves together)
   if (tid == 0) abort_cta = *(volatile int *)err;
   __syncthreads();
-  if (abort_cta != 0 || (int)blockIdx.x >= ntiles) return;
+  if (abort_cta != 0 || (int)blockIdx.x >= ntiles || nch < 1) return;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)), "r"(TC_BN));
@@ -163,35 +175,41 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base_s;
-  const int ksteps = (k + 7) / 8;
-  const int kpad = ksteps * 8;
-  const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+  const uint32_t s0 = smem_u32(sbase);
+  // my tiles: blockIdx.x + i * gridDim.x; global chunk g = i * nch + c
+  const int my_tiles = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int G = my_tiles * nch;
   uint32_t phase = 0;
-  // operands of the first tile; later tiles' operands are issued as soon as the
-  // previous tile's MMAs are complete, so they arrive during its epilogue
-  if ((int)blockIdx.x < ntiles)
-    tc_issue_operands(a0, b0, A, lda, Bt, ldbt, m, n, k, kpad, ((int)blockIdx.x / tiles_n) * TC_BM,
-                      ((int)blockIdx.x % tiles_n) * TC_BN, tid);
+  const int q = warp & 3, hc = warp >> 2;
+  const int r = q * 32 + lane;
+  float4 cv[32];
 
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  {  // chunk 0 into stage 0
+    const int t0 = blockIdx.x;
+    tc_issue_chunk(s0, s0 + TC_STAGE_A, A, lda, Bt, ldbt, m, n, k, 0, (t0 / tiles_n) * TC_BM, (t0 % tiles_n) * TC_BN, tid);
+  }
+  for (int g = 0; g < G; g++) {
+    const int i = g / nch, c = g - i * nch;
+    const int tile = blockIdx.x + i * gridDim.x;
     const int row0 = (tile / tiles_n) * TC_BM, col0 = (tile % tiles_n) * TC_BN;
-    const int next = tile + (int)gridDim.x;
-    // ---- 1. this tile's operands: wait for the copies, round to TF32
+    const int st = g & 1;
+    unsigned char *sa = sbase + st * TC_STAGE, *sb = sa + TC_STAGE_A;
+    // ---- this chunk's operands: wait for the copies, round to TF32
     asm volatile("cp.async.wait_all;" ::: "memory");
-    tc_round_operands(sA, sB, kpad, tid);
-    // generic-proxy smem writes -> visible to the tensor core (async proxy)
+    tc_round_chunk(sa, sb, tid);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-    // ---- 2. MMAs (one thread)
+    // ---- MMAs of the chunk (one thread): 8 steps of K = 8
     if (tid == 0) {
       const uint32_t idesc = umma_idesc(0);
-      for (int s = 0; s < ksteps; s++) {
-        uint64_t da = umma_desc(a0 + 256u * s, 128u, 4096u);
-        uint64_t db = umma_desc(b0 + 256u * s, 128u, 4096u);
-        uint32_t acc = (s > 0) ? 1u : 0u;
+      const uint32_t ua = smem_u32(sa), ub = smem_u32(sb);
+#pragma unroll
+      for (int s = 0; s < TC_KC / 8; s++) {
+        uint64_t da = umma_desc(ua + 256u * s, 128u, 2048u);
+        uint64_t db = umma_desc(ub + 256u * s, 128u, 2048u);
+        uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
@@ -200,28 +218,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&mbar))
                    : "memory");
     }
-
-    // ---- meanwhile: this thread's C values (row r, 128 columns)
-    const int q = warp & 3, hc = warp >> 2;
-    const int r = q * 32 + lane;
-    const int gr = row0 + r, gcb = col0 + hc * 128;
-    float4 cv[32];
+    // ---- next chunk into the other stage (its last reader, chunk g-1, is complete)
+    if (g + 1 < G) {
+      const int i1 = (g + 1) / nch, c1 = (g + 1) - i1 * nch;
+      const int t1 = blockIdx.x + i1 * gridDim.x;
+      const uint32_t so = s0 + (st ^ 1) * TC_STAGE;
+      tc_issue_chunk(so, so + TC_STAGE_A, A, lda, Bt, ldbt, m, n, k, c1 * TC_KC, (t1 / tiles_n) * TC_BM,
+                     (t1 % tiles_n) * TC_BN, tid);
+    }
+    // ---- first chunk of a tile: this thread's C values (row r, 128 columns)
+    if (c == 0) {
+      const int gr = row0 + r, gcb = col0 + hc * 128;
 #pragma unroll
-    for (int j = 0; j < 32; j++) {
-      int gc = gcb + 4 * j;
-      cv[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (!overwrite && gr < m) {
-        const float *src = C + (size_t)gr * ldc + gc;
-        if (gc + 3 < n) cv[j] = *reinterpret_cast<const float4 *>(src);
-        else if (gc < n) {
-          cv[j].x = src[0];
-          if (gc + 1 < n) cv[j].y = src[1];
-          if (gc + 2 < n) cv[j].z = src[2];
+      for (int j = 0; j < 32; j++) {
+        int gc = gcb + 4 * j;
+        cv[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!overwrite && gr < m) {
+          const float *src = C + (size_t)gr * ldc + gc;
+          if (gc + 3 < n) cv[j] = *reinterpret_cast<const float4 *>(src);
+          else if (gc < n) {
+            cv[j].x = src[0];
+            if (gc + 1 < n) cv[j].y = src[1];
+            if (gc + 2 < n) cv[j].z = src[2];
+          }
         }
       }
     }
-
-    // ---- bounded wait for the MMAs of this tile
+    // ---- bounded wait for the chunk's MMAs
     {
       uint32_t done = 0;
       long long spins = 0;
@@ -241,11 +264,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
     if (timed_out) break;
-    // the MMAs no longer read shared memory: fetch the next tile's operands now
-    if (next < ntiles)
-      tc_issue_operands(a0, b0, A, lda, Bt, ldbt, m, n, k, kpad, (next / tiles_n) * TC_BM, (next % tiles_n) * TC_BN, tid);
+    if (c != nch - 1) continue;
 
-    // ---- 3. epilogue: TMEM -> registers -> C (warp w: TMEM lanes 32 (w % 4), columns 128 (w / 4))
+    // ---- last chunk: epilogue, TMEM -> registers -> C (warp w: TMEM lanes 32 (w % 4), columns 128 (w / 4))
+    const int gr = row0 + r, gcb = col0 + hc * 128;
 #pragma unroll
     for (int cb = 0; cb < 128; cb += 16) {
       uint32_t v[16];
@@ -274,25 +296,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
         }
       }
     }
-    // TMEM reads and smem uses of this tile complete before the next tile's copies / MMAs
+    // TMEM reads done before the next tile's first MMAs overwrite the accumulators
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
+  // no copies may still be landing in shared memory when the CTA exits
+  asm volatile("cp.async.wait_all;" ::: "memory");
   if (timed_out && tid == 0) atomicExch(err, 2);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
 }
 
-// CUDA-core reference for the self-test: C -= A B (FP32 inputs rounded to TF32 like the tensor path)
-__global__ void tc_ref_kernel(float *C, int ld, int m, int n, int k, const float *A, const float *B)
+// CUDA-core reference for the self-test: C -= A B or C = A B (FP32 inputs
+// rounded to TF32 like the tensor path)
+__global__ void tc_ref_kernel(float *C, int ld, int m, int n, int k, const float *A, const float *B, int overwrite)
 {
   int r = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= m || c >= n) return;
   float s = 0.f;
   for (int q = 0; q < k; q++) s = fmaf(to_tf32(A[(size_t)r * ld + q]), to_tf32(B[(size_t)q * ld + c]), s);
-  C[(size_t)r * ld + c] -= s;
+  C[(size_t)r * ld + c] = overwrite ? s : C[(size_t)r * ld + c] - s;
 }
 
 static int g_tc_state = -1;   // -1 untested, 0 disabled, 1 enabled
@@ -315,7 +340,7 @@ __global__ void tc_transpose_kernel(const float *__restrict__ B, int ldb, int k,
   }
 }
 
-static DBuf g_tc_bt;   // B^T scratch, [n x TC_BK] floats
+static DBuf g_tc_bt;   // B^T scratch, [n x ldbt] floats, ldbt = k rounded up to 4
 
 // max_ctas > 0 caps the persistent grid (the self-test uses it to make every
 // CTA loop over several tiles)
@@ -323,77 +348,88 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, const float *A, int
                      cudaStream_t st, int overwrite = 0, int max_ctas = 0)
 {
   long long tiles = (long long)((n + TC_BN - 1) / TC_BN) * ((m + TC_BM - 1) / TC_BM);
-  if (tiles > (1ll << 30) || k > TC_BK) { set_error("tensor-core update shape out of range"); return RADB200_E_ARG; }
+  if (tiles > (1ll << 30) || k < 1 || k > (1 << 20)) { set_error("tensor-core update shape out of range"); return RADB200_E_ARG; }
+  const int ldbt = (k + 3) / 4 * 4;
   static int nsm = 0;
   if (!nsm) {
     int dev = 0;
     RB_CUDA(cudaGetDevice(&dev));
     RB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   }
-  RB_TRY(g_tc_bt.alloc((size_t)n * TC_BK * sizeof(float)));
-  tc_transpose_kernel<<<dim3((n + 31) / 32, (k + 31) / 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, g_tc_bt.as<float>(), TC_BK);
+  RB_TRY(g_tc_bt.alloc((size_t)n * ldbt * sizeof(float)));
+  tc_transpose_kernel<<<dim3((n + 31) / 32, (k + 31) / 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, g_tc_bt.as<float>(), ldbt);
   RB_TRY(check_launch("tc_transpose_kernel"));
   int grid = (int)std::min<long long>(tiles, max_ctas > 0 ? max_ctas : nsm);
   RB_CUDA(cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-  tc_update_kernel<<<grid, TC_THREADS, TC_SMEM, st>>>(C, ldc, m, n, k, A, lda, g_tc_bt.as<float>(), TC_BK,
+  tc_update_kernel<<<grid, TC_THREADS, TC_SMEM, st>>>(C, ldc, m, n, k, A, lda, g_tc_bt.as<float>(), ldbt,
                                                       g_tc_err_flag.as<int>(), overwrite);
   return check_launch("tc_update_kernel");
 }
 
-// Runs a random 300 x 400 x 120 update (ragged in m, n and k on purpose) on
-// 2 CTAs, so each CTA loops over 3 tiles, and keeps the tensor-core path only
-// if it matches the CUDA-core reference.
-static int tc_selftest()
+// One self-test case: a random m x n x k update inside an ld-wide buffer
+// (A = rows k.. cols 0..k-1, B = rows 0..k-1 cols k.., C = rows k.. cols k..)
+// on 2 CTAs, so each CTA loops over several tiles and K chunks; returns the
+// relative max deviation from the CUDA-core reference in *err, or sets
+// *timeout when an MMA completion wait ran out.
+static int tc_selftest_case(int m, int n, int k, int overwrite, double *err, int *timeout)
 {
-  const int m = 300, n = 520, k = 120, ld = 640;
+  const int ld = ((k + n + 3) / 4) * 4;
   std::vector<float> h((size_t)(m + k) * ld);
-  unsigned s = 12345u;
+  unsigned s = 12345u + (unsigned)(m * 7 + n * 13 + k);
   for (auto &x : h) { s = s * 1664525u + 1013904223u; x = (float)((s >> 8) * (1.0 / 16777216.0) - 0.5); }
   DBuf buf, ref;
   RB_TRY(buf.alloc(h.size() * 4));
   RB_TRY(ref.alloc(h.size() * 4));
-  RB_TRY(g_tc_err_flag.alloc(sizeof(int)));
-  float *A = buf.as<float>() + (size_t)k * ld;          // rows k.. : A (m x k) at col 0, C at col k
-  float *Bm = buf.as<float>() + k;                      // rows 0..k-1, cols k.. : B
-  float *C = buf.as<float>() + (size_t)k * ld + k;
+  float *A = buf.as<float>() + (size_t)k * ld, *Bm = buf.as<float>() + k, *C = buf.as<float>() + (size_t)k * ld + k;
   float *Ar = ref.as<float>() + (size_t)k * ld, *Br = ref.as<float>() + k, *Cr = ref.as<float>() + (size_t)k * ld + k;
-  int nn = n - k;  // C is m x (n-k) inside the ld-wide buffer
   RB_CUDA(cudaMemcpy(ref.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
-  tc_ref_kernel<<<dim3((nn + 127) / 128, m), 128>>>(Cr, ld, m, nn, k, Ar, Br);
+  RB_CUDA(cudaMemcpy(buf.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
+  tc_ref_kernel<<<dim3((n + 127) / 128, m), 128>>>(Cr, ld, m, n, k, Ar, Br, overwrite);
   RB_TRY(check_launch("tc_ref_kernel"));
-  std::vector<float> cref((size_t)(m + k) * ld), ctc((size_t)(m + k) * ld);
-  RB_CUDA(cudaMemcpy(cref.data(), ref.p, h.size() * 4, cudaMemcpyDeviceToHost));
-  g_tc_state = 0;
-  for (int variant = 1; variant <= 1; variant++) {
-    RB_CUDA(cudaMemcpy(buf.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
-    RB_CUDA(cudaMemset(g_tc_err_flag.p, 0, sizeof(int)));
-    int rc = launch_tc(C, ld, m, nn, k, A, ld, Bm, ld, 0, 0, 2);
-    cudaError_t e = cudaDeviceSynchronize();
-    if (rc != 0 || e != cudaSuccess) {
-      cudaGetLastError();
-      set_error("tensor-core self-test launch failed (variant %d): %s", variant, cudaGetErrorString(e));
-      if (e != cudaSuccess) return RADB200_E_CUDA;  // context may be unusable: stop here
-      continue;
-    }
-    int flag = 0;
-    RB_CUDA(cudaMemcpy(&flag, g_tc_err_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) {  // an MMA never completed: leave the tensor-core path off, try nothing else
-      set_error("tensor-core self-test: MMA completion wait timed out (variant %d)", variant);
-      g_tc_state = 0;
-      return 0;
-    }
-    RB_CUDA(cudaMemcpy(ctc.data(), buf.p, h.size() * 4, cudaMemcpyDeviceToHost));
-    double maxd = 0.0, maxr = 0.0;
-    for (size_t i = 0; i < ctc.size(); i++) {
-      maxd = std::max(maxd, (double)fabs(ctc[i] - cref[i]));
-      maxr = std::max(maxr, (double)fabs(cref[i]));
-    }
-    g_tc_err = maxd / maxr;
-    if (flag == 0 && g_tc_err < 1e-4) {
-      g_tc_state = variant;
-      return 0;
-    }
+  RB_CUDA(cudaMemset(g_tc_err_flag.p, 0, sizeof(int)));
+  int rc = launch_tc(C, ld, m, n, k, A, ld, Bm, ld, 0, overwrite, 2);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (rc != 0 || e != cudaSuccess) {
+    cudaGetLastError();
+    set_error("tensor-core self-test launch failed: %s", cudaGetErrorString(e));
+    return e != cudaSuccess ? RADB200_E_CUDA : rc;
   }
+  int flag = 0;
+  RB_CUDA(cudaMemcpy(&flag, g_tc_err_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+  *timeout = flag != 0;
+  std::vector<float> cref(h.size()), ctc(h.size());
+  RB_CUDA(cudaMemcpy(cref.data(), ref.p, h.size() * 4, cudaMemcpyDeviceToHost));
+  RB_CUDA(cudaMemcpy(ctc.data(), buf.p, h.size() * 4, cudaMemcpyDeviceToHost));
+  double maxd = 0.0, maxr = 0.0;
+  for (size_t i = 0; i < ctc.size(); i++) {
+    maxd = std::max(maxd, (double)fabs(ctc[i] - cref[i]));
+    maxr = std::max(maxr, (double)fabs(cref[i]));
+  }
+  *err = maxd / maxr;
+  return 0;
+}
+
+// Keeps the tensor-core path only if every case matches the CUDA-core
+// reference to TF32 accuracy: K of 2 chunks (120) and of 5 (300), ragged m
+// and n, and the overwrite form the LU panels use.
+static int tc_selftest()
+{
+  RB_TRY(g_tc_err_flag.alloc(sizeof(int)));
+  g_tc_state = 0;
+  g_tc_err = 0.0;
+  const int cases[3][4] = {{300, 400, 120, 0}, {300, 300, 300, 0}, {260, 290, 64, 1}};
+  for (auto &cs : cases) {
+    double err = 1.0;
+    int timeout = 0;
+    RB_TRY(tc_selftest_case(cs[0], cs[1], cs[2], cs[3], &err, &timeout));
+    if (timeout) {  // an MMA never completed: leave the tensor-core path off
+      set_error("tensor-core self-test: MMA completion wait timed out");
+      return 0;
+    }
+    g_tc_err = std::max(g_tc_err, err);
+    if (!(err < 1e-4)) return 0;
+  }
+  g_tc_state = 1;
   return 0;
 }
 
@@ -402,7 +438,7 @@ int tc_gemm_f32(float *C, int ldc, int m, int n, int k, const float *A, int lda,
 {
   *used = 0;
   if (getenv("RADB200_NO_TC")) return 0;
-  if (k > TC_BK || m <= 0 || n <= 0 || (ldc % 4) || (lda % 4) || (ldb % 4) || ((uintptr_t)C & 15) || ((uintptr_t)A & 15) ||
+  if (k < 1 || m <= 0 || n <= 0 || (ldc % 4) || (lda % 4) || (ldb % 4) || ((uintptr_t)C & 15) || ((uintptr_t)A & 15) ||
       ((uintptr_t)B & 15))
     return 0;
   if (g_tc_state < 0) RB_TRY(tc_selftest());

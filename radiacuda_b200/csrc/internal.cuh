@@ -173,10 +173,11 @@ int lu_precond_transposed(Intrc &I, double *x, cudaStream_t st);
 // slots) into the interaction's LU buffers; of_d marks factors of I - D N
 int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_seconds);
 
-// TF32 tensor-core trailing update A -= L U (gemm_tc.cu); *used = 0 when the
-// shape is not supported and the caller must fall back to the CUDA-core GEMM.
+// TF32 tensor-core GEMM update (gemm_tc.cu); *used = 0 when the shape is not
+// supported and the caller must fall back to the CUDA-core GEMM.
 // C[m x n] -= A[m x k] B[k x n] (overwrite != 0: C = A B), FP32 row-major,
-// k <= 128, leading dimensions multiples of 4, 16-byte aligned pointers.
+// any k, leading dimensions multiples of 4, 16-byte aligned pointers, C not
+// aliasing A or B.
 int tc_gemm_f32(float *C, int ldc, int m, int n, int k, const float *A, int lda, const float *B, int ldb, cudaStream_t st,
                 int *used, int overwrite = 0);
 int tc_error_flag(int *flag);  // 2 when a tensor-core CTA hit its wait limit

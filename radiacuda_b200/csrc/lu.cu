@@ -8,13 +8,15 @@
 // positive semi-definite, so A is (close to) positive definite and needs no
 // row exchanges; a vanishing pivot is reported as RADB200_E_NUMERIC.
 //
-// Panel step k (width nb = 128):
+// Two levels: outer panels of 512 columns, 128-wide steps inside.  Step k
+// (width nb = 128) inside a panel:
 //   1. one CTA factors the diagonal block in shared memory (FP64) and writes
 //      the inverses of its unit-lower and upper triangles, L_kk^-1 and U_kk^-1;
-//   2. L21 = A21 U_kk^-1 and U12 = L_kk^-1 A12 as GEMMs (out of place, then
-//      copied back), so the triangular solves of the panel also run on the
-//      GEMM engine;
-//   3. trailing update A22 -= L21 U12.
+//   2. L21 = A21 U_kk^-1 and the panel's U12 = L_kk^-1 A12 as GEMMs (out of
+//      place, then copied back), so the triangular solves of the panel also
+//      run on the GEMM engine; a narrow update of the panel's other columns.
+// After the panel: its U block row by block forward substitution, then one
+// trailing update A22 -= L21 U12 with K = 512.
 //   mode F64  : FP64 factors, GEMMs on the FP64 pipe (CUDA cores).
 //   mode TF32 : FP32 factors, GEMMs on the tcgen05 tensor cores in TF32 with
 //               FP32 accumulation (gemm_tc.cu), then right-preconditioned FP64
@@ -378,6 +380,15 @@ static int g_update_timing = 0;
 static UpdEvents g_upd_ev;
 static double g_upd_bytes = 0.0;
 
+// Two-level right-looking LU.  Outer panels of LU_OUTER columns; inside a
+// panel, 128-wide steps (diagonal block, L21 = A21 U^-1, the panel's own
+// U12 = L^-1 A12 and a narrow update of the panel's remaining columns).  The
+// panel's U block row for the trailing columns is then solved by block
+// forward substitution over its 128-row sub-blocks, and the trailing matrix
+// receives ONE update with K = LU_OUTER: the C traffic of the dominant GEMM
+// drops by LU_OUTER / 128 against 128-wide steps.
+constexpr int LU_OUTER = 512;
+
 template <typename T>
 static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaStream_t st, int *tc_used)
 {
@@ -396,39 +407,58 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
     t_last = t;
     return 0;
   };
-  for (int k0 = 0; k0 < n3; k0 += LU_NB) {
-    int nb = std::min(LU_NB, n3 - k0);
-    diag_factor_kernel<T><<<1, 256, (size_t)nb * (nb + 1) * sizeof(double), st>>>(A, ld, k0, nb, Linv, Uinv, d_err);
-    RB_TRY(check_launch("diag_factor_kernel"));
-    RB_TRY(phase(0));
-    int rest = k0 + nb;
-    if (rest >= n3) break;
-    int m = n3 - rest;
-    // L21 = A21 U_kk^-1   (tmp: m x LU_NB)
-    RB_TRY(gemm<T>(tmp, LU_NB, m, nb, nb, A + (size_t)rest * ld + k0, ld, Uinv + (size_t)k0 * LU_NB, LU_NB, 1, st, tc_used));
-    RB_TRY(copy2d<T>(A + (size_t)rest * ld + k0, ld, tmp, LU_NB, m, nb, st));
-    RB_TRY(phase(1));
-    // U12 = L_kk^-1 A12   (tmp: nb x ld)
-    RB_TRY(gemm<T>(tmp, ld, nb, m, nb, Linv + (size_t)k0 * LU_NB, LU_NB, A + (size_t)k0 * ld + rest, ld, 1, st, tc_used));
-    RB_TRY(copy2d<T>(A + (size_t)k0 * ld + rest, ld, tmp, ld, nb, m, st));
+  auto at = [&](int r, int c) { return A + (size_t)r * ld + c; };
+  for (int K0 = 0; K0 < n3; K0 += LU_OUTER) {
+    const int NBe = std::min(LU_OUTER, n3 - K0);
+    const int pend = K0 + NBe;  // end of the panel's columns
+    // ---- factor the panel columns [K0, pend) over rows [K0, n3)
+    for (int j0 = K0; j0 < pend; j0 += LU_NB) {
+      const int jb = std::min(LU_NB, pend - j0);
+      diag_factor_kernel<T><<<1, 256, (size_t)jb * (jb + 1) * sizeof(double), st>>>(A, ld, j0, jb, Linv, Uinv, d_err);
+      RB_TRY(check_launch("diag_factor_kernel"));
+      RB_TRY(phase(0));
+      const int rest = j0 + jb, m = n3 - rest;
+      if (m <= 0) break;
+      // L21 = A21 U_jj^-1   (tmp: m x LU_NB)
+      RB_TRY(gemm<T>(tmp, LU_NB, m, jb, jb, at(rest, j0), ld, Uinv + (size_t)j0 * LU_NB, LU_NB, 1, st, tc_used));
+      RB_TRY(copy2d<T>(at(rest, j0), ld, tmp, LU_NB, m, jb, st));
+      const int w = pend - rest;  // panel columns right of this step
+      if (w > 0) {
+        // U12 inside the panel = L_jj^-1 A12   (tmp: jb x w)
+        RB_TRY(gemm<T>(tmp, ld, jb, w, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, rest), ld, 1, st, tc_used));
+        RB_TRY(copy2d<T>(at(j0, rest), ld, tmp, ld, jb, w, st));
+        // narrow update of the panel: A[rest:, rest:pend] -= L21 U12
+        RB_TRY(gemm<T>(at(rest, rest), ld, m, w, jb, at(rest, j0), ld, at(j0, rest), ld, 0, st, tc_used));
+      }
+      RB_TRY(phase(1));
+    }
+    const int T0 = pend, mT = n3 - pend;
+    if (mT <= 0) break;
+    // ---- U block row of the trailing columns: forward substitution with the
+    // panel's unit-lower diagonal block, 128 rows at a time
+    for (int j0 = K0; j0 < pend; j0 += LU_NB) {
+      const int jb = std::min(LU_NB, pend - j0);
+      if (j0 > K0) RB_TRY(gemm<T>(at(j0, T0), ld, jb, mT, j0 - K0, at(j0, K0), ld, at(K0, T0), ld, 0, st, tc_used));
+      RB_TRY(gemm<T>(tmp, ld, jb, mT, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, T0), ld, 1, st, tc_used));
+      RB_TRY(copy2d<T>(at(j0, T0), ld, tmp, ld, jb, mT, st));
+    }
     RB_TRY(phase(2));
-    // A22 -= L21 U12
+    // ---- trailing update A22 -= L21 U12 with K = NBe
     if (g_update_timing) {
       RB_TRY(g_upd_ev.grow());
       RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used], st));
     }
-    RB_TRY(gemm<T>(A + (size_t)rest * ld + rest, ld, m, m, nb, A + (size_t)rest * ld + k0, ld, A + (size_t)k0 * ld + rest, ld,
-                   0, st, tc_used));
+    RB_TRY(gemm<T>(at(T0, T0), ld, mT, mT, NBe, at(T0, K0), ld, at(K0, T0), ld, 0, st, tc_used));
     if (g_update_timing) {
       RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used + 1], st));
       g_upd_ev.used++;
       // algorithmic bytes: C read + written, the L and U panels read once
-      g_upd_bytes += (double)sizeof(T) * (2.0 * m * m + 2.0 * m * nb);
+      g_upd_bytes += (double)sizeof(T) * (2.0 * mT * mT + 2.0 * mT * NBe);
     }
     RB_TRY(phase(3));
   }
   if (timing)
-    fprintf(stderr, "[radb200 LU n=%d %s] diag %.3f s, L panel %.3f s, U panel %.3f s, trailing %.3f s\n", n3,
+    fprintf(stderr, "[radb200 LU n=%d %s] diag %.3f s, panel %.3f s, U block rows %.3f s, trailing %.3f s\n", n3,
             sizeof(T) == 4 ? "fp32/tf32" : "fp64", tph[0], tph[1], tph[2], tph[3]);
   return 0;
 }
