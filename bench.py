@@ -181,7 +181,8 @@ def run_ours(args, rank, world):
         dist.barrier()
     torch.cuda.synchronize()
     launches_before = _native.kernel_launches()
-    L.radb200_update_stats.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.radb200_update_stats.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double)]
     L.radb200_update_timing(1)
     with clocks:
         for _ in range(args.steps):
@@ -194,8 +195,8 @@ def run_ours(args, rank, world):
             t_fld.append(ev[2].elapsed_time(ev[3]) / 1e3)
             times.append(ev[0].elapsed_time(ev[3]) / 1e3)
     launches = (_native.kernel_launches() - launches_before) // max(args.steps, 1)
-    upd_n, upd_s, upd_b = C.c_int64(0), C.c_double(0), C.c_double(0)
-    L.radb200_update_stats(C.byref(upd_n), C.byref(upd_s), C.byref(upd_b))
+    upd_n, upd_s, upd_b, upd_f = C.c_int64(0), C.c_double(0), C.c_double(0), C.c_double(0)
+    L.radb200_update_stats(C.byref(upd_n), C.byref(upd_s), C.byref(upd_b), C.byref(upd_f))
     L.radb200_update_timing(0)
     torch.cuda.synchronize()
     t_step = float(np.mean(times))
@@ -218,27 +219,33 @@ def run_ours(args, rank, world):
     if not e2e:
         e2e = [float("nan")]
 
-    # roofline of the LU trailing update (TF32 tcgen05, bounded by its C
-    # read-modify-write in HBM): algorithmic bytes per launch / event-timed
-    # launch duration, against the measured copy bandwidth
+    # roofline of the LU trailing update (TF32 tcgen05 GEMM, K = 512): its
+    # flops (2 m^2 K per launch) over the event-timed launch durations,
+    # against the dense TF32 rate (half the measured bf16 rate); the HBM side
+    # (C read + written, panels once) beside it
     peaks = _peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
+    bf16 = peaks.get("bf16_tflops")
+    tf32_peak = float(bf16) / 2.0 if bf16 else 1590.0 / 2.0
+    upd_tflops = upd_f.value / max(upd_s.value, 1e-30) / 1e12
     upd_gbs = upd_b.value / max(upd_s.value, 1e-30) / 1e9
     upd_bytes_per_launch = upd_b.value / max(upd_n.value, 1)
-    roof_upd = {"kernel": "tc_update_kernel (LU trailing update A22 -= L21 U12)", "bound": "hbm",
-                "achieved": round(upd_gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(upd_gbs / hbm, 4),
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+    roof_upd = {"kernel": "tc_update_kernel (LU trailing update A22 -= L21 U12, K = 512)", "bound": "tensor",
+                "achieved": round(upd_tflops, 1), "peak": round(tf32_peak, 1), "unit": "TFLOP/s",
+                "frac": round(upd_tflops / tf32_peak, 4),
+                "peak_source": ("measured bf16 dense / 2 (TF32 runs at half the bf16 rate)" if bf16 else
+                                "fallback bf16 / 2"),
+                "hbm_achieved_gbs": round(upd_gbs, 1), "hbm_peak_gbs": hbm, "hbm_frac": round(upd_gbs / hbm, 4),
                 "traffic": round(TC_TRAFFIC_OVER_ALGORITHMIC * upd_bytes_per_launch),
                 "traffic_note": "ncu dram bytes / algorithmic bytes of the same kernel on a 9,000^2 LU, "
                                 "scaled to the launches of this step",
                 "launches_per_step": int(upd_n.value // max(args.steps, 1)),
                 "seconds_per_step": round(upd_s.value / max(args.steps, 1), 4),
-                "algorithmic": "8 m^2 + 8 m k bytes per launch (FP32 C read + written, panels read once)"}
+                "algorithmic": "2 m^2 K flops; 8 m^2 + 8 m K bytes per launch (FP32 C read + written, panels read once)"}
     # the field kernel (FP64 pipe, transcendental-bound) against the measured FP64 FMA peak
-    n_faces = src["face"].shape[0]
-    ops_per_face = FIELD_OPS_PER_TRIANGLE
+    n_tets = src["poly"].shape[0]
     fld_s = float(np.mean(t_fld))
-    achieved = P.shape[0] * n_faces * ops_per_face / fld_s / 1e12
+    achieved = P.shape[0] * n_tets * FIELD_OPS_PER_TET / fld_s / 1e12
     res = {
         "metric": METRIC, "value": round(t_step, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * t_step, 2), "higher_is_better": False,
@@ -258,7 +265,7 @@ def run_ours(args, rank, world):
         "roofline_field": {"kernel": "field_kernel<double, tetrahedron>", "bound": "fp64 pipe", "achieved": round(achieved, 3),
                      "peak": round(fp64_peak.value, 3), "unit": "TFLOP/s", "frac": round(achieved / fp64_peak.value, 4),
                      "peak_source": "measured FP64 FMA loop (radb200_measure_fma_peak) on this GPU",
-                     "algorithmic": f"{ops_per_face} FP64 ops per (point, triangular face)",
+                     "algorithmic": f"{FIELD_OPS_PER_TET} FP64 ops per (point, tetrahedron)",
                      "traffic": None},
         "clocks": clocks.summary(int(os.environ.get("LOCAL_RANK", 0))),
     }
@@ -305,6 +312,7 @@ def adjoint_ratio(reps=3):
         f, b = float(np.median(tf)), float(np.median(tb))
         out[name] = {"n_elements": int(prob.n), "n_points": int(pts.shape[0]), "forward_s": round(f, 4),
                      "adjoint_s": round(b, 4), "adjoint_over_forward": round(b / f, 3),
+                     "phases_s": {k: round(v, 4) for k, v in prob.last_timing.items()},
                      "adjoint_residual": float(prob.last_status["adjoint"][0]),
                      "adjoint_iterations": int(prob.last_status["adjoint"][1])}
     return out
@@ -316,11 +324,13 @@ def adjoint_ratio(reps=3):
 TC_TRAFFIC_OVER_ALGORITHMIC = 1.0
 
 
-# FP64 operations of one triangular face term of radTPolygon::B_comp as
-# restated in csrc/formulas.cuh, counting an add/mul/compare as 1, an FMA as
-# 2 and each elementary function by the cost of a standard implementation:
-# sqrt 8, div 8, log 20, atan2 30 (3 edges + the per-face log and frame).
-FIELD_OPS_PER_TRIANGLE = 3 * (2 * 8 + 5 * 8 + 20 + 30 + 75) + 20 + 60
+# FP64 operations of one (point, tetrahedron) term of the vertex/edge form
+# (tet_fast in csrc/formulas.cuh), counting an add/mul/compare as 1, an FMA
+# as 2 and each elementary function by the cost of a standard implementation
+# (sqrt, div 8; log1p 20; atan2 30): 4 vertex vectors and norms (4 x 16),
+# 6 edge dot products (6 x 5), 6 edge logarithms with their accumulation
+# (6 x 40), 4 solid angles with theirs (4 x 51), final scaling (3).
+FIELD_OPS_PER_TET = 4 * 16 + 6 * 5 + 6 * 40 + 4 * 51 + 3
 
 
 # ---------------------------------------------------------------------------

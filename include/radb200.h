@@ -131,10 +131,10 @@ RADB200_API int radb200_device_sync(void);
 /* Profiling hook, no counterpart in the reference: CUDA-event timing of the
  * dense LU's trailing updates on their own stream.  radb200_update_timing(1)
  * starts collecting (and clears), 0 stops; radb200_update_stats returns the
- * launches timed, their summed device seconds and algorithmic bytes (C read
- * and written, panels read once) since then.                                */
+ * launches timed, their summed device seconds, algorithmic bytes (C read and
+ * written, panels read once) and flops (2 m^2 K per update) since then.      */
 RADB200_API int radb200_update_timing(int on);
-RADB200_API int radb200_update_stats(int64_t *launches, double *seconds, double *bytes);
+RADB200_API int radb200_update_stats(int64_t *launches, double *seconds, double *bytes, double *flops);
 /* Diagnostics, no counterpart in the reference: measured FMA throughput of
  * the FP64 (fp64 != 0) or FP32 pipe of the current device in TFLOP/s, the
  * roofline denominator of the transcendental-bound assembly / field kernels. */

@@ -25,6 +25,7 @@ No counterpart in the reference: Radia has no derivatives.
 """
 from __future__ import annotations
 
+import time
 from typing import Dict, Optional, Sequence
 
 import numpy as np
@@ -60,6 +61,7 @@ class FieldProblem:
         self._intrc: Optional[_native.NativeInteraction] = None
         self._M: Optional[np.ndarray] = None
         self.last_status: Dict[str, np.ndarray] = {}
+        self.last_timing: Dict[str, float] = {}   # wall seconds of each phase of the last passes
 
     # ---- parameter helpers -------------------------------------------------
     def elements_of(self, handle: int) -> np.ndarray:
@@ -108,7 +110,9 @@ class FieldProblem:
                     self.centre0 if centre is None else centre, self.dims0 if dims is None else dims)
         if self._intrc is not None:
             self._intrc.free()
+        t0 = time.perf_counter()
         I = _native.NativeInteraction(self.pack, storage=self.storage)
+        t1 = time.perf_counter()
         if self.solver == "direct":
             M, st = I.direct(0 if self.storage == 1 else 1, self.prec, self.max_iter)
         else:
@@ -116,6 +120,7 @@ class FieldProblem:
                                np.zeros(3 * self.n))
         self._intrc, self._M = I, M
         self.last_status["forward"] = st
+        t2 = time.perf_counter()
         g = {k: v.copy() for k, v in self.pack.elems.items()}
         for e, (kind, idx) in enumerate(self.pack.elem_src):
             if kind == 0:
@@ -125,6 +130,8 @@ class FieldProblem:
         F = _native.field(g, self.pts, self.what, 0)
         if self.pack.ext is not None:
             F = F + _native.field(self.pack.ext, self.pts, self.what, 0)
+        t3 = time.perf_counter()
+        self.last_timing.update(assembly=t1 - t0, solve=t2 - t1, field=t3 - t2)
         return F
 
     def backward(self, W) -> Dict[str, np.ndarray]:
@@ -133,10 +140,15 @@ class FieldProblem:
             raise RuntimeError("backward before forward")
         I = self._intrc
         W = np.ascontiguousarray(np.asarray(W, dtype=np.float64).reshape(-1, 3))
+        t0 = time.perf_counter()
         gM, gc, gd = I.field_vjp(self._M, self.pts, self.what, W)
+        t1 = time.perf_counter()
         lam, st = I.adjoint_solve(gM, self.adj_rtol, 500)
+        t2 = time.perf_counter()
         self.last_status["adjoint"] = st
         g = I.adjoint_grad(lam)
+        t3 = time.perf_counter()
+        self.last_timing.update(field_vjp=t1 - t0, adjoint_solve=t2 - t1, adjoint_grad=t3 - t2)
         return dict(mr=g["Mr"].reshape(-1, 3), chi=g["chi"].reshape(-1, 3, 3),
                     centre=(g["c"] + gc).reshape(-1, 3), dims=(g["d"] + gd).reshape(-1, 3))
 

@@ -53,12 +53,17 @@ __device__ __forceinline__ void cuboid_dQ(V3<double> q, V3<double> hd, const dou
     double xx = X * X, yy = Y * Y, zz = Z * Z;
     double sxy = xx + yy, sxz = xx + zz, syz = yy + zz;
     if (!(sxy > 0.0 && sxz > 0.0 && syz > 0.0)) continue;
-    double R = sqrt(sxy + zz);
-    double iR = 1.0 / R, ixy = 1.0 / sxy, ixz = 1.0 / sxz, iyz = 1.0 / syz;
-    // 1/(Z + R) without cancellation for negative Z: (R - Z)/(X^2 + Y^2), etc.
-    double izr = Z >= 0.0 ? 1.0 / (Z + R) : (R - Z) * ixy;
-    double iyr = Y >= 0.0 ? 1.0 / (Y + R) : (R - Y) * ixz;
-    double ixr = X >= 0.0 ? 1.0 / (X + R) : (R - X) * iyz;
+    // 1/R by rsqrt; the three 1/(a^2 + b^2) from one division of their product
+    const double iR = rsqrt(sxy + zz), R = (sxy + zz) * iR;
+    const double pxy = sxz * syz, inv3 = 1.0 / (sxy * pxy);
+    const double ixy = pxy * inv3, ixz = sxy * syz * inv3, iyz = sxy * sxz * inv3;
+    // 1/(Z + R) without cancellation for negative Z: (R - Z)/(X^2 + Y^2), etc.;
+    // the divisions of the non-negative cases merged into one
+    const double dz = Z >= 0.0 ? Z + R : 1.0, dy = Y >= 0.0 ? Y + R : 1.0, dx = X >= 0.0 ? X + R : 1.0;
+    const double invd = 1.0 / (dz * dy * dx);
+    const double izr = Z >= 0.0 ? dy * dx * invd : (R - Z) * ixy;
+    const double iyr = Y >= 0.0 ? dz * dx * invd : (R - Y) * ixz;
+    const double ixr = X >= 0.0 ? dz * dy * invd : (R - X) * iyz;
     double XiR = X * iR, YiR = Y * iR, ZiR = Z * iR;
     double YZ = Y * ZiR, XZ = X * ZiR, XY = X * YiR;
     double gx = -w[0] * YZ * (ixz + ixy) + w[1] * YZ * ixy + w[2] * YZ * ixz;
@@ -106,7 +111,7 @@ __device__ __forceinline__ SrcInfo load_src(const GeomView &g, const int *elem_s
 //   ac -= d(u.G m)/dq     (= d/dc of the source centre, object frame)
 //   ad += d(u.G m)/dd     (full widths)
 //   ax += d(u.G m)/dx     (observer position, lab)
-template <bool WANT_M, bool WANT_SRC, bool WANT_OBS>
+template <bool WANT_M, bool WANT_SRC, bool WANT_OBS, bool RECT_ONLY = false>
 __device__ __forceinline__ void pair_adj(const GeomView &g, const SrcInfo &s, V3<double> x, V3<double> u, int what,
                                          double *aM, double *ac, double *ad, double *ax)
 {
@@ -123,11 +128,12 @@ __device__ __forceinline__ void pair_adj(const GeomView &g, const SrcInfo &s, V3
     double ut2 = __ldg(F + 2) * u.x + __ldg(F + 5) * u.y + __ldg(F + 8) * u.z;
     if (WANT_M) {
       double Q[9];
-      elem_tensor(g, s.kind, s.idx, q, Q);
+      if (RECT_ONLY) cuboid_tensor(g, s.idx, q, Q);
+      else elem_tensor(g, s.kind, s.idx, q, Q);
       aM[0] += Q[0] * ut0 + Q[3] * ut1 + Q[6] * ut2;
       aM[1] += Q[1] * ut0 + Q[4] * ut1 + Q[7] * ut2;
       aM[2] += Q[2] * ut0 + Q[5] * ut1 + Q[8] * ut2;
-      if (what == 0 && elem_inside(g, s.kind, s.idx, q)) { aM[0] += ut0; aM[1] += ut1; aM[2] += ut2; }
+      if (what == 0 && elem_inside(g, RECT_ONLY ? 0 : s.kind, s.idx, q)) { aM[0] += ut0; aM[1] += ut1; aM[2] += ut2; }
     }
     if ((WANT_SRC || WANT_OBS) && s.kind == 0) {
       double w[6] = {ut0 * s.m0, ut1 * s.m1, ut2 * s.m2, ut0 * s.m1 + ut1 * s.m0, ut0 * s.m2 + ut2 * s.m0,
@@ -151,7 +157,7 @@ constexpr int ADJ_T = 128;
 
 // Thread per source j; observers [k0, k1) of chunk blockIdx.y staged in shared
 // memory.  part[chunk][j][9] = (aM, ac, ad).
-template <bool WANT_M>
+template <bool WANT_M, bool RECT_ONLY>
 __global__ void __launch_bounds__(ADJ_T) adj_src_kernel(GeomView g, const int *__restrict__ elem_src,
                                                         const double *__restrict__ m, int n, const double *__restrict__ X,
                                                         const double *__restrict__ U, int nobs, int per_chunk, int what,
@@ -177,8 +183,8 @@ __global__ void __launch_bounds__(ADJ_T) adj_src_kernel(GeomView g, const int *_
     if (j < n)
       for (int kk = 0; kk < cnt; kk++) {
         const double *o = sx + 6 * kk;
-        pair_adj<WANT_M, true, false>(g, s, mk3<double>(o[0], o[1], o[2]), mk3<double>(o[3], o[4], o[5]), what, aM, ac, ad,
-                                      nullptr);
+        pair_adj<WANT_M, true, false, RECT_ONLY>(g, s, mk3<double>(o[0], o[1], o[2]), mk3<double>(o[3], o[4], o[5]), what,
+                                                 aM, ac, ad, nullptr);
       }
   }
   if (j < n) {
@@ -489,7 +495,7 @@ int adjoint_solve(Intrc &I, const double *dLdM, double rtol, int max_iter, doubl
 static void pair_chunks(int rows, int cols, int *nchunk, int *per_chunk)
 {
   int bx = (rows + ADJ_T - 1) / ADJ_T;
-  int c = std::max(1, std::min((148 * 4 + bx - 1) / bx, (cols + 31) / 32));
+  int c = std::max(1, std::min((148 * 8 + bx - 1) / bx, (cols + 31) / 32));
   int per = (cols + c - 1) / c;
   *per_chunk = std::max(per, 1);
   *nchunk = std::max(1, (cols + *per_chunk - 1) / *per_chunk);
@@ -504,8 +510,14 @@ static int src_pass(Intrc &I, const double *m, const double *X, const double *U,
   DBuf part;
   RB_TRY(part.alloc((size_t)nchunk * I.n * 9 * sizeof(double)));
   dim3 grid((I.n + ADJ_T - 1) / ADJ_T, nchunk);
-  adj_src_kernel<WANT_M><<<grid, ADJ_T>>>(I.geom.view(I.fast), I.elem_src.as<int>(), m, I.n, X, U, nobs, per, what,
-                                          part.as<double>());
+  // models of cuboids only (the undulators) get the variant without the
+  // polyhedron code paths (fewer registers, no spills)
+  if (I.geom.n_poly == 0)
+    adj_src_kernel<WANT_M, true><<<grid, ADJ_T>>>(I.geom.view(I.fast), I.elem_src.as<int>(), m, I.n, X, U, nobs, per, what,
+                                                  part.as<double>());
+  else
+    adj_src_kernel<WANT_M, false><<<grid, ADJ_T>>>(I.geom.view(I.fast), I.elem_src.as<int>(), m, I.n, X, U, nobs, per,
+                                                   what, part.as<double>());
   RB_TRY(check_launch("adj_src_kernel"));
   int64_t len = (int64_t)I.n * 9;
   adj_reduce_kernel<<<(unsigned)((len + 255) / 256), 256>>>(part.as<double>(), nchunk, len, out);

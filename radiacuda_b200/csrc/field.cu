@@ -165,6 +165,119 @@ __global__ void chunk_reduce_kernel(const double *__restrict__ part, int nc, int
   out[i] = s;
 }
 
+// All polyhedra are tetrahedra (fixed-topology vertex/edge form).  A block
+// of 128 threads takes 128 PPT points (PPT per thread: with 2, two
+// independent evaluation chains to interleave) and walks its unit range in tiles of 32
+// units whose records -- tetrahedron record, image transform, magnetization
+// -- it first stages in shared memory, so the per-pair reads are
+// shared-memory broadcasts.
+constexpr int TET_TILE = 32;
+constexpr int TET_U = TET_REC_FIELD + 21 + 3;  // record, Minv V sM (21), M (3)
+
+template <typename T>
+__device__ __forceinline__ void tet_unit(const double *su, V3<double> P, int what, double *acc)
+{
+  const double *Tr = su + TET_REC_FIELD, *M = Tr + 21;
+  double dx = P.x - Tr[9], dy = P.y - Tr[10], dz = P.z - Tr[11];
+  V3<double> q = mk3<double>(Tr[0] * dx + Tr[1] * dy + Tr[2] * dz, Tr[3] * dx + Tr[4] * dy + Tr[5] * dz,
+                             Tr[6] * dx + Tr[7] * dy + Tr[8] * dz);
+  double h[3];
+  int in = tet_fast<T, false, true>(su, q, h);
+  V3<double> f;
+  if (what == 2) f = in ? mk3<double>(M[0], M[1], M[2]) : mk3<double>(0, 0, 0);
+  else {
+    f = mk3<double>(h[0], h[1], h[2]);
+    if (what == 0 && in) { f.x += M[0]; f.y += M[1]; f.z += M[2]; }
+  }
+  const double *F = Tr + 12;
+  acc[0] += F[0] * f.x + F[1] * f.y + F[2] * f.z;
+  acc[1] += F[3] * f.x + F[4] * f.y + F[5] * f.z;
+  acc[2] += F[6] * f.x + F[7] * f.y + F[8] * f.z;
+}
+
+template <typename T, int PPT>
+__global__ void __launch_bounds__(128) field_tet_kernel(GeomView g, const double *__restrict__ pts, int64_t npts, int what,
+                                                        double *__restrict__ out, int ub, int ue, int chunk, int accumulate)
+{
+  __shared__ double su[TET_TILE * TET_U];
+  const int tid = threadIdx.x;
+  const int64_t i0 = (int64_t)blockIdx.x * (128 * PPT) + tid, i1 = PPT == 2 ? i0 + 128 : npts;
+  const int u0 = ub + blockIdx.y * chunk, u1 = min(ue, u0 + chunk);
+  V3<double> P0 = mk3<double>(0, 0, 0), P1 = P0;
+  if (i0 < npts) P0 = mk3<double>(pts[3 * i0], pts[3 * i0 + 1], pts[3 * i0 + 2]);
+  if (i1 < npts) P1 = mk3<double>(pts[3 * i1], pts[3 * i1 + 1], pts[3 * i1 + 2]);
+  double a0[3] = {0, 0, 0}, a1[3] = {0, 0, 0};
+  for (int base = u0; base < u1; base += TET_TILE) {
+    const int cnt = min(TET_TILE, u1 - base);
+    __syncthreads();
+    for (int e = tid; e < cnt * TET_U; e += 128) {
+      const int k = e / TET_U, f = e - k * TET_U;
+      const int4 un = __ldg(g.units + base + k);  // {kind, polyhedron, transform, 0}
+      double v;
+      if (f < TET_REC_FIELD) v = __ldg(g.tetrec + (size_t)__ldg(g.tetidx + un.y) * TET_REC_FIELD + f);
+      else if (f < TET_REC_FIELD + 21) v = __ldg(g.trf + (size_t)un.z * RADB200_TRF_STRIDE + (f - TET_REC_FIELD));
+      else v = __ldg(g.poly + (size_t)un.y * RADB200_POLY_STRIDE + 3 + (f - TET_REC_FIELD - 21));
+      su[e] = v;
+    }
+    __syncthreads();
+    for (int k = 0; k < cnt; k++) {
+      tet_unit<T>(su + k * TET_U, P0, what, a0);
+      if (PPT == 2) tet_unit<T>(su + k * TET_U, P1, what, a1);
+    }
+  }
+  if (i0 < npts) {
+    double *o = out + ((size_t)blockIdx.y * npts + i0) * 3;
+    if (accumulate) { o[0] += a0[0]; o[1] += a0[1]; o[2] += a0[2]; }
+    else { o[0] = a0[0]; o[1] = a0[1]; o[2] = a0[2]; }
+  }
+  if (i1 < npts) {
+    double *o = out + ((size_t)blockIdx.y * npts + i1) * 3;
+    if (accumulate) { o[0] += a1[0]; o[1] += a1[1]; o[2] += a1[2]; }
+    else { o[0] = a1[0]; o[1] = a1[1]; o[2] = a1[2]; }
+  }
+}
+
+template <typename T, int PPT>
+static int launch_tet_ppt(const GeomView &g, const double *d_pts, int64_t npts, int what, double *d_out, int ub, int ue,
+                          int accumulate, DBuf &scratch, cudaStream_t st)
+{
+  int64_t nblk = (npts + 128 * PPT - 1) / (128 * PPT);
+  int nu = ue - ub;
+  int nchunk = 1;
+  const int64_t target = 148 * 6;
+  if (nblk < target) nchunk = (int)((target + nblk - 1) / nblk);
+  if (nchunk > nu) nchunk = nu;
+  if (nchunk > 65535) nchunk = 65535;
+  int chunk = (nu + nchunk - 1) / nchunk;
+  nchunk = (nu + chunk - 1) / chunk;
+  dim3 grid((unsigned)nblk, (unsigned)nchunk);
+  if (nchunk == 1) {
+    field_tet_kernel<T, PPT><<<grid, 128, 0, st>>>(g, d_pts, npts, what, d_out, ub, ue, chunk, accumulate);
+    return check_launch("field_tet_kernel");
+  }
+  RB_TRY(scratch.alloc((size_t)nchunk * npts * 3 * sizeof(double)));
+  field_tet_kernel<T, PPT><<<grid, 128, 0, st>>>(g, d_pts, npts, what, scratch.as<double>(), ub, ue, chunk, 0);
+  RB_TRY(check_launch("field_tet_kernel"));
+  int64_t n3 = npts * 3;
+  chunk_reduce_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(scratch.as<double>(), nchunk, n3, d_out, accumulate);
+  return check_launch("chunk_reduce_kernel");
+}
+
+// points per thread: 1 (more resident warps) or 2 (two interleaved chains);
+// RADB200_TET_PPT overrides the default for tuning
+template <typename T>
+static int launch_tet(const GeomView &g, const double *d_pts, int64_t npts, int what, double *d_out, int ub, int ue,
+                      int accumulate, DBuf &scratch, cudaStream_t st)
+{
+  static int ppt = 0;
+  if (!ppt) {
+    const char *e = getenv("RADB200_TET_PPT");
+    ppt = (e && atoi(e) == 2) ? 2 : 1;
+  }
+  if (ppt == 2) return launch_tet_ppt<T, 2>(g, d_pts, npts, what, d_out, ub, ue, accumulate, scratch, st);
+  return launch_tet_ppt<T, 1>(g, d_pts, npts, what, d_out, ub, ue, accumulate, scratch, st);
+}
+
 template <typename T, int KIND>
 static int launch_kind(const GeomView &g, const double *d_pts, int64_t npts, int what, double *d_out, int ub, int ue,
                        int accumulate, DBuf &scratch, cudaStream_t st)
@@ -211,8 +324,8 @@ int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what,
     if (kind == 0)
       rc = launch_kind<double, UK_REC>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
     else if (kind == 1 && g.fast && g.all_tets)
-      rc = (precision == 1) ? launch_kind<float, UK_TET>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st)
-                            : launch_kind<double, UK_TET>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
+      rc = (precision == 1) ? launch_tet<float>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st)
+                            : launch_tet<double>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
     else if (kind == 1 && g.fast)
       rc = (precision == 1) ? launch_kind<float, UK_POLY_FAST>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st)
                             : launch_kind<double, UK_POLY_FAST>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);

@@ -504,16 +504,24 @@ __host__ __device__ constexpr int tet_face_c(int f) { return f == 3 ? 2 : 3; }
 // index of the vertex pair (i < j) in the edge list
 __host__ __device__ constexpr int tet_pair(int i, int j) { return i == 0 ? j - 1 : (i == 1 ? j + 1 : 5); }
 
-template <typename T, bool TENSOR>
+template <bool SMEM>
+__device__ __forceinline__ double rd_rec(const double *p)
+{
+  if (SMEM) return *p;
+  return __ldg(p);
+}
+
+// SMEM: the record lives in shared memory (plain loads instead of __ldg)
+template <typename T, bool TENSOR, bool SMEM = false>
 __device__ __forceinline__ int tet_fast(const double *__restrict__ rec, V3<double> q, double *out)
 {
   const double C = 1.0 / (4.0 * 3.141592653589793238);
   T rx[4], ry[4], rz[4], R[4];
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    rx[k] = T(__ldg(rec + 3 * k) - q.x);
-    ry[k] = T(__ldg(rec + 3 * k + 1) - q.y);
-    rz[k] = T(__ldg(rec + 3 * k + 2) - q.z);
+    rx[k] = T(rd_rec<SMEM>(rec + 3 * k) - q.x);
+    ry[k] = T(rd_rec<SMEM>(rec + 3 * k + 1) - q.y);
+    rz[k] = T(rd_rec<SMEM>(rec + 3 * k + 2) - q.z);
     R[k] = sqrtT(rx[k] * rx[k] + ry[k] * ry[k] + rz[k] * rz[k]);
   }
   T d[6];  // r_i . r_j per edge
@@ -528,7 +536,7 @@ __device__ __forceinline__ int tet_fast(const double *__restrict__ rec, V3<doubl
 #pragma unroll
   for (int e = 0; e < 6; e++) {
     const int a = tet_edge_a(e), b = tet_edge_b(e);
-    T l = T(__ldg(rec + 12 + e));
+    T l = T(rd_rec<SMEM>(rec + 12 + e));
     T D;
     if (d[e] >= T(0)) D = R[a] * R[b] + d[e];
     else {
@@ -538,28 +546,28 @@ __device__ __forceinline__ int tet_fast(const double *__restrict__ rec, V3<doubl
     double L = (double)log1pT<T>(l * (R[a] + R[b] + l) / D);
     if (TENSOR) {
 #pragma unroll
-      for (int k = 0; k < 9; k++) acc[k] += L * __ldg(rec + 42 + 9 * e + k);
+      for (int k = 0; k < 9; k++) acc[k] += L * rd_rec<SMEM>(rec + 42 + 9 * e + k);
     } else {
 #pragma unroll
-      for (int k = 0; k < 3; k++) acc[k] += L * __ldg(rec + 42 + 3 * e + k);
+      for (int k = 0; k < 3; k++) acc[k] += L * rd_rec<SMEM>(rec + 42 + 3 * e + k);
     }
   }
   double omega_tot = 0.0;
 #pragma unroll
   for (int f = 0; f < 4; f++) {
     const int a = tet_face_a(f), b = tet_face_b(f), c = tet_face_c(f);
-    T num = rx[a] * T(__ldg(rec + 18 + 3 * f)) + ry[a] * T(__ldg(rec + 19 + 3 * f)) + rz[a] * T(__ldg(rec + 20 + 3 * f));
+    T num = rx[a] * T(rd_rec<SMEM>(rec + 18 + 3 * f)) + ry[a] * T(rd_rec<SMEM>(rec + 19 + 3 * f)) + rz[a] * T(rd_rec<SMEM>(rec + 20 + 3 * f));
     T den = R[a] * R[b] * R[c] + d[tet_pair(a, b)] * R[c] + d[tet_pair(a, c)] * R[b] + d[tet_pair(b, c)] * R[a];
     double om = 2.0 * (double)atan2T(-num, den);
     omega_tot += om;
     if (TENSOR) {
-      double n0 = __ldg(rec + 30 + 3 * f), n1 = __ldg(rec + 31 + 3 * f), n2 = __ldg(rec + 32 + 3 * f);
+      double n0 = rd_rec<SMEM>(rec + 30 + 3 * f), n1 = rd_rec<SMEM>(rec + 31 + 3 * f), n2 = rd_rec<SMEM>(rec + 32 + 3 * f);
       acc[0] += om * n0 * n0; acc[1] += om * n0 * n1; acc[2] += om * n0 * n2;
       acc[3] += om * n1 * n0; acc[4] += om * n1 * n1; acc[5] += om * n1 * n2;
       acc[6] += om * n2 * n0; acc[7] += om * n2 * n1; acc[8] += om * n2 * n2;
     } else {
 #pragma unroll
-      for (int k = 0; k < 3; k++) acc[k] += om * __ldg(rec + 30 + 3 * f + k);
+      for (int k = 0; k < 3; k++) acc[k] += om * rd_rec<SMEM>(rec + 30 + 3 * f + k);
     }
   }
 #pragma unroll

@@ -4,11 +4,14 @@
 //
 // Persistent CTAs of 8 warps loop over 128 x 256 tiles of C (one CTA per SM,
 // 192 KB of staged operands):
+//   0. A is rounded to TF32 (round to nearest) in place and B is transposed
+//      to K-major with the same rounding, once per call, so the tensor core
+//      reads exact TF32 values (in the LU, A is always an L panel or an
+//      inverse, which the factorization keeps at TF32 accuracy anyway);
 //   1. K runs in chunks of 64 through two shared-memory stages: cp.async
 //      brings chunk g+1 of A (128 x 64) and B^T (256 x 64) into one stage,
 //      in the canonical no-swizzle UMMA layout (8-row x 16-byte core
-//      matrices), while the tensor core works on chunk g in the other; each
-//      thread rounds the chunks it copied to TF32 (round to nearest);
+//      matrices), while the tensor core works on chunk g in the other;
 //   2. one elected thread issues 8 tcgen05.mma.kind::tf32 (M=128, N=256,
 //      K=8) per chunk into 256 TMEM columns and commits them to an mbarrier;
 //      at a tile's first chunk every thread loads the 128 C values of its row
@@ -111,29 +114,6 @@ __device__ __forceinline__ void tc_issue_chunk(uint32_t sa, uint32_t sb, const f
   }
 }
 
-// round the chunks this thread copied into stage (sa, sb) to TF32 (visible to
-// it after cp.async.wait_all)
-__device__ __forceinline__ void tc_round_chunk(unsigned char *sa, unsigned char *sb, int tid)
-{
-  constexpr int NA = (TC_BM / 8) * (TC_KC / 4) * 8, NB = (TC_BN / 8) * (TC_KC / 4) * 8;
-#pragma unroll 4
-  for (int it = tid; it < NA; it += TC_THREADS) {
-    int rr = it & 7, rest = it >> 3;
-    int kc = rest & (TC_KC / 4 - 1), rg = rest / (TC_KC / 4);
-    float4 *p = reinterpret_cast<float4 *>(sa + rg * 2048 + kc * 128 + rr * 16);
-    float4 v = *p;
-    *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
-  }
-#pragma unroll 4
-  for (int it = tid; it < NB; it += TC_THREADS) {
-    int nr = it & 7, rest = it >> 3;
-    int kc = rest & (TC_KC / 4 - 1), ngp = rest / (TC_KC / 4);
-    float4 *p = reinterpret_cast<float4 *>(sb + ngp * 2048 + kc * 128 + nr * 16);
-    float4 v = *p;
-    *p = make_float4(to_tf32(v.x), to_tf32(v.y), to_tf32(v.z), to_tf32(v.w));
-  }
-}
-
 // overwrite == 0: C -= A B;  overwrite == 1: C = A B.  C must not alias A or B.
 // Bt = B^T (n x ldbt, K contiguous).  Persistent: CTA b handles tiles b,
 // b + gridDim.x, ... (n-tiles fastest, so neighbouring CTAs share A rows in L2).
@@ -194,9 +174,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
     const int row0 = (tile / tiles_n) * TC_BM, col0 = (tile % tiles_n) * TC_BN;
     const int st = g & 1;
     unsigned char *sa = sbase + st * TC_STAGE, *sb = sa + TC_STAGE_A;
-    // ---- this chunk's operands: wait for the copies, round to TF32
+    // ---- this chunk's operands (already TF32 values): wait for the copies
     asm volatile("cp.async.wait_all;" ::: "memory");
-    tc_round_chunk(sa, sb, tid);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -324,7 +303,18 @@ static int g_tc_state = -1;   // -1 untested, 0 disabled, 1 enabled
 static double g_tc_err = -1.0;
 static DBuf g_tc_err_flag;
 
-// Bt[c][r] = B[r][c] for r < k, c < n (32 x 32 tiles through shared memory)
+// A[r][c] <- TF32(A[r][c]) for r < m, c < k, in place
+__global__ void tc_round_kernel(float *__restrict__ A, int lda, int m, int k)
+{
+  int64_t tot = (int64_t)m * k;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    int r = (int)(i / k), c = (int)(i - (int64_t)r * k);
+    float *p = A + (size_t)r * lda + c;
+    *p = to_tf32(*p);
+  }
+}
+
+// Bt[c][r] = TF32(B[r][c]) for r < k, c < n (32 x 32 tiles through shared memory)
 __global__ void tc_transpose_kernel(const float *__restrict__ B, int ldb, int k, int n, float *__restrict__ Bt, int ldbt)
 {
   __shared__ float t[32][33];
@@ -336,7 +326,7 @@ __global__ void tc_transpose_kernel(const float *__restrict__ B, int ldb, int k,
   __syncthreads();
   for (int i = threadIdx.y; i < 32; i += 8) {
     int c = c0 + i, r = r0 + threadIdx.x;
-    if (r < k && c < n) Bt[(size_t)c * ldbt + r] = t[threadIdx.x][i];
+    if (r < k && c < n) Bt[(size_t)c * ldbt + r] = to_tf32(t[threadIdx.x][i]);
   }
 }
 
@@ -344,7 +334,7 @@ static DBuf g_tc_bt;   // B^T scratch, [n x ldbt] floats, ldbt = k rounded up to
 
 // max_ctas > 0 caps the persistent grid (the self-test uses it to make every
 // CTA loop over several tiles)
-static int launch_tc(float *C, int ldc, int m, int n, int k, const float *A, int lda, const float *B, int ldb,
+static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb,
                      cudaStream_t st, int overwrite = 0, int max_ctas = 0)
 {
   long long tiles = (long long)((n + TC_BN - 1) / TC_BN) * ((m + TC_BM - 1) / TC_BM);
@@ -357,6 +347,12 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, const float *A, int
     RB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   }
   RB_TRY(g_tc_bt.alloc((size_t)n * ldbt * sizeof(float)));
+  {
+    int64_t tot = (int64_t)m * k;
+    int nb = (int)std::min<int64_t>((tot + 255) / 256, 148 * 16);
+    tc_round_kernel<<<std::max(nb, 1), 256, 0, st>>>(A, lda, m, k);
+    RB_TRY(check_launch("tc_round_kernel"));
+  }
   tc_transpose_kernel<<<dim3((n + 31) / 32, (k + 31) / 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, g_tc_bt.as<float>(), ldbt);
   RB_TRY(check_launch("tc_transpose_kernel"));
   int grid = (int)std::min<long long>(tiles, max_ctas > 0 ? max_ctas : nsm);
@@ -433,7 +429,7 @@ static int tc_selftest()
   return 0;
 }
 
-int tc_gemm_f32(float *C, int ldc, int m, int n, int k, const float *A, int lda, const float *B, int ldb, cudaStream_t st,
+int tc_gemm_f32(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb, cudaStream_t st,
                 int *used, int overwrite)
 {
   *used = 0;

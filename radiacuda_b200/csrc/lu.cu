@@ -227,13 +227,13 @@ static int copy2d(T *dst, int ldd, const T *src, int lds, int rows, int cols, cu
 }
 
 template <typename T>
-static int gemm(T *C, int ldc, int m, int n, int k, const T *A, int lda, const T *B, int ldb, int overwrite, cudaStream_t st,
+static int gemm(T *C, int ldc, int m, int n, int k, T *A, int lda, const T *B, int ldb, int overwrite, cudaStream_t st,
                 int *tc_used)
 {
   if (m <= 0 || n <= 0) return 0;
   if (sizeof(T) == 4) {
     int used = 0;
-    RB_TRY(tc_gemm_f32((float *)C, ldc, m, n, k, (const float *)A, lda, (const float *)B, ldb, st, &used, overwrite));
+    RB_TRY(tc_gemm_f32((float *)C, ldc, m, n, k, (float *)A, lda, (const float *)B, ldb, st, &used, overwrite));
     if (used) { *tc_used = 1; return 0; }
   }
   dim3 grid((n + 63) / 64, (m + 63) / 64);
@@ -360,8 +360,8 @@ static int lu_solve_t(const T *A, const T *Linv, const T *Uinv, int n3, int ld, 
 
 // Optional CUDA-event timing of the trailing updates (A22 -= L21 U12) on the
 // stream they are launched on: radb200_update_timing(1) starts collecting,
-// radb200_update_stats() returns launches, summed device time and algorithmic
-// bytes (C read + written, panels read once) since then.
+// radb200_update_stats() returns launches, summed device time, algorithmic
+// bytes (C read + written, panels read once) and flops (2 m^2 K) since then.
 struct UpdEvents {
   std::vector<cudaEvent_t> ev;
   int used = 0;
@@ -378,7 +378,7 @@ struct UpdEvents {
 };
 static int g_update_timing = 0;
 static UpdEvents g_upd_ev;
-static double g_upd_bytes = 0.0;
+static double g_upd_bytes = 0.0, g_upd_flops = 0.0;
 
 // Two-level right-looking LU.  Outer panels of LU_OUTER columns; inside a
 // panel, 128-wide steps (diagonal block, L21 = A21 U^-1, the panel's own
@@ -454,6 +454,7 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
       g_upd_ev.used++;
       // algorithmic bytes: C read + written, the L and U panels read once
       g_upd_bytes += (double)sizeof(T) * (2.0 * mT * mT + 2.0 * mT * NBe);
+      g_upd_flops += 2.0 * mT * mT * NBe;
     }
     RB_TRY(phase(3));
   }
@@ -608,10 +609,11 @@ extern "C" RADB200_API int radb200_update_timing(int on)
   rb::g_update_timing = on;
   rb::g_upd_ev.used = 0;
   rb::g_upd_bytes = 0.0;
+  rb::g_upd_flops = 0.0;
   return 0;
 }
 
-extern "C" RADB200_API int radb200_update_stats(int64_t *launches, double *seconds, double *bytes)
+extern "C" RADB200_API int radb200_update_stats(int64_t *launches, double *seconds, double *bytes, double *flops)
 {
   RB_CUDA(cudaDeviceSynchronize());
   double ms_total = 0.0;
@@ -623,5 +625,6 @@ extern "C" RADB200_API int radb200_update_stats(int64_t *launches, double *secon
   *launches = rb::g_upd_ev.used;
   *seconds = 1e-3 * ms_total;
   *bytes = rb::g_upd_bytes;
+  *flops = rb::g_upd_flops;
   return 0;
 }

@@ -9,6 +9,19 @@
 
 namespace rb {
 
+// cuboid only: Q at q (object frame) of rectangular record idx
+__device__ __forceinline__ void cuboid_tensor(const GeomView &g, int idx, V3<double> q, double *Q)
+{
+  const double *r = g.rec + (size_t)idx * RADB200_REC_STRIDE;
+  V3<double> qc = mk3<double>(q.x - __ldg(r + 0), q.y - __ldg(r + 1), q.z - __ldg(r + 2));
+  V3<double> hd = mk3<double>(0.5 * __ldg(r + 3), 0.5 * __ldg(r + 4), 0.5 * __ldg(r + 5));
+  V3<double> Tt, Ss;
+  cuboid_TS<double>(qc, hd, g.g, Tt, Ss);
+  Q[0] = Tt.x;  Q[1] = -Ss.z; Q[2] = -Ss.y;
+  Q[3] = -Ss.z; Q[4] = Tt.y;  Q[5] = -Ss.x;
+  Q[6] = -Ss.y; Q[7] = -Ss.x; Q[8] = Tt.z;
+}
+
 __device__ __forceinline__ void elem_tensor(const GeomView &g, int kind, int idx, V3<double> q, double *Q)
 {
   if (kind == 0) {
