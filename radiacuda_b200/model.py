@@ -154,6 +154,16 @@ class Material:
         return chi, mr.copy()
 
     def record(self, magn) -> np.ndarray:
+        if self.kind == 0 and self.mr is not None:
+            # independent of the element's magnetization: computed once
+            cached = getattr(self, "_rec_cache", None)
+            if cached is None:
+                cached = self._record(None)
+                object.__setattr__(self, "_rec_cache", cached)
+            return cached.copy()
+        return self._record(magn)
+
+    def _record(self, magn) -> np.ndarray:
         r = np.zeros(MAT_STRIDE)
         if self.kind == 0:
             chi, mr = self.resolve(magn)
@@ -392,13 +402,23 @@ class Packed:
         self.bkg: List[np.ndarray] = []
         self.bkg_img: List[Tuple[int, int]] = []
         self.abs_rand = self.rel_rand = self.zero_rand = 0.0
+        # leaves with the same transform chain (the same Trf objects, e.g. all
+        # the untransformed members of a mesh) share one run of image records
+        self._chains: Dict[tuple, Tuple[int, int, List["Trf"]]] = {}
+        self.last_images: List["Trf"] = []
 
     def _images(self, trf_list) -> Tuple[int, int]:
-        ims = images_of(trf_list)
-        first = len(self.trf)
-        for t in ims:
-            self.trf.append(t.record())
-        return first, len(ims)
+        key = tuple((mult, id(t)) for mult, t in trf_list)
+        hit = self._chains.get(key)
+        if hit is None:
+            ims = images_of(trf_list)
+            first = len(self.trf)
+            for t in ims:
+                self.trf.append(t.record())
+            hit = (first, len(ims), ims)
+            self._chains[key] = hit
+        self.last_images = hit[2]
+        return hit[0], hit[1]
 
     def add_leaf(self, leaf: Leaf, magn=None) -> Tuple[int, int]:
         """Returns (source kind, index) with kind 0 rec, 1 poly, 2 arc, 3 bkg."""
@@ -495,6 +515,7 @@ def pack_interaction(objs, handle, srcobj, rand) -> InteractionPack:
             elem_src.append((kind, idx))
             mat = o.mat
             rec = mat.record(o.m)
+            # the main image of this element: first image of its chain
             if mat.kind == 2:
                 rec[0] = len(mh_rows)
                 rec[1] = mat.table.shape[0]
@@ -502,7 +523,7 @@ def pack_interaction(objs, handle, srcobj, rand) -> InteractionPack:
             mat_kind.append(mat.kind)
             mats.append(rec)
             relax_leaves.append(lf)
-            mains.append(images_of(lf.trf_list)[0])
+            mains.append(pe.last_images[0])
         else:
             px.add_leaf(lf)
             n_ext += 1

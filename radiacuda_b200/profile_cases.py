@@ -4,6 +4,7 @@
     python -m radiacuda_b200.profile_cases assemble [--tets N]
     python -m radiacuda_b200.profile_cases lu       [--tets N] [--mode 0|1]
     python -m radiacuda_b200.profile_cases relax    [--blocks N]
+    python -m radiacuda_b200.profile_cases adjoint  [--pairs N] [--points P]
 
 Each case builds a seeded model of the benchmark's shapes (tetrahedral mesh
 of chi = 1000 material, magnet array) at a size that keeps one launch of the
@@ -29,7 +30,8 @@ def _models():
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["field", "assemble", "lu", "relax"])
+    ap.add_argument("case", choices=["field", "assemble", "lu", "relax", "adjoint"])
+    ap.add_argument("--pairs", type=int, default=20)
     ap.add_argument("--tets", type=int, default=20000)
     ap.add_argument("--points", type=int, default=20000)
     ap.add_argument("--blocks", type=int, default=16)
@@ -58,6 +60,15 @@ def main(argv=None):
             t0 = time.perf_counter()
             st = rad.RlxAuto(im, 1e-13, 200, 12 if a.mode == 0 else 13)
             print("lu mode", a.mode, time.perf_counter() - t0, "s", st)
+    elif a.case == "adjoint":
+        from .adjoint import FieldProblem
+        h = MD.hybrid_undulator(rad, n_pairs=a.pairs)[0]
+        P = MD.hybrid_points(a.points, n_pairs=a.pairs)
+        prob = FieldProblem(h, P, "b", prec=1e-12)
+        prob.forward()
+        t0 = time.perf_counter()
+        prob.backward(np.random.default_rng(1).normal(size=P.shape))
+        print("adjoint", prob.n, "elements", P.shape[0], "points", time.perf_counter() - t0, "s", prob.last_timing)
     else:
         h = MD.magnet_array(rad, nside=int(np.sqrt(a.blocks)), div=3)
         im = rad.RlxPre(h)
