@@ -138,6 +138,17 @@ struct Intrc {
   int has_ext = 0;
   std::vector<int> h_elem_src;        // [2n]
   std::vector<double> h_obsJ;         // [9n] row-major
+  // the triangular solves with the current factors, captured once as CUDA
+  // graphs ([0] A^-1, [1] A^-T) acting on lu_gx; dropped when the factors change
+  cudaGraphExec_t lu_graph[2] = {nullptr, nullptr};
+  long long lu_graph_kernels[2] = {0, 0};  // kernels per replay (launch counter)
+  DBuf lu_gx;
+  void drop_lu_graphs()
+  {
+    for (auto &g : lu_graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  }
+  ~Intrc() { drop_lu_graphs(); }
 };
 
 // ---- small vector helpers (relax.cu) ---------------------------------------

@@ -73,24 +73,27 @@ __global__ void apply_A_kernel(const double *__restrict__ x, const double *__res
 }
 
 // ---- diagonal block: factor (unpivoted) and invert both triangles ----------
-// The block lives in shared memory at row pitch nb + 1 (so that threads
-// reading different rows at one column hit different banks).
+// One CTA of 1024 threads; the block lives in shared memory at row pitch
+// nb + 1 (threads reading different rows at one column hit different banks).
 //   factor:  for k: scale column k below the pivot, rank-1 update of the
 //            trailing block (warp per row, lanes across columns);
 //   invert:  in place, L^-1 column by column from the right (unit lower,
 //            Linv[i][j] = -(L[i][j] + sum_{j<q<i} Linv[i][q] L[q][j])) by
-//            threads 0..127, and U^-1 column by column from the left
+//            threads 0..511, and U^-1 column by column from the left
 //            (Uinv[i][j] = -sum_{i<=q<j} Uinv[i][q] U[q][j] / U[j][j]) by
-//            threads 128..255, each column copied aside first.
+//            threads 512..1023: 4 threads per row split the inner product;
+//            each column is copied aside first.
+constexpr int DIAG_T = 1024;
+
 template <typename T>
-__global__ void __launch_bounds__(256) diag_factor_kernel(T *__restrict__ A, int ld, int k0, int nb, T *__restrict__ Linv,
-                                                          T *__restrict__ Uinv, int *__restrict__ err)
+__global__ void __launch_bounds__(DIAG_T) diag_factor_kernel(T *__restrict__ A, int ld, int k0, int nb, T *__restrict__ Linv,
+                                                             T *__restrict__ Uinv, int *__restrict__ err)
 {
   extern __shared__ double sblk[];  // nb x (nb + 1)
   __shared__ double colL[LU_NB], colU[LU_NB];
   const int P = nb + 1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
+  for (int e = tid; e < nb * nb; e += DIAG_T) {
     int r = e / nb, c = e - r * nb;
     sblk[r * P + c] = (double)A[(size_t)(k0 + r) * ld + k0 + c];
   }
@@ -99,7 +102,7 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(T *__restrict__ A, int
     const double piv = sblk[k * P + k];
     if (tid == 0 && !(fabs(piv) > 1e-300)) err[0] = 1;
     const double ip = 1.0 / piv;
-    for (int r = k + 1 + warp; r < nb; r += 8) {
+    for (int r = k + 1 + warp; r < nb; r += DIAG_T / 32) {
       const double l = sblk[r * P + k] * ip;
       __syncwarp();
       for (int c = k + 1 + lane; c < nb; c += 32) sblk[r * P + c] -= l * sblk[k * P + c];
@@ -107,13 +110,14 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(T *__restrict__ A, int
     }
     __syncthreads();
   }
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
+  for (int e = tid; e < nb * nb; e += DIAG_T) {
     int r = e / nb, c = e - r * nb;
     A[(size_t)(k0 + r) * ld + k0 + c] = (T)sblk[r * P + c];
   }
   __syncthreads();
-  const bool lower = tid < 128;
-  const int t = tid & 127;
+  const bool lower = tid < DIAG_T / 2;
+  const int t = tid & (DIAG_T / 2 - 1);
+  const int i = t >> 2, sub = t & 3;  // row and its quarter of the inner product
   for (int s = 0; s < nb; s++) {
     const int jl = nb - 1 - s, ju = s;
     if (lower) {
@@ -122,35 +126,35 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(T *__restrict__ A, int
       colU[t] = sblk[t * P + ju];
     }
     __syncthreads();
+    double acc = 0.0;
     if (lower) {
-      const int i = t;
-      if (i > jl && i < nb) {
-        double acc = colL[i];
-        for (int q = jl + 1; q < i; q++) acc += sblk[i * P + q] * colL[q];
-        sblk[i * P + jl] = -acc;
-      }
-    } else {
-      const int i = t;
-      const double d = 1.0 / colU[ju];
-      if (i < ju) {
-        double acc = 0.0;
-        for (int q = i; q < ju; q++) acc += sblk[i * P + q] * colU[q];
-        sblk[i * P + ju] = -acc * d;
-      } else if (i == ju) {
-        sblk[i * P + ju] = d;
+      if (i > jl && i < nb)
+        for (int q = jl + 1 + sub; q < i; q += 4) acc += sblk[i * P + q] * colL[q];
+    } else if (i < ju) {
+      for (int q = i + sub; q < ju; q += 4) acc += sblk[i * P + q] * colU[q];
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    if (sub == 0) {
+      if (lower) {
+        if (i > jl && i < nb) sblk[i * P + jl] = -(colL[i] + acc);
+      } else {
+        const double d = 1.0 / colU[ju];
+        if (i < ju) sblk[i * P + ju] = -acc * d;
+        else if (i == ju) sblk[i * P + ju] = d;
       }
     }
     __syncthreads();
   }
-  for (int e = tid; e < nb * LU_NB; e += blockDim.x) {
-    int i = e / LU_NB, j = e - i * LU_NB;
+  for (int e = tid; e < nb * LU_NB; e += DIAG_T) {
+    int ii = e / LU_NB, j = e - ii * LU_NB;
     double l = 0.0, u = 0.0;
     if (j < nb) {
-      l = (i > j) ? sblk[i * P + j] : (i == j ? 1.0 : 0.0);
-      u = (i <= j) ? sblk[i * P + j] : 0.0;
+      l = (ii > j) ? sblk[ii * P + j] : (ii == j ? 1.0 : 0.0);
+      u = (ii <= j) ? sblk[ii * P + j] : 0.0;
     }
-    Linv[(size_t)(k0 + i) * LU_NB + j] = (T)l;
-    Uinv[(size_t)(k0 + i) * LU_NB + j] = (T)u;
+    Linv[(size_t)(k0 + ii) * LU_NB + j] = (T)l;
+    Uinv[(size_t)(k0 + ii) * LU_NB + j] = (T)u;
   }
 }
 
@@ -414,7 +418,7 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
     // ---- factor the panel columns [K0, pend) over rows [K0, n3)
     for (int j0 = K0; j0 < pend; j0 += LU_NB) {
       const int jb = std::min(LU_NB, pend - j0);
-      diag_factor_kernel<T><<<1, 256, (size_t)jb * (jb + 1) * sizeof(double), st>>>(A, ld, j0, jb, Linv, Uinv, d_err);
+      diag_factor_kernel<T><<<1, DIAG_T, (size_t)jb * (jb + 1) * sizeof(double), st>>>(A, ld, j0, jb, Linv, Uinv, d_err);
       RB_TRY(check_launch("diag_factor_kernel"));
       RB_TRY(phase(0));
       const int rest = j0 + jb, m = n3 - rest;
@@ -490,27 +494,66 @@ static int lu_solve(const T *A, const T *Linv, const T *Uinv, int n3, int ld, do
   return 0;
 }
 
-int lu_precond(Intrc &I, double *x, cudaStream_t st)
+static int lu_solve_direct(Intrc &I, int transposed, double *x, cudaStream_t st)
 {
-  if (I.lu_mode == RADB200_LU_F64)
-    return lu_solve<double>(I.LU64.as<double>(), I.LUinv.as<double>(), I.LUinv.as<double>() + (size_t)I.n3 * LU_NB, I.n3,
-                            I.ld, x, st);
-  return lu_solve<float>(I.LU32.as<float>(), I.LUinv.as<float>(), I.LUinv.as<float>() + (size_t)I.n3 * LU_NB, I.n3, I.ld,
-                         x, st);
-}
-
-// x <- A^-T x with the kept factors (the adjoint's preconditioner)
-int lu_precond_transposed(Intrc &I, double *x, cudaStream_t st)
-{
-  if (I.lu_mode == RADB200_LU_F64)
-    return lu_solve_t<double>(I.LU64.as<double>(), I.LUinv.as<double>(), I.LUinv.as<double>() + (size_t)I.n3 * LU_NB, I.n3,
-                              I.ld, x, st);
-  if (I.lu_mode == RADB200_LU_TF32)
-    return lu_solve_t<float>(I.LU32.as<float>(), I.LUinv.as<float>(), I.LUinv.as<float>() + (size_t)I.n3 * LU_NB, I.n3,
-                             I.ld, x, st);
+  const int n3 = I.n3, ld = I.ld;
+  if (I.lu_mode == RADB200_LU_F64) {
+    const double *L = I.LUinv.as<double>(), *U = L + (size_t)n3 * LU_NB;
+    return transposed ? lu_solve_t<double>(I.LU64.as<double>(), L, U, n3, ld, x, st)
+                      : lu_solve<double>(I.LU64.as<double>(), L, U, n3, ld, x, st);
+  }
+  if (I.lu_mode == RADB200_LU_TF32) {
+    const float *L = I.LUinv.as<float>(), *U = L + (size_t)n3 * LU_NB;
+    return transposed ? lu_solve_t<float>(I.LU32.as<float>(), L, U, n3, ld, x, st)
+                      : lu_solve<float>(I.LU32.as<float>(), L, U, n3, ld, x, st);
+  }
   set_error("no LU factors on this interaction");
   return RADB200_E_ARG;
 }
+
+// x <- A^-1 x (or A^-T x) with the kept factors.  The ~4 n / 128 small
+// launches of the block sweeps are captured once per factorization into a
+// CUDA graph on a fixed buffer and replayed: one launch per application.
+static int lu_apply(Intrc &I, int transposed, double *x, cudaStream_t st)
+{
+  cudaGraphExec_t &ex = I.lu_graph[transposed];
+  if (!ex) {
+    RB_TRY(I.lu_gx.alloc((size_t)I.ld * sizeof(double)));
+    cudaStream_t cs;
+    RB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    int rc = 0;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess) {
+      const long long before = g_launches;
+      rc = lu_solve_direct(I, transposed, I.lu_gx.as<double>(), cs);
+      I.lu_graph_kernels[transposed] = g_launches - before;
+      g_launches = before;  // captured, not launched
+      e = cudaStreamEndCapture(cs, &graph);
+      if (e == cudaSuccess && rc == 0) e = cudaGraphInstantiate(&ex, graph, 0);
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    if (rc) return rc;
+    if (e != cudaSuccess) {
+      // no graph: run the sweeps directly (same kernels, launched one by one)
+      cudaGetLastError();
+      ex = nullptr;
+      return lu_solve_direct(I, transposed, x, st);
+    }
+  }
+  const size_t bytes = (size_t)I.n3 * sizeof(double);
+  RB_CUDA(cudaMemcpyAsync(I.lu_gx.p, x, bytes, cudaMemcpyDeviceToDevice, st));
+  RB_CUDA(cudaGraphLaunch(ex, st));
+  g_launches += I.lu_graph_kernels[transposed];
+  RB_CUDA(cudaMemcpyAsync(x, I.lu_gx.p, bytes, cudaMemcpyDeviceToDevice, st));
+  return 0;
+}
+
+int lu_precond(Intrc &I, double *x, cudaStream_t st) { return lu_apply(I, 0, x, st); }
+
+// x <- A^-T x with the kept factors (the adjoint's preconditioner)
+int lu_precond_transposed(Intrc &I, double *x, cudaStream_t st) { return lu_apply(I, 1, x, st); }
 
 struct LinOp : Op {
   Intrc &I;
@@ -536,6 +579,7 @@ int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_sec
   auto t0 = std::chrono::steady_clock::now();
   const int n3 = I.n3, ld = I.ld;
   I.lu_mode = -1;
+  I.drop_lu_graphs();
   DBuf err;
   RB_TRY(err.alloc(sizeof(int)));
   RB_CUDA(cudaMemset(err.p, 0, sizeof(int)));
