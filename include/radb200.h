@@ -140,9 +140,9 @@ RADB200_API int radb200_update_stats(int64_t *launches, double *seconds, double 
  * roofline denominator of the transcendental-bound assembly / field kernels. */
 RADB200_API int radb200_measure_fma_peak(int fp64, double *tflops);
 /* Diagnostics, no counterpart in the reference: runs (once) the self-test of
- * the tcgen05 TF32 trailing-update kernel of the LU against a CUDA-core GEMM.
- * state: 0 tensor-core path disabled, 1 / 2 enabled (shared-memory layout
- * variant of the B operand); err: max relative deviation seen.              */
+ * the tcgen05 TF32 GEMM kernels of the LU against a CUDA-core GEMM.
+ * state: 0 tensor-core path disabled, 1 the cp.async-fed kernel in use,
+ * 2 the TMA-fed kernel in use; err: max relative deviation seen.            */
 RADB200_API int radb200_tc_selftest(int *state, double *err);
 
 /* ---- field evaluation ------------------------------------------------------

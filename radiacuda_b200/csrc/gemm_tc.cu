@@ -31,6 +31,7 @@
 // The first use runs a self-test against the CUDA-core GEMM (ragged m, n, k,
 // several tiles and chunks per CTA) and keeps the tensor-core path only if it
 // agrees to TF32 accuracy.
+#include <cuda.h>
 #include <math.h>
 #include <stdlib.h>
 
@@ -288,6 +289,220 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
 }
 
+// ---- TMA variant ---------------------------------------------------------------
+// Same tiles and epilogue, but the operands come in by TMA: per K chunk of 32
+// one 2-D bulk tensor load of A (32 x 128) and one of B^T (32 x 256), written
+// by the copy engine in the 128-byte-swizzled K-major layout (8-row x 128-byte
+// atoms, 1024-byte aligned) and completed on the stage's "full" mbarrier with
+// a transaction count.  One lane of warp 0 issues the loads and the MMAs
+// through TM_NST stages (loads run TM_NST - 1 chunks ahead; a stage is
+// refilled once the MMAs that read it have committed to its "empty"
+// mbarrier); all 8 warps load C and write the results.  Descriptors: start
+// address of the atom + 32 bytes per K=8 step, SBO 1024, layout 128B swizzle.
+constexpr int TM_KC = 32;
+constexpr int TM_NST = 4;
+constexpr int TM_STAGE_A = TC_BM * TM_KC * 4;   // 16 KB
+constexpr int TM_STAGE_B = TC_BN * TM_KC * 4;   // 32 KB
+constexpr int TM_STAGE = TM_STAGE_A + TM_STAGE_B;
+constexpr int TM_SMEM = TM_NST * TM_STAGE + 1024;
+
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
+{
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;             // leading byte offset: not used by swizzled K-major operands
+  d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset: 8 rows x 128 bytes
+  d |= (uint64_t)1 << 46;             // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;             // layout: 128-byte swizzle
+  return d;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar)
+{
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ int tm_wait(uint32_t bar, uint32_t parity)
+{
+  uint32_t done = 0;
+  long long spins = 0;
+  while (!done) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (!done && ++spins > TC_SPIN_LIMIT) return 0;
+  }
+  return 1;
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_update_tma_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                                      const __grid_constant__ CUtensorMap tmB,
+                                                                      float *__restrict__ C, int ldc, int m, int n, int k,
+                                                                      int *__restrict__ err, int overwrite)
+{
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *sbase = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ uint64_t full[TM_NST], empty[TM_NST];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int timed_out;
+  __shared__ int abort_cta;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles_n = (n + TC_BN - 1) / TC_BN, tiles_m = (m + TC_BM - 1) / TC_BM;
+  const int ntiles = tiles_n * tiles_m;
+  const int nch = (k + TM_KC - 1) / TM_KC;
+  if (tid == 0) abort_cta = *(volatile int *)err;
+  __syncthreads();
+  if (abort_cta != 0 || (int)blockIdx.x >= ntiles || nch < 1) return;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)), "r"(TC_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int b = 0; b < TM_NST; b++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[b])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[b])));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    timed_out = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t s0 = smem_u32(sbase);
+  const int my_tiles = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int G = my_tiles * nch;
+  const int q = warp & 3, hc = warp >> 2;
+  const int r = q * 32 + lane;
+  float4 cv[32];
+  int issued = 0, consumed = 0;  // lane 0 of warp 0 only
+
+  auto issue = [&](int gg) {
+    const int ii = gg / nch, cc = gg - ii * nch;
+    const int tt = blockIdx.x + ii * gridDim.x;
+    const uint32_t so = s0 + (gg % TM_NST) * TM_STAGE, fb = smem_u32(&full[gg % TM_NST]);
+    mbar_expect_tx(fb, (uint32_t)TM_STAGE);
+    tma_load_2d(so, &tmA, cc * TM_KC, (tt / tiles_n) * TC_BM, fb);
+    tma_load_2d(so + TM_STAGE_A, &tmB, cc * TM_KC, (tt % tiles_n) * TC_BN, fb);
+  };
+  if (tid == 0)
+    for (; issued < TM_NST - 1 && issued < G; issued++) issue(issued);
+
+  for (int g = 0; g < G; g++) {
+    const int i = g / nch, c = g - i * nch;
+    const int tile = blockIdx.x + i * gridDim.x;
+    const int row0 = (tile / tiles_n) * TC_BM, col0 = (tile % tiles_n) * TC_BN;
+    const int st = g % TM_NST;
+    // ---- first chunk of a tile: this thread's C values (row r, 128 columns)
+    if (c == 0) {
+      const int gr = row0 + r, gcb = col0 + hc * 128;
+#pragma unroll
+      for (int j = 0; j < 32; j++) {
+        int gc = gcb + 4 * j;
+        cv[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!overwrite && gr < m) {
+          const float *src = C + (size_t)gr * ldc + gc;
+          if (gc + 3 < n) cv[j] = *reinterpret_cast<const float4 *>(src);
+          else if (gc < n) {
+            cv[j].x = src[0];
+            if (gc + 1 < n) cv[j].y = src[1];
+            if (gc + 2 < n) cv[j].z = src[2];
+          }
+        }
+      }
+    }
+    // ---- lane 0 of warp 0: MMAs of chunk g, then the loads of chunk g + TM_NST - 1
+    if (warp == 0) {
+      if (lane == 0 && !timed_out) {
+        if (!tm_wait(smem_u32(&full[st]), (uint32_t)((g / TM_NST) & 1))) {
+          timed_out = 1;
+        } else {
+          consumed++;
+          const uint32_t idesc = umma_idesc(0);
+          const uint32_t ua = s0 + st * TM_STAGE, ub = ua + TM_STAGE_A;
+#pragma unroll
+          for (int s = 0; s < TM_KC / 8; s++) {
+            uint64_t da = umma_desc_sw128(ua + 32u * s);
+            uint64_t db = umma_desc_sw128(ub + 32u * s);
+            uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           smem_u32(&empty[st]))
+                       : "memory");
+          if (issued < G) {
+            // the stage of chunk issued - TM_NST must be free: its MMAs committed
+            const int old = issued - TM_NST;
+            if (old >= 0 && !tm_wait(smem_u32(&empty[old % TM_NST]), (uint32_t)((old / TM_NST) & 1))) timed_out = 1;
+            else issue(issued++);
+          }
+        }
+      }
+      __syncwarp();
+    }
+    if (c != nch - 1) continue;
+
+    // ---- last chunk of the tile: accumulators complete, then TMEM -> registers -> C
+    if (!timed_out && !tm_wait(smem_u32(&empty[st]), (uint32_t)((g / TM_NST) & 1))) timed_out = 1;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (timed_out) break;
+    const int gr = row0 + r, gcb = col0 + hc * 128;
+#pragma unroll
+    for (int cb = 0; cb < 128; cb += 16) {
+      uint32_t v[16];
+      uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(hc * 128 + cb);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+            "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (gr < m) {
+#pragma unroll
+        for (int j4 = 0; j4 < 4; j4++) {
+          const int j = cb / 4 + j4;
+          const int gc = gcb + 4 * j;
+          float4 t = make_float4(__uint_as_float(v[4 * j4]), __uint_as_float(v[4 * j4 + 1]), __uint_as_float(v[4 * j4 + 2]),
+                                 __uint_as_float(v[4 * j4 + 3]));
+          float4 o = overwrite ? t : make_float4(cv[j].x - t.x, cv[j].y - t.y, cv[j].z - t.z, cv[j].w - t.w);
+          float *dst = C + (size_t)gr * ldc + gc;
+          if (gc + 3 < n) *reinterpret_cast<float4 *>(dst) = o;
+          else if (gc < n) {
+            dst[0] = o.x;
+            if (gc + 1 < n) dst[1] = o.y;
+            if (gc + 2 < n) dst[2] = o.z;
+          }
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  // after a timeout: wait (bounded) for bulk copies still in flight before the CTA exits
+  if (tid == 0)
+    for (int j = consumed; j < issued; j++) tm_wait(smem_u32(&full[j % TM_NST]), (uint32_t)((j / TM_NST) & 1));
+  if (timed_out && tid == 0) atomicExch(err, 2);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+}
+
 // CUDA-core reference for the self-test: C -= A B or C = A B (FP32 inputs
 // rounded to TF32 like the tensor path)
 __global__ void tc_ref_kernel(float *C, int ld, int m, int n, int k, const float *A, const float *B, int overwrite)
@@ -300,6 +515,7 @@ __global__ void tc_ref_kernel(float *C, int ld, int m, int n, int k, const float
 }
 
 static int g_tc_state = -1;   // -1 untested, 0 disabled, 1 enabled
+static int g_tc_tma = 0;      // 1: the TMA-fed kernel passed the self-test and is used
 static double g_tc_err = -1.0;
 static DBuf g_tc_err_flag;
 
@@ -334,9 +550,51 @@ static DBuf g_tc_bt;   // B^T scratch, [n x ldbt] floats, ldbt = k rounded up to
 
 // max_ctas > 0 caps the persistent grid (the self-test uses it to make every
 // CTA loop over several tiles)
-static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb,
-                     cudaStream_t st, int overwrite = 0, int max_ctas = 0)
+typedef CUresult (*TensorMapEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda)
+static TensorMapEncodeFn tensor_map_encoder()
 {
+  static TensorMapEncodeFn fn = nullptr;
+  static int tried = 0;
+  if (!tried) {
+    tried = 1;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (TensorMapEncodeFn)p;
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+// 2-D FP32 map of a row-major rows x cols matrix (pitch ld floats), boxes of
+// 32 columns x box_rows rows, 128-byte swizzle, zero fill outside
+static int encode_map(CUtensorMap *map, const float *base, int rows, int cols, int ld, int box_rows)
+{
+  TensorMapEncodeFn enc = tensor_map_encoder();
+  if (!enc) return RADB200_E_UNSUPPORTED;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
+  cuuint32_t box[2] = {(cuuint32_t)TM_KC, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("tensor map encoding failed (%d)", (int)r);
+    return RADB200_E_UNSUPPORTED;
+  }
+  return 0;
+}
+
+static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb,
+                     cudaStream_t st, int overwrite = 0, int max_ctas = 0, int use_tma = -1)
+{
+  if (use_tma < 0) use_tma = g_tc_tma;
   long long tiles = (long long)((n + TC_BN - 1) / TC_BN) * ((m + TC_BM - 1) / TC_BM);
   if (tiles > (1ll << 30) || k < 1 || k > (1 << 20)) { set_error("tensor-core update shape out of range"); return RADB200_E_ARG; }
   const int ldbt = (k + 3) / 4 * 4;
@@ -356,6 +614,14 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
   tc_transpose_kernel<<<dim3((n + 31) / 32, (k + 31) / 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, g_tc_bt.as<float>(), ldbt);
   RB_TRY(check_launch("tc_transpose_kernel"));
   int grid = (int)std::min<long long>(tiles, max_ctas > 0 ? max_ctas : nsm);
+  if (use_tma) {
+    CUtensorMap ma, mb;
+    RB_TRY(encode_map(&ma, A, m, k, lda, TC_BM));
+    RB_TRY(encode_map(&mb, g_tc_bt.as<float>(), n, k, ldbt, TC_BN));
+    RB_CUDA(cudaFuncSetAttribute(tc_update_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TM_SMEM));
+    tc_update_tma_kernel<<<grid, TC_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(), overwrite);
+    return check_launch("tc_update_tma_kernel");
+  }
   RB_CUDA(cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
   tc_update_kernel<<<grid, TC_THREADS, TC_SMEM, st>>>(C, ldc, m, n, k, A, lda, g_tc_bt.as<float>(), ldbt,
                                                       g_tc_err_flag.as<int>(), overwrite);
@@ -367,7 +633,7 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
 // on 2 CTAs, so each CTA loops over several tiles and K chunks; returns the
 // relative max deviation from the CUDA-core reference in *err, or sets
 // *timeout when an MMA completion wait ran out.
-static int tc_selftest_case(int m, int n, int k, int overwrite, double *err, int *timeout)
+static int tc_selftest_case(int m, int n, int k, int overwrite, int use_tma, double *err, int *timeout)
 {
   const int ld = ((k + n + 3) / 4) * 4;
   std::vector<float> h((size_t)(m + k) * ld);
@@ -383,7 +649,12 @@ static int tc_selftest_case(int m, int n, int k, int overwrite, double *err, int
   tc_ref_kernel<<<dim3((n + 127) / 128, m), 128>>>(Cr, ld, m, n, k, Ar, Br, overwrite);
   RB_TRY(check_launch("tc_ref_kernel"));
   RB_CUDA(cudaMemset(g_tc_err_flag.p, 0, sizeof(int)));
-  int rc = launch_tc(C, ld, m, n, k, A, ld, Bm, ld, 0, overwrite, 2);
+  int rc = launch_tc(C, ld, m, n, k, A, ld, Bm, ld, 0, overwrite, 2, use_tma);
+  if (rc == RADB200_E_UNSUPPORTED) {  // no tensor-map encoder: nothing was launched
+    *err = 1.0;
+    *timeout = 0;
+    return 0;
+  }
   cudaError_t e = cudaDeviceSynchronize();
   if (rc != 0 || e != cudaSuccess) {
     cudaGetLastError();
@@ -406,26 +677,34 @@ static int tc_selftest_case(int m, int n, int k, int overwrite, double *err, int
 }
 
 // Keeps the tensor-core path only if every case matches the CUDA-core
-// reference to TF32 accuracy: K of 2 chunks (120) and of 5 (300), ragged m
-// and n, and the overwrite form the LU panels use.
+// reference to TF32 accuracy: K of 4 chunks of 32 (120) and of 10 (300),
+// ragged m and n, and the overwrite form the LU panels use.  The cp.async-fed
+// kernel is tested first; the TMA-fed kernel is then tested on the same cases
+// and used only if it passes them all.
 static int tc_selftest()
 {
   RB_TRY(g_tc_err_flag.alloc(sizeof(int)));
   g_tc_state = 0;
+  g_tc_tma = 0;
   g_tc_err = 0.0;
   const int cases[3][4] = {{300, 400, 120, 0}, {300, 300, 300, 0}, {260, 290, 64, 1}};
-  for (auto &cs : cases) {
-    double err = 1.0;
-    int timeout = 0;
-    RB_TRY(tc_selftest_case(cs[0], cs[1], cs[2], cs[3], &err, &timeout));
-    if (timeout) {  // an MMA never completed: leave the tensor-core path off
-      set_error("tensor-core self-test: MMA completion wait timed out");
-      return 0;
+  for (int use_tma = 0; use_tma <= 1; use_tma++) {
+    double worst = 0.0;
+    for (auto &cs : cases) {
+      double err = 1.0;
+      int timeout = 0;
+      RB_TRY(tc_selftest_case(cs[0], cs[1], cs[2], cs[3], use_tma, &err, &timeout));
+      if (timeout) {  // an MMA or copy never completed: leave this kernel off
+        set_error("tensor-core self-test: a completion wait timed out (%s kernel)", use_tma ? "TMA" : "cp.async");
+        RB_CUDA(cudaMemset(g_tc_err_flag.p, 0, sizeof(int)));  // the other kernel may still run
+        return 0;
+      }
+      worst = std::max(worst, err);
     }
-    g_tc_err = std::max(g_tc_err, err);
-    if (!(err < 1e-4)) return 0;
+    if (!(worst < 1e-4)) return 0;
+    if (use_tma) g_tc_tma = 1;
+    else { g_tc_state = 1; g_tc_err = worst; }
   }
-  g_tc_state = 1;
   return 0;
 }
 
@@ -458,7 +737,7 @@ int tc_error_flag(int *flag)
 extern "C" RADB200_API int radb200_tc_selftest(int *state, double *err)
 {
   if (rb::g_tc_state < 0) RB_TRY(rb::tc_selftest());
-  *state = rb::g_tc_state;
+  *state = rb::g_tc_state + rb::g_tc_tma;  // 0 off, 1 cp.async-fed kernel, 2 TMA-fed kernel
   *err = rb::g_tc_err;
   return 0;
 }

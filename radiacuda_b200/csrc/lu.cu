@@ -511,11 +511,14 @@ static int lu_solve_direct(Intrc &I, int transposed, double *x, cudaStream_t st)
   return RADB200_E_ARG;
 }
 
-// x <- A^-1 x (or A^-T x) with the kept factors.  The ~4 n / 128 small
-// launches of the block sweeps are captured once per factorization into a
-// CUDA graph on a fixed buffer and replayed: one launch per application.
+// x <- A^-1 x (or A^-T x) with the kept factors.  For systems of 64 blocks
+// and more, the ~4 n / 128 small launches of the block sweeps are captured
+// once per factorization into a CUDA graph on a fixed buffer and replayed:
+// one launch per application.
 static int lu_apply(Intrc &I, int transposed, double *x, cudaStream_t st)
 {
+  // small systems: a few applications per factorization do not repay a capture
+  if (I.n3 < 64 * LU_NB) return lu_solve_direct(I, transposed, x, st);
   cudaGraphExec_t &ex = I.lu_graph[transposed];
   if (!ex) {
     RB_TRY(I.lu_gx.alloc((size_t)I.ld * sizeof(double)));
