@@ -237,6 +237,7 @@ static void build_topo(const RadB200Geom *G, bool tensor, HostTopo &h)
 int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs)
 {
   RB_TRY(validate_geom(G));
+  all_tets = 0;
   if (G->n_poly > 0) {
     HostTopo h;
     build_topo(G, tensor_coeffs, h);
@@ -310,6 +311,10 @@ GeomView DevGeom::view(int fast) const
 static std::map<int64_t, std::unique_ptr<Intrc>> g_intrc;
 static int64_t g_next_handle = 1;
 static DBuf g_fld_pts, g_fld_out, g_fld_scratch;
+// device copy of the sources of the last field call: its buffers are reused
+// by the next call when they are large enough (no allocation, no
+// synchronizing free per call; the library is not reentrant)
+static DevGeom g_fld_geom;
 
 Intrc *find_intrc(int64_t h)
 {
@@ -345,9 +350,8 @@ int radb200_device_sync(void)
 int radb200_field_dev(const RadB200Geom *g, const double *d_pts, int64_t npts, int what, int precision, double *d_out)
 {
   if (npts < 0 || what < 0 || what > 2 || precision < 0 || precision > 2) { set_error("bad field arguments"); return RADB200_E_ARG; }
-  DevGeom dg;
-  RB_TRY(dg.upload(g));
-  RB_TRY(launch_field(dg.view(precision != 0), d_pts, npts, what, precision == 1 ? 1 : 0, d_out, g_fld_scratch, 0));
+  RB_TRY(g_fld_geom.upload(g));
+  RB_TRY(launch_field(g_fld_geom.view(precision != 0), d_pts, npts, what, precision == 1 ? 1 : 0, d_out, g_fld_scratch, 0));
   RB_CUDA(cudaStreamSynchronize(0));
   return 0;
 }

@@ -294,11 +294,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
 // one 2-D bulk tensor load of A (32 x 128) and one of B^T (32 x 256), written
 // by the copy engine in the 128-byte-swizzled K-major layout (8-row x 128-byte
 // atoms, 1024-byte aligned) and completed on the stage's "full" mbarrier with
-// a transaction count.  One lane of warp 0 issues the loads and the MMAs
-// through TM_NST stages (loads run TM_NST - 1 chunks ahead; a stage is
+// a transaction count.  One lane of a producer warp issues the loads and the
+// MMAs through TM_NST stages (loads run TM_NST - 1 chunks ahead; a stage is
 // refilled once the MMAs that read it have committed to its "empty"
-// mbarrier); all 8 warps load C and write the results.  Descriptors: start
-// address of the atom + 32 bytes per K=8 step, SBO 1024, layout 128B swizzle.
+// mbarrier) into two alternating TMEM accumulators; 8 epilogue warps load C
+// and write the results.  Descriptors: start address of the atom + 32 bytes
+// per K=8 step, SBO 1024, layout 128B swizzle.
 constexpr int TM_KC = 32;
 constexpr int TM_NST = 4;
 constexpr int TM_STAGE_A = TC_BM * TM_KC * 4;   // 16 KB
@@ -345,14 +346,22 @@ __device__ __forceinline__ int tm_wait(uint32_t bar, uint32_t parity)
   return 1;
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_update_tma_kernel(const __grid_constant__ CUtensorMap tmA,
+constexpr int TM_THREADS = 288;  // warps 0-7: epilogue; warp 8: TMA loads and MMAs
+
+// Warp-specialised: warp 8 (one lane) streams the chunks of all of the CTA's
+// tiles through the operand stages into two TMEM accumulators (columns
+// 0-255 and 256-511, alternating per tile) and commits each finished tile to
+// that buffer's "full" barrier; warps 0-7 drain a finished buffer (C loaded
+// beforehand, C - AB stored) and arrive on its "empty" barrier, so the MMAs
+// of tile i+1 run while tile i is written back.  Every wait is bounded.
+__global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                                       const __grid_constant__ CUtensorMap tmB,
                                                                       float *__restrict__ C, int ldc, int m, int n, int k,
                                                                       int *__restrict__ err, int overwrite)
 {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *sbase = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ uint64_t full[TM_NST], empty[TM_NST];
+  __shared__ uint64_t full[TM_NST], empty[TM_NST], accf[2], acce[2];
   __shared__ uint32_t tmem_base_s;
   __shared__ int timed_out;
   __shared__ int abort_cta;
@@ -365,13 +374,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_tma_kernel(const __gr
   if (abort_cta != 0 || (int)blockIdx.x >= ntiles || nch < 1) return;
 
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)), "r"(TC_BN));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                 "r"(2 * TC_BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
     for (int b = 0; b < TM_NST; b++) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[b])));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[b])));
+    }
+    for (int b = 0; b < 2; b++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accf[b])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(smem_u32(&acce[b])));
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     timed_out = 0;
@@ -382,31 +396,75 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_tma_kernel(const __gr
   const uint32_t tmem = tmem_base_s;
   const uint32_t s0 = smem_u32(sbase);
   const int my_tiles = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
-  const int G = my_tiles * nch;
-  const int q = warp & 3, hc = warp >> 2;
-  const int r = q * 32 + lane;
-  float4 cv[32];
-  int issued = 0, consumed = 0;  // lane 0 of warp 0 only
 
-  auto issue = [&](int gg) {
-    const int ii = gg / nch, cc = gg - ii * nch;
-    const int tt = blockIdx.x + ii * gridDim.x;
-    const uint32_t so = s0 + (gg % TM_NST) * TM_STAGE, fb = smem_u32(&full[gg % TM_NST]);
-    mbar_expect_tx(fb, (uint32_t)TM_STAGE);
-    tma_load_2d(so, &tmA, cc * TM_KC, (tt / tiles_n) * TC_BM, fb);
-    tma_load_2d(so + TM_STAGE_A, &tmB, cc * TM_KC, (tt % tiles_n) * TC_BN, fb);
-  };
-  if (tid == 0)
-    for (; issued < TM_NST - 1 && issued < G; issued++) issue(issued);
-
-  for (int g = 0; g < G; g++) {
-    const int i = g / nch, c = g - i * nch;
-    const int tile = blockIdx.x + i * gridDim.x;
-    const int row0 = (tile / tiles_n) * TC_BM, col0 = (tile % tiles_n) * TC_BN;
-    const int st = g % TM_NST;
-    // ---- first chunk of a tile: this thread's C values (row r, 128 columns)
-    if (c == 0) {
+  if (warp == 8) {
+    // ---------------- producer: TMA loads and MMAs (lane 0) ----------------
+    int issued = 0, consumed = 0;
+    if (lane == 0) {
+      const int G = my_tiles * nch;
+      auto issue = [&](int gg) {
+        const int ii = gg / nch, cc = gg - ii * nch;
+        const int tt = blockIdx.x + ii * gridDim.x;
+        const uint32_t so = s0 + (gg % TM_NST) * TM_STAGE, fb = smem_u32(&full[gg % TM_NST]);
+        mbar_expect_tx(fb, (uint32_t)TM_STAGE);
+        tma_load_2d(so, &tmA, cc * TM_KC, (tt / tiles_n) * TC_BM, fb);
+        tma_load_2d(so + TM_STAGE_A, &tmB, cc * TM_KC, (tt % tiles_n) * TC_BN, fb);
+      };
+      for (; issued < TM_NST - 1 && issued < G; issued++) issue(issued);
+      const uint32_t idesc = umma_idesc(0);
+      for (int i = 0; i < my_tiles && !timed_out; i++) {
+        const int buf = i & 1;
+        // the epilogue of tile i - 2 has released this accumulator buffer
+        if (i >= 2 && !tm_wait(smem_u32(&acce[buf]), (uint32_t)(((i - 2) / 2) & 1))) { timed_out = 1; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t dacc = tmem + (uint32_t)(buf * TC_BN);
+        for (int c = 0; c < nch; c++) {
+          const int g = i * nch + c, st = g % TM_NST;
+          if (!tm_wait(smem_u32(&full[st]), (uint32_t)((g / TM_NST) & 1))) { timed_out = 1; break; }
+          consumed++;
+          const uint32_t ua = s0 + st * TM_STAGE, ub = ua + TM_STAGE_A;
+#pragma unroll
+          for (int s = 0; s < TM_KC / 8; s++) {
+            uint64_t da = umma_desc_sw128(ua + 32u * s);
+            uint64_t db = umma_desc_sw128(ub + 32u * s);
+            uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dacc),
+                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           smem_u32(&empty[st]))
+                       : "memory");
+          if (issued < G) {
+            const int old = issued - TM_NST;  // the chunk whose stage is refilled
+            if (old >= 0 && !tm_wait(smem_u32(&empty[old % TM_NST]), (uint32_t)((old / TM_NST) & 1))) {
+              timed_out = 1;
+              break;
+            }
+            issue(issued++);
+          }
+        }
+        if (timed_out) break;
+        // the tile's accumulators are complete once everything issued so far is
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&accf[buf]))
+                     : "memory");
+      }
+      // after a timeout: wait (bounded) for bulk copies still in flight
+      for (int j = consumed; j < issued; j++) tm_wait(smem_u32(&full[j % TM_NST]), (uint32_t)((j / TM_NST) & 1));
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue: warps 0-7 ----------------
+    const int q = warp & 3, hc = warp >> 2;
+    const int r = q * 32 + lane;
+    for (int i = 0; i < my_tiles; i++) {
+      const int tile = blockIdx.x + i * gridDim.x;
+      const int row0 = (tile / tiles_n) * TC_BM, col0 = (tile % tiles_n) * TC_BN;
+      const int buf = i & 1;
       const int gr = row0 + r, gcb = col0 + hc * 128;
+      float4 cv[32];
 #pragma unroll
       for (int j = 0; j < 32; j++) {
         int gc = gcb + 4 * j;
@@ -421,86 +479,46 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_tma_kernel(const __gr
           }
         }
       }
-    }
-    // ---- lane 0 of warp 0: MMAs of chunk g, then the loads of chunk g + TM_NST - 1
-    if (warp == 0) {
-      if (lane == 0 && !timed_out) {
-        if (!tm_wait(smem_u32(&full[st]), (uint32_t)((g / TM_NST) & 1))) {
-          timed_out = 1;
-        } else {
-          consumed++;
-          const uint32_t idesc = umma_idesc(0);
-          const uint32_t ua = s0 + st * TM_STAGE, ub = ua + TM_STAGE_A;
+      if (!tm_wait(smem_u32(&accf[buf]), (uint32_t)((i / 2) & 1))) { timed_out = 1; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-          for (int s = 0; s < TM_KC / 8; s++) {
-            uint64_t da = umma_desc_sw128(ua + 32u * s);
-            uint64_t db = umma_desc_sw128(ub + 32u * s);
-            uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                "l"(da), "l"(db), "r"(idesc), "r"(acc));
-          }
-          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                           smem_u32(&empty[st]))
-                       : "memory");
-          if (issued < G) {
-            // the stage of chunk issued - TM_NST must be free: its MMAs committed
-            const int old = issued - TM_NST;
-            if (old >= 0 && !tm_wait(smem_u32(&empty[old % TM_NST]), (uint32_t)((old / TM_NST) & 1))) timed_out = 1;
-            else issue(issued++);
-          }
-        }
-      }
-      __syncwarp();
-    }
-    if (c != nch - 1) continue;
-
-    // ---- last chunk of the tile: accumulators complete, then TMEM -> registers -> C
-    if (!timed_out && !tm_wait(smem_u32(&empty[st]), (uint32_t)((g / TM_NST) & 1))) timed_out = 1;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (timed_out) break;
-    const int gr = row0 + r, gcb = col0 + hc * 128;
+      for (int cb = 0; cb < 128; cb += 16) {
+        uint32_t v[16];
+        uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * TC_BN + hc * 128 + cb);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+              "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (gr < m) {
 #pragma unroll
-    for (int cb = 0; cb < 128; cb += 16) {
-      uint32_t v[16];
-      uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(hc * 128 + cb);
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-            "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (gr < m) {
-#pragma unroll
-        for (int j4 = 0; j4 < 4; j4++) {
-          const int j = cb / 4 + j4;
-          const int gc = gcb + 4 * j;
-          float4 t = make_float4(__uint_as_float(v[4 * j4]), __uint_as_float(v[4 * j4 + 1]), __uint_as_float(v[4 * j4 + 2]),
-                                 __uint_as_float(v[4 * j4 + 3]));
-          float4 o = overwrite ? t : make_float4(cv[j].x - t.x, cv[j].y - t.y, cv[j].z - t.z, cv[j].w - t.w);
-          float *dst = C + (size_t)gr * ldc + gc;
-          if (gc + 3 < n) *reinterpret_cast<float4 *>(dst) = o;
-          else if (gc < n) {
-            dst[0] = o.x;
-            if (gc + 1 < n) dst[1] = o.y;
-            if (gc + 2 < n) dst[2] = o.z;
+          for (int j4 = 0; j4 < 4; j4++) {
+            const int j = cb / 4 + j4;
+            const int gc = gcb + 4 * j;
+            float4 t = make_float4(__uint_as_float(v[4 * j4]), __uint_as_float(v[4 * j4 + 1]),
+                                   __uint_as_float(v[4 * j4 + 2]), __uint_as_float(v[4 * j4 + 3]));
+            float4 o = overwrite ? t : make_float4(cv[j].x - t.x, cv[j].y - t.y, cv[j].z - t.z, cv[j].w - t.w);
+            float *dst = C + (size_t)gr * ldc + gc;
+            if (gc + 3 < n) *reinterpret_cast<float4 *>(dst) = o;
+            else if (gc < n) {
+              dst[0] = o.x;
+              if (gc + 1 < n) dst[1] = o.y;
+              if (gc + 2 < n) dst[2] = o.z;
+            }
           }
         }
       }
+      // this thread's reads of the buffer are done: release it to the producer
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acce[buf])) : "memory");
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
-  // after a timeout: wait (bounded) for bulk copies still in flight before the CTA exits
-  if (tid == 0)
-    for (int j = consumed; j < issued; j++) tm_wait(smem_u32(&full[j % TM_NST]), (uint32_t)((j / TM_NST) & 1));
   if (timed_out && tid == 0) atomicExch(err, 2);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_BN));
 }
 
 // CUDA-core reference for the self-test: C -= A B or C = A B (FP32 inputs
@@ -619,7 +637,7 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
     RB_TRY(encode_map(&ma, A, m, k, lda, TC_BM));
     RB_TRY(encode_map(&mb, g_tc_bt.as<float>(), n, k, ldbt, TC_BN));
     RB_CUDA(cudaFuncSetAttribute(tc_update_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TM_SMEM));
-    tc_update_tma_kernel<<<grid, TC_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(), overwrite);
+    tc_update_tma_kernel<<<grid, TM_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(), overwrite);
     return check_launch("tc_update_tma_kernel");
   }
   RB_CUDA(cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
