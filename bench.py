@@ -318,6 +318,52 @@ def adjoint_ratio(reps=3):
     return out
 
 
+def fldint_timing(reps=3):
+    """Field integrals through the public API (rad.FldInt: host packing,
+    device quadrature, host result) on the relaxed planar undulator
+    (2 x 40 blocks 50x10x5 mm, 2x2x2 subdivision, 640 elements) along its
+    axis: the infinite first field integral and the finite one over +-150 mm,
+    at PrcBInt 1e-3 (the reference's default) and 1e-6.  Median wall time of
+    `reps` calls after one warm-up; beside it the reference CPU module's
+    FldInt on the same relaxed model (when oracle/_ref is present) and the
+    largest difference between the two."""
+    import torch
+
+    from radiacuda_b200 import rad
+    import models as MD
+
+    p1, p2 = [0.137, 0.091, -150.0], [0.137, 0.091, 150.0]
+    lines = [("inf", 1e-3), ("inf", 1e-6), ("fin", 1e-3), ("fin", 1e-6)]
+
+    def run(R, sync):
+        h = MD.undulator(R, nper_row=40, div=2)[0]
+        R.Solve(h, 1e-10, 1000, 4)
+        out = {}
+        for mode, prc in lines:
+            R.FldCmpCrt(1e-4, 1e-3, prc, 1.0, 1e-5, 1e-5)
+            ts, v = [], None
+            for r in range(reps + 1):
+                sync()
+                t0 = time.perf_counter()
+                v = R.FldInt(h, mode, "ib", p1, p2)
+                sync()
+                if r:
+                    ts.append(time.perf_counter() - t0)
+            out[f"{mode}_{prc:.0e}"] = (float(np.median(ts)), v)
+        R.FldCmpCrt(1e-4, 1e-3, 1e-3, 1.0, 1e-5, 1e-5)
+        return out
+
+    ours = run(rad, torch.cuda.synchronize)
+    res = {"model": "undulator_640 (relaxed)", "line": [p1, p2], "id": "ib",
+           "ours_s": {k: round(t, 5) for k, (t, _) in ours.items()}}
+    R = _ref_module()
+    if R is not None:
+        ref = run(R, lambda: None)
+        res["reference_cpu_s"] = {k: round(t, 5) for k, (t, _) in ref.items()}
+        res["max_abs_diff_Tmm"] = {k: float(np.abs(np.array(ours[k][1]) - np.array(ref[k][1])).max()) for k in ours}
+    return res
+
+
 # dram__bytes_read.sum + dram__bytes_write.sum over the algorithmic bytes of the
 # trailing-update kernel (561 MB / 611 MB), from the ncu capture summarised in
 # profiles/tc_update_tma_kernel_lu9000.md
@@ -430,6 +476,7 @@ def main():
     res = run_ours(args, rank, world)
     if not args.profile:
         res["adjoint"] = adjoint_ratio()
+        res["fldint"] = fldint_timing()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = reference_sample()
         res["cpu_baseline"] = cb if cb is not None else {"value": None, "unavailable": "oracle/_ref missing"}

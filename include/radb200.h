@@ -172,6 +172,37 @@ RADB200_API int radb200_field_noalloc(const RadB200Geom *g, const double *d_pts,
 RADB200_API int radb200_field_dev(const RadB200Geom *g, const double *d_pts, int64_t npts,
                       int what, int precision, double *d_out);
 
+/* ---- field integrals along a straight line ---------------------------------
+ * Replaces radTApplication::ComputeFieldInt (cpp/src/core/radapl3.cpp:356-385),
+ * which RadFldInt (cpp/src/lib/radentry.cpp:1310-1325) and radpy FldInt
+ * (cpp/src/clients/python/radpy.cpp:2501-2531) call.
+ *   P1, P2     [3] host points on the line (mm).
+ *   infinite   0: integral from P1 to P2; 1: over the whole line through P1
+ *              and P2 (uniform background fields contribute zero there, as in
+ *              the reference, radarccu.h:306-316).
+ *   what       bit 0: integral of B into out[0..2]; bit 1: of H into out[3..5].
+ *   precision  as radb200_field.
+ *   abs_prec   absolute accuracy in T mm (the reference's PrcBInt, FldCmpCrt;
+ *              its default is 1e-3): adaptive Gauss-Kronrod panels are split
+ *              until the sum of their error estimates is below it.
+ *   out        [6] host.
+ *   status     [6] host or NULL: error estimate (T mm), field points
+ *              evaluated, refinement levels, panels, 1 if abs_prec was met
+ *              (2 if the panels still above it stopped converging at the
+ *              rounding noise of the field, 0 if the level cap was hit),
+ *              seconds.                                                       */
+RADB200_API int radb200_field_int(const RadB200Geom *g, const double *P1, const double *P2, int infinite,
+                                  int what, int precision, double abs_prec, double *out, double *status);
+/* The same quadrature around a caller-supplied point field (no device use):
+ * fn(ctx, g', pts, npts, what, out) must write the field (what 0 B, 1 H) of
+ * geometry g' at npts host points and return 0; g' is g with the background
+ * fields removed for infinite lines.  No counterpart in the reference.      */
+typedef int (*RadB200PointField)(void *ctx, const RadB200Geom *g, const double *pts, int64_t npts, int what,
+                                 double *out);
+RADB200_API int radb200_field_int_cb(const RadB200Geom *g, RadB200PointField fn, void *ctx, const double *P1,
+                                     const double *P2, int infinite, int what, double abs_prec, double *out,
+                                     double *status);
+
 /* ---- interaction (assembly + solver state) ---------------------------------
  * Replaces radGPU_PackGeometryForAsm + radGPU_AssembleMatrix +
  * radGPU_PublishAssembledMatrix (radgpu_asm.h:149-187): assembles the dense

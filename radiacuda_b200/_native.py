@@ -19,6 +19,8 @@ LIBPATH = os.path.join(HERE, "libradb200.so")
 
 _lib = None
 _vp, _dp, _i64 = C.c_void_p, C.POINTER(C.c_double), C.c_int64
+# RadB200PointField: (ctx, geometry, pts, npts, what, out) -> 0
+POINT_FIELD = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, _dp, _i64, C.c_int, _dp)
 
 
 def lib():
@@ -44,6 +46,9 @@ def lib():
         L.radb200_adjoint_solve.argtypes = [_i64, _dp, C.c_double, C.c_int, _dp, _dp]
         L.radb200_adjoint_grad.argtypes = [_i64, _dp, _dp, _dp, _dp, _dp]
         L.radb200_field_vjp.argtypes = [_i64, _dp, _dp, _i64, C.c_int, _dp, _dp, _dp, _dp]
+        L.radb200_field_int.argtypes = [_vp, _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_double, _dp, _dp]
+        L.radb200_field_int_cb.argtypes = [_vp, POINT_FIELD, _vp, _dp, _dp, C.c_int, C.c_int, C.c_double, _dp,
+                                           _dp]
         _lib = L
     return _lib
 
@@ -69,6 +74,44 @@ def field(geom: Dict[str, np.ndarray], pts: np.ndarray, what: int, precision: in
     if P.shape[0]:
         check(lib().radb200_field(C.cast(g.ptr, _vp), _p(P), P.shape[0], what, precision, _p(out)), "radb200_field")
     return out
+
+
+def field_int(geom: Dict[str, np.ndarray], P1, P2, infinite: bool, what: int, precision: int = 0,
+              abs_prec: float = 1e-3) -> Tuple[np.ndarray, np.ndarray]:
+    """Integral of B (what bit 0 -> out[0:3]) and/or H (bit 1 -> out[3:6])
+    along the line P1 -> P2 (finite) or through P1, P2 (infinite), T mm.
+    Returns (out[6], status[6]) as radb200_field_int."""
+    g = GeomHolder(geom)
+    a = np.ascontiguousarray(P1, dtype=np.float64).reshape(3)
+    b = np.ascontiguousarray(P2, dtype=np.float64).reshape(3)
+    out, st = np.zeros(6), np.zeros(6)
+    check(lib().radb200_field_int(C.cast(g.ptr, _vp), _p(a), _p(b), int(bool(infinite)), int(what), int(precision),
+                                  float(abs_prec), _p(out), _p(st)), "radb200_field_int")
+    return out, st
+
+
+def field_int_cb(geom: Dict[str, np.ndarray], point_field, P1, P2, infinite: bool, what: int,
+                 abs_prec: float = 1e-3) -> Tuple[np.ndarray, np.ndarray]:
+    """The quadrature of field_int around ``point_field(geom_ptr, pts[n,3],
+    what) -> [n,3]`` (host code, no device use)."""
+    g = GeomHolder(geom)
+
+    def cb(ctx, gp, pts, n, w, out):
+        try:
+            P = np.ctypeslib.as_array(pts, shape=(n, 3))
+            O = np.ctypeslib.as_array(out, shape=(n, 3))
+            O[:] = point_field(gp, P, w)
+            return 0
+        except Exception:  # reported to the library as a failed evaluation
+            return 1
+
+    fn = POINT_FIELD(cb)
+    a = np.ascontiguousarray(P1, dtype=np.float64).reshape(3)
+    b = np.ascontiguousarray(P2, dtype=np.float64).reshape(3)
+    out, st = np.zeros(6), np.zeros(6)
+    check(lib().radb200_field_int_cb(C.cast(g.ptr, _vp), fn, None, _p(a), _p(b), int(bool(infinite)), int(what),
+                                     float(abs_prec), _p(out), _p(st)), "radb200_field_int_cb")
+    return out, st
 
 
 def field_dev(geom: Dict[str, np.ndarray], d_pts_ptr: int, npts: int, what: int, d_out_ptr: int, precision: int = 0):

@@ -28,7 +28,7 @@ __all__ = [
     "ObjCnt", "ObjAddToCnt", "ObjCntStuf", "ObjCntSize", "ObjDivMag", "ObjM", "ObjSetM",
     "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
     "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
-    "RlxPre", "RlxAuto", "Solve", "Fld", "FldLst", "FldLenRndSw", "FldLenTol",
+    "RlxPre", "RlxAuto", "Solve", "Fld", "FldLst", "FldInt", "FldCmpCrt", "FldCmpPrc", "FldLenRndSw", "FldLenTol",
     "UtiDel", "UtiDelAll", "UtiVer", "UtiFldLastBackend", "UtiAsmLastBackend", "UtiGpuFallback",
 ]
 
@@ -40,6 +40,10 @@ _next = [1]
 # radTConvergRepair defaults (radcnvrg.h:37-45); FldLenRndSw('off') zeroes them
 _rand_on = [1e-09, 1e-11, 1e-09]
 _rand = list(_rand_on)
+# radTCompCriterium defaults (cpp/src/core/radg3d.h:468-485); FldInt reads PrcBInt
+_PRC_DEFAULT = {"PrcB": 1e-4, "PrcA": 1e-3, "PrcBInt": 1e-3, "PrcForce": 1.0, "PrcTorque": 10.0,
+                "PrcEnergy": 10.0, "PrcCoord": -1.0, "PrcAngle": -1.0}
+_prc = dict(_PRC_DEFAULT)
 _last_fld = ["none"]
 _last_asm = ["none"]
 _fallback = ["cpu"]
@@ -568,6 +572,113 @@ def FldLst(obj: int, fid: str, P1, P2, np_: int, arg: str = "noarg", strt: float
         step = np.linalg.norm(P2 - P1) / max(int(np_) - 1, 1)
         return [[strt + i * step, v] for i, v in enumerate(vals)]
     return vals
+
+
+def _fldint_items(cmpn: str):
+    """Quantities and output layout of a field-integral id string.
+
+    Which integrals are computed follows ValidateFieldIntChar
+    (cpp/src/core/radapl1.cpp:132-168); the order and count of the returned
+    values follow radTSend::OutFieldIntCompRes (cpp/src/core/radsend.cpp:888-1003):
+    'ibx' -> Ib.x, 'ib' / 'i' / '' -> Ib (3 values), 'ihz' -> Ih.z, a bare
+    'x' / 'y' / 'z' not preceded by i, b or h -> that component of Ib."""
+    s = str(cmpn)
+    low = s.lower()
+    i_used = "i" in low
+    ib = (not s) or ("b" in low)
+    ih = "h" in low
+    if not ib and not ih:
+        if not i_used:
+            raise RadiaError("Radia::Error032: Incorrect input: Field Integral component identification string "
+                             "should contain either combination of characters I,i,B,b,H,h,x,y,z or nothing.")
+        ib = True
+    n_items = 0
+    prev = ""
+    for ch in low:
+        if ch in "bh" or (ch in "xyz" and prev not in ("b", "h")):
+            n_items += 1
+        prev = ch
+    walk = low if (low and not (i_used and n_items == 0)) else "ib"
+    items = []
+    for k, ch in enumerate(walk):
+        nxt = walk[k + 1] if k + 1 < len(walk) else ""
+        prv = walk[k - 1] if k > 0 else ""
+        comp = "xyz".index(nxt) if nxt and nxt in "xyz" else None
+        if ch == "i":
+            if comp is not None:
+                items.append(("b", comp))
+            elif not (nxt and nxt in "bh"):
+                items.append(("b", None))
+                break
+        elif ch in "bh":
+            items.append((ch, comp))
+        elif ch in "xyz" and not (prv and prv in "ibh"):
+            items.append(("b", "xyz".index(ch)))
+    return ib, ih, items
+
+
+def FldInt(obj: int, inf_or_fin: str, cmpn: str, P1, P2, precision: str = "double"):
+    """Field integral along a straight line (radpy FldInt, radpy.cpp:2501-2531;
+    radTApplication::ComputeFieldInt, radapl3.cpp:356-385), T mm.
+
+    'fin' integrates from P1 to P2, 'inf' over the whole line through them
+    (uniform background fields contribute zero to an infinite integral, as in
+    the reference).  The accuracy is the absolute PrcBInt of FldCmpCrt /
+    FldCmpPrc (default 1e-3 T mm).  One value is returned as a float, more
+    as a list, as in the reference."""
+    mode = str(inf_or_fin)
+    if mode in ("inf", "Inf", "INF"):
+        infinite = True
+    elif mode in ("fin", "Fin", "FIN"):
+        infinite = False
+    else:
+        raise RadiaError("Radia::Error033: Incorrect input: Integral identification string should be either "
+                         " inf  or  fin .")
+    ib, ih, items = _fldint_items(cmpn)
+    a, b = _v3(P1, "first point defining integration line"), _v3(P2, "second point defining integration line")
+    prec = {"double": 0, "single": 1, "fast": 2}.get(str(precision).lower())
+    if prec is None:
+        raise RadiaError("Radia::Error000: precision must be 'double', 'single' or 'fast'")
+    geom = pack_sources(_objs, int(obj), tuple(_rand))
+    what = (1 if ib else 0) | (2 if ih else 0)
+    out, _st = _native.field_int(geom, a, b, infinite, what, prec, _prc["PrcBInt"])
+    _last_fld[0] = "gpu"
+    vals = []
+    for q, comp in items:
+        v = out[0:3] if q == "b" else out[3:6]
+        vals.extend(float(x) for x in (v if comp is None else v[comp:comp + 1]))
+    return vals[0] if len(vals) == 1 else vals
+
+
+def FldCmpCrt(prcB: float, prcA: float, prcBint: float, prcFrc: float, prcTrjCrd: float, prcTrjAng: float) -> int:
+    """Absolute accuracy levels (radpy FldCmpCrt, radpy.cpp:2845-2865;
+    SetCompCriterium, radapl2.cpp:2056-2075).  Of these, FldInt uses prcBint."""
+    vals = [float(v) for v in (prcB, prcA, prcBint, prcFrc, prcTrjCrd, prcTrjAng)]
+    if any(not (v > 0) for v in vals):
+        raise RadiaError("Radia::Error000: FldCmpCrt: incorrect or missing function argument")
+    for k, v in zip(("PrcB", "PrcA", "PrcBInt", "PrcForce", "PrcCoord", "PrcAngle"), vals):
+        _prc[k] = v
+    return 1
+
+
+def FldCmpPrc(opts: str) -> int:
+    """Accuracy levels by option string 'PrcB->v,PrcBInt->v,...' (radpy
+    FldCmpPrc, radpy.cpp:2870-2895; SetCompPrecisions, radapl2.cpp:2029-2052)."""
+    text = str(opts).replace(" ", "")
+    parts = [p for p in text.replace(";", ",").split(",") if p]
+    upd = {}
+    for p in parts:
+        name, sep, val = p.partition("->")
+        if not sep or name not in _PRC_DEFAULT:
+            raise RadiaError("Radia::Error057: Incorrect input: Improper definition of absolute precision "
+                             "value(s). See the usage message for the function.")
+        try:
+            upd[name] = float(val)
+        except ValueError:
+            raise RadiaError("Radia::Error057: Incorrect input: Improper definition of absolute precision "
+                             "value(s). See the usage message for the function.") from None
+    _prc.update(upd)
+    return 1
 
 
 def FldLenRndSw(onoff: str) -> int:
