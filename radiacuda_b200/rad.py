@@ -97,26 +97,82 @@ def ObjPolyhdr(V, F, M=(0.0, 0.0, 0.0)) -> int:
     return _add(Polyhedron(np.asarray(V, dtype=np.float64), faces, _v3(M)))
 
 
+def _abs_rand_magnitude(a: float) -> float:
+    """radTConvergRepair::AbsRandMagnitude (cpp/src/core/radcnvrg.h:85-91)."""
+    abs_r, rel_r, zero_r = _rand
+    m = max(abs_r, rel_r * a)
+    return m if a != 0.0 else max(m, zero_r)
+
+
+def _thckpgn_rectangle(pts: np.ndarray):
+    """Centre and sides of an axis-aligned 4-point polygon, or None
+    (CheckIfExtrudedPolygonIsRecMag, cpp/src/core/radappl.h:339-372).  The
+    tolerance is twice the randomization magnitude, so with FldLenRndSw('off')
+    no polygon qualifies."""
+    if pts.shape[0] != 4:
+        return None
+    d1 = np.linalg.norm(pts[2] - pts[0])
+    d2 = np.linalg.norm(pts[3] - pts[1])
+    tol = 2.0 * _abs_rand_magnitude(max(d1, d2))
+    if abs(d2 - d1) > tol:
+        return None
+    e = np.abs(np.roll(pts, -1, axis=0) - pts)     # |p1-p0|, |p2-p1|, |p3-p2|, |p0-p3|
+    small, big = e < tol, e > tol
+    alt1 = small[0, 0] and big[0, 1] and big[1, 0] and small[1, 1] and small[2, 0] and big[2, 1] and big[3, 0] and small[3, 1]
+    alt2 = big[0, 0] and small[0, 1] and small[1, 0] and big[1, 1] and big[2, 0] and small[2, 1] and small[3, 0] and big[3, 1]
+    if not (alt1 or alt2):
+        return None
+    cen, dim = np.zeros(2), np.zeros(2)
+    for k in range(2):   # the longer of the first two sides along each 2-D axis
+        da, db = abs(pts[1, k] - pts[0, k]), abs(pts[2, k] - pts[1, k])
+        if da > db:
+            cen[k], dim[k] = 0.5 * (pts[1, k] + pts[0, k]), da
+        else:
+            cen[k], dim[k] = 0.5 * (pts[2, k] + pts[1, k]), db
+    return cen, dim
+
+
 def ObjThckPgn(x, lx, pts, a="x", M=(0.0, 0.0, 0.0)) -> int:
-    """Extruded convex polygon, converted to a polyhedron (radgpu_fld.cpp:511-536)."""
+    """Extruded convex polygon (radpy ObjThckPgn, radpy.cpp:190-225;
+    radTApplication::SetExtrudedPolygon, radapl1.cpp:318-480).
+
+    The polygon [[u, v], ...] is extruded over [x - lx/2, x + lx/2] along
+    a.  As in the reference, an axis-aligned rectangle becomes a block
+    (within the randomization tolerance: never with FldLenRndSw('off')); any
+    other polygon is built along x in its own frame, u -> y and v -> z, and for
+    a = 'y' or 'z' carries the orientation transform of
+    FindSpaceTransToOrientObjAlongMainAxis (radapl1.cpp:1486-1560): a rotation
+    about (1, 1, 1) by 2 pi / 3 or 4 pi / 3, with M taken back into the
+    element's frame.  The extruded polygon is a polyhedron here, relaxed and
+    evaluated by the polyhedron kernels (the reference's GPU assembly declines
+    it, radgpu_asm.cpp:228-233)."""
     pts = np.asarray(pts, dtype=np.float64).reshape(-1, 2)
+    ax = str(a)[:1].lower()
+    if ax not in ("x", "y", "z"):
+        raise RadiaError("Radia::Error000: ObjThckPgn: orientation definition should be 'x', 'y' or 'z'")
+    if pts.shape[0] < 3:
+        raise RadiaError("Radia::Error048: a face needs at least 3 points")
+    M = _v3(M)
+    x, lx = float(x), float(lx)
+    rect = _thckpgn_rectangle(pts)
+    if rect is not None:
+        (cu, cv), (du, dv) = rect
+        c = {"x": [x, cu, cv], "y": [cv, x, cu], "z": [cu, cv, x]}[ax]
+        d = {"x": [lx, du, dv], "y": [dv, lx, du], "z": [du, dv, lx]}[ax]
+        return _add(RecMag(np.array(c), np.array(d), M))
     n = pts.shape[0]
-    ax = a.lower()
     lo, hi = x - 0.5 * lx, x + 0.5 * lx
-
-    def p3(t, u, v):
-        if ax == "x":
-            return [t, u, v]
-        if ax == "y":
-            return [v, t, u]
-        return [u, v, t]
-
-    V = [p3(lo, *pts[k]) for k in range(n)] + [p3(hi, *pts[k]) for k in range(n)]
-    F = [list(range(1, n + 1)), list(range(n + 1, 2 * n + 1))]
+    V = [[lo, pts[k, 0], pts[k, 1]] for k in range(n)] + [[hi, pts[k, 0], pts[k, 1]] for k in range(n)]
+    F = [list(range(n)), list(range(n, 2 * n))]
     for k in range(n):
         k2 = (k + 1) % n
-        F.append([k + 1, k2 + 1, n + k2 + 1, n + k + 1])
-    return ObjPolyhdr(V, F, M)
+        F.append([k, k2, n + k2, n + k])
+    if ax == "x":
+        return _add(Polyhedron(np.asarray(V), F, M))
+    t = trf_rotation(np.zeros(3), np.ones(3), (2.0 if ax == "y" else 4.0) * math.pi / 3.0)
+    o = Polyhedron(np.asarray(V), F, (t.Minv @ M) / t.s)
+    o.add_transform(1, t)
+    return _add(o)
 
 
 def _axis_trf(P, orient: str) -> Optional[Trf]:

@@ -34,6 +34,7 @@ CASES = {
     "mixed_sym": (MD.mixed_sym, {}, None, 1e-8, 3000),
     "iron_dipole_300": (MD.iron_dipole, dict(n_target=300), MD.iron_dipole_points(5), 1e-7, 3000),
     "tet_mesh_150": (MD.tet_mesh, dict(ncell=3, n_tets=150, chi=5.0), None, 1e-7, 3000),
+    "thckpgn_4": (MD.thckpgn_model, {}, None, 1e-9, 3000),
 }
 
 

@@ -312,6 +312,26 @@ def mixed_sym(R, seed=3):
 
 
 # ---------------------------------------------------------------------------
+# extruded polygons along x, y and z, anisotropic linear and saturating
+# materials (with FldLenRndSw('off') the reference keeps even the rectangle
+# as an extruded polygon)
+# ---------------------------------------------------------------------------
+def thckpgn_model(R):
+    reset(R)
+    hexagon = [[6.0 * np.cos(k * np.pi / 3) + 0.3, 6.0 * np.sin(k * np.pi / 3) - 0.2] for k in range(6)]
+    a = R.ObjThckPgn(4.0, 8.0, hexagon, "x", [0.9, 0.2, -0.1])
+    b = R.ObjThckPgn(20.0, 5.0, [[0.0, 0.0], [9.0, 1.5], [3.0, 7.0]], "y", [0.1, 1.1, 0.3])
+    pent = [[5.0 * np.cos(2 * np.pi * k / 5) + 25.0, 5.0 * np.sin(2 * np.pi * k / 5) - 3.0] for k in range(5)]
+    c = R.ObjThckPgn(-7.0, 6.0, pent, "z", [0.0, 0.0, 1.0])
+    d = R.ObjThckPgn(12.0, 4.0, [[30.0, 10.0], [38.0, 10.0], [38.0, 16.0], [30.0, 16.0]], "z", [0.5, 0.0, 0.0])
+    R.MatApl(a, R.MatLin([0.05, 0.15], [0.9, 0.2, -0.1]))
+    R.MatApl(b, R.MatLin([0.06, 0.12], [0.1, 1.1, 0.3]))
+    R.MatApl(c, R.MatSatIsoFrm([2000, 1.5], [100, 0.4], [10, 0.2]))
+    R.MatApl(d, R.MatLin([0.05, 0.15], [0.5, 0.0, 0.0]))
+    return R.ObjCnt([a, b, c, d])
+
+
+# ---------------------------------------------------------------------------
 # the reference's MPI-solve regression models (tests/test_mpi_solve.py of the
 # reference), rebuilt with the same seeded draws so the golden B values of
 # its tests/_mpi_solve_reference.json apply

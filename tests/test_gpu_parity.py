@@ -28,6 +28,7 @@ BUILDERS = {
     "mixed_sym": MD.mixed_sym,
     "iron_dipole_300": MD.iron_dipole,
     "tet_mesh_150": MD.tet_mesh,
+    "thckpgn_4": MD.thckpgn_model,
 }
 LINEAR = {"magnet_array_2x2", "sym_blocks", "tet_mesh_150"}
 
