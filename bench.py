@@ -332,7 +332,7 @@ def fldint_timing(reps=3):
     from radiacuda_b200 import rad
     import models as MD
 
-    p1, p2 = [0.137, 0.091, -150.0], [0.137, 0.091, 150.0]
+    p1, p2 = [0.137, 0.091, -150.3], [0.137, 0.091, 149.9]
     lines = [("inf", 1e-3), ("inf", 1e-6), ("fin", 1e-3), ("fin", 1e-6)]
 
     def run(R, sync):
@@ -361,6 +361,52 @@ def fldint_timing(reps=3):
         ref = run(R, lambda: None)
         res["reference_cpu_s"] = {k: round(t, 5) for k, (t, _) in ref.items()}
         res["max_abs_diff_Tmm"] = {k: float(np.abs(np.array(ours[k][1]) - np.array(ref[k][1])).max()) for k in ours}
+    return res
+
+
+def trajectory_timing(reps=3):
+    """Electron trajectories through the public API (rad.FldPtcTrj) in the
+    relaxed iron dipole (about 360 saturating cuboids with 4 images each, a
+    racetrack coil): one 0.3 GeV trajectory through the gap over +-200 mm at
+    401 points (default fixed-step Runge-Kutta: 1,600 field evaluations in
+    sequence), and a batch of 1,024 trajectories (one CTA each).  Median wall
+    time of `reps` after one warm-up; the reference CPU module's FldPtcTrj on
+    the same relaxed model beside it, with the largest difference."""
+    import torch
+
+    from radiacuda_b200 import rad
+    import models as MD
+
+    init, lim, npt = [0.3, 0.0, 0.7, 0.0], [-200.13, 200.31], 401
+    rng = np.random.default_rng(2)
+    batch = np.column_stack([rng.uniform(-10, 10, 1024), rng.normal(0, 2e-3, 1024), rng.uniform(-8, 8, 1024),
+                             rng.normal(0, 2e-3, 1024)])
+
+    def timed(f, sync):
+        ts, v = [], None
+        for r in range(reps + 1):
+            sync()
+            t0 = time.perf_counter()
+            v = f()
+            sync()
+            if r:
+                ts.append(time.perf_counter() - t0)
+        return float(np.median(ts)), v
+
+    h = MD.iron_dipole(rad, n_target=300)
+    rad.Solve(h, 1e-7, 3000, 4)
+    t1, ours = timed(lambda: rad.FldPtcTrj(h, 0.3, init, lim, npt), torch.cuda.synchronize)
+    tb, _ = timed(lambda: rad.FldPtcTrj(h, 0.3, batch, lim, npt), torch.cuda.synchronize)
+    res = {"model": "iron_dipole_300 (relaxed)", "energy_GeV": 0.3, "points": npt,
+           "ours_s": {"one": round(t1, 5), "batch_1024": round(tb, 5)},
+           "trajectories_per_s_batch": round(1024 / tb, 1)}
+    R = _ref_module()
+    if R is not None:
+        hr = MD.iron_dipole(R, n_target=300)
+        R.Solve(hr, 1e-7, 3000, 4)
+        tr, ref = timed(lambda: R.FldPtcTrj(hr, 0.3, init, lim, npt), lambda: None)
+        res["reference_cpu_s"] = {"one": round(tr, 5)}
+        res["max_abs_diff"] = float(np.abs(np.array(ours) - np.array(ref)).max())
     return res
 
 
@@ -477,6 +523,7 @@ def main():
     if not args.profile:
         res["adjoint"] = adjoint_ratio()
         res["fldint"] = fldint_timing()
+        res["trajectory"] = trajectory_timing()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = reference_sample()
         res["cpu_baseline"] = cb if cb is not None else {"value": None, "unavailable": "oracle/_ref missing"}

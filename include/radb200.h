@@ -193,6 +193,24 @@ RADB200_API int radb200_field_dev(const RadB200Geom *g, const double *d_pts, int
  *              seconds.                                                       */
 RADB200_API int radb200_field_int(const RadB200Geom *g, const double *P1, const double *P2, int infinite,
                                   int what, int precision, double abs_prec, double *out, double *status);
+/* Relativistic electron trajectories in the field of g: replaces
+ * radTApplication::ComputeParticleTrajectory (cpp/src/core/radapl3.cpp:639-672)
+ * behind RadFldPtcTrj / radpy FldPtcTrj (radpy.cpp:2537-2569).
+ *   energy_gev  electron energy (GeV).
+ *   init        [n_traj * 4] host: x, dx/dy, z, dz/dy at y0 (mm, rad).
+ *   y0, y1, np  tabulation y0 + k (y1 - y0) / (np - 1), k = 0 .. np-1.
+ *   prec        NULL: one fourth-order Runge-Kutta step per interval (the
+ *               reference's default); else [4] accuracies of x, x', z, z'
+ *               (the reference's PrcCoord, PrcAngle, PrcCoord, PrcAngle)
+ *               for its step-doubling control, 0 meaning none.
+ *   out         [n_traj * np * 5] host: y, x, dx/dy, z, dz/dy per point.
+ *   status      [n_traj] host or NULL: 0, or 1 step too small (Error200),
+ *               2 step limit (Error201), 3 no acceptable step.
+ * One CTA per trajectory (the stages of one trajectory are a chain); many
+ * trajectories in one call run concurrently.  Returns RADB200_E_NOCONV when
+ * any trajectory failed.                                                    */
+RADB200_API int radb200_trajectories(const RadB200Geom *g, double energy_gev, int n_traj, const double *init,
+                                     double y0, double y1, int np, const double *prec, double *out, int *status);
 /* The same quadrature around a caller-supplied point field (no device use):
  * fn(ctx, g', pts, npts, what, out) must write the field (what 0 B, 1 H) of
  * geometry g' at npts host points and return 0; g' is g with the background

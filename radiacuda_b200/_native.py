@@ -46,6 +46,8 @@ def lib():
         L.radb200_adjoint_solve.argtypes = [_i64, _dp, C.c_double, C.c_int, _dp, _dp]
         L.radb200_adjoint_grad.argtypes = [_i64, _dp, _dp, _dp, _dp, _dp]
         L.radb200_field_vjp.argtypes = [_i64, _dp, _dp, _i64, C.c_int, _dp, _dp, _dp, _dp]
+        L.radb200_trajectories.argtypes = [_vp, C.c_double, C.c_int, _dp, C.c_double, C.c_double, C.c_int, _dp, _dp,
+                                           C.POINTER(C.c_int)]
         L.radb200_field_int.argtypes = [_vp, _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_double, _dp, _dp]
         L.radb200_field_int_cb.argtypes = [_vp, POINT_FIELD, _vp, _dp, _dp, C.c_int, C.c_int, C.c_double, _dp,
                                            _dp]
@@ -88,6 +90,21 @@ def field_int(geom: Dict[str, np.ndarray], P1, P2, infinite: bool, what: int, pr
     check(lib().radb200_field_int(C.cast(g.ptr, _vp), _p(a), _p(b), int(bool(infinite)), int(what), int(precision),
                                   float(abs_prec), _p(out), _p(st)), "radb200_field_int")
     return out, st
+
+
+def trajectories(geom: Dict[str, np.ndarray], energy_gev: float, init: np.ndarray, y0: float, y1: float, np_: int,
+                 prec=None) -> np.ndarray:
+    """Electron trajectories (radb200_trajectories): init [n, 4] (x, x', z, z')
+    -> [n, np_, 5] (y, x, x', z, z')."""
+    g = GeomHolder(geom)
+    X = np.ascontiguousarray(init, dtype=np.float64).reshape(-1, 4)
+    out = np.zeros((X.shape[0], int(np_), 5))
+    st = np.zeros(X.shape[0], dtype=np.int32)
+    pr = None if prec is None else np.ascontiguousarray(prec, dtype=np.float64).reshape(4)
+    check(lib().radb200_trajectories(C.cast(g.ptr, _vp), float(energy_gev), X.shape[0], _p(X), float(y0), float(y1),
+                                     int(np_), _p(pr), _p(out), st.ctypes.data_as(C.POINTER(C.c_int))),
+          "radb200_trajectories")
+    return out
 
 
 def field_int_cb(geom: Dict[str, np.ndarray], point_field, P1, P2, infinite: bool, what: int,

@@ -360,4 +360,204 @@ int launch_rowtrans_vec(const double *rowT, const double *in, double *out, int n
   return check_launch("rowtrans_kernel");
 }
 
+// ---------------------------------------------------------------------------
+// Relativistic electron trajectories (FldPtcTrj).  The reference integrates
+// x(y), x'(y), z(y), z'(y) with the field of the whole source evaluated at
+// every Runge-Kutta stage (radTPrtclTrj::TrjEqs, cpp/src/core/radptrj.h:91-105;
+// RungeKutta4 / Tabulation / RungeKuttaStep5 / AutoPropagate,
+// radptrj.cpp:94-240).  The stages of one trajectory are a dependent chain,
+// so one CTA carries one trajectory: at every stage its threads split the
+// (source, image) units, the partial fields are reduced in shared memory, and
+// every thread then advances an identical copy of the integrator state, so
+// the control flow (the step-size control included) stays uniform.  Many
+// trajectories run as many CTAs.
+// ---------------------------------------------------------------------------
+constexpr int TRJ_THREADS = 256;
+
+struct TrjArgs {
+  double y0, step, ctm;  // start, tabulation step (mm), charge / momentum (1 / (T mm))
+  int np, adaptive, max_steps;
+  long long max_evals;   // field evaluations allowed per trajectory (bounds the kernel's run time)
+  double prec[4], eps_tol;
+};
+
+// B at P from every unit, reduced over the block; every thread gets the sum
+__device__ V3<double> trj_block_field(const GeomView &g, V3<double> P, double *red)
+{
+  double ax = 0, ay = 0, az = 0;
+  for (int u = g.ustart[0] + threadIdx.x; u < g.ustart[1]; u += blockDim.x) {
+    V3<double> f = eval_unit<double, UK_REC>(g, __ldg(g.units + u), P, 0);
+    ax += f.x; ay += f.y; az += f.z;
+  }
+  for (int u = g.ustart[1] + threadIdx.x; u < g.ustart[2]; u += blockDim.x) {
+    V3<double> f = eval_unit<double, UK_POLY>(g, __ldg(g.units + u), P, 0);
+    ax += f.x; ay += f.y; az += f.z;
+  }
+  for (int u = g.ustart[2] + threadIdx.x; u < g.ustart[3]; u += blockDim.x) {
+    V3<double> f = eval_unit<double, UK_ARC>(g, __ldg(g.units + u), P, 0);
+    ax += f.x; ay += f.y; az += f.z;
+  }
+  for (int u = g.ustart[3] + threadIdx.x; u < g.ustart[4]; u += blockDim.x) {
+    V3<double> f = eval_unit<double, UK_BKG>(g, __ldg(g.units + u), P, 0);
+    ax += f.x; ay += f.y; az += f.z;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ax += __shfl_down_sync(0xffffffffu, ax, o);
+    ay += __shfl_down_sync(0xffffffffu, ay, o);
+    az += __shfl_down_sync(0xffffffffu, az, o);
+  }
+  int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();  // the previous stage's readers are done with red
+  if ((threadIdx.x & 31) == 0) { red[3 * w] = ax; red[3 * w + 1] = ay; red[3 * w + 2] = az; }
+  __syncthreads();
+  double bx = 0, by = 0, bz = 0;
+  for (int k = 0; k < nw; k++) { bx += red[3 * k]; by += red[3 * k + 1]; bz += red[3 * k + 2]; }
+  return mk3<double>(bx, by, bz);
+}
+
+// dF/dy for F = (x, x', z, z') at longitudinal position s
+__device__ void trj_eqs(const GeomView &g, const TrjArgs &a, double s, const double *F, double *dF, double *red,
+                        long long &ne)
+{
+  ne++;
+  double xd = F[1], zd = F[3];
+  double xdxd = xd * xd, zdzd = zd * zd, xdzd = xd * zd;
+  double buf = a.ctm * sqrt(1.0 + xdxd + zdzd);
+  V3<double> B = trj_block_field(g, mk3<double>(F[0], s, F[2]), red);
+  dF[0] = xd;
+  dF[1] = -buf * (zd * B.y - (1.0 + xdxd) * B.z + xdzd * B.x);
+  dF[2] = zd;
+  dF[3] = buf * (xd * B.y - (1.0 + zdzd) * B.x + xdzd * B.z);
+}
+
+// classical fourth-order step of size h from (x, y) with slope dydx
+__device__ void trj_rk4(const GeomView &g, const TrjArgs &a, const double *y, const double *dydx, double x, double h,
+                        double *yout, double *red, long long &ne)
+{
+  double hh = 0.5 * h, h6 = h / 6.0, xh = x + hh;
+  double yt[4], dyt[4], dym[4];
+  for (int i = 0; i < 4; i++) yt[i] = y[i] + hh * dydx[i];
+  trj_eqs(g, a, xh, yt, dyt, red, ne);
+  for (int i = 0; i < 4; i++) yt[i] = y[i] + hh * dyt[i];
+  trj_eqs(g, a, xh, yt, dym, red, ne);
+  for (int i = 0; i < 4; i++) {
+    yt[i] = y[i] + h * dym[i];
+    dym[i] += dyt[i];
+  }
+  trj_eqs(g, a, x + h, yt, dyt, red, ne);
+  for (int i = 0; i < 4; i++) yout[i] = y[i] + h6 * (dydx[i] + dyt[i] + 2.0 * dym[i]);
+}
+
+// step-doubling control: one step of size h against two of h/2, accepted when
+// the difference over prec, over eps_tol, is at most 1; 0 ok, 1 step too small,
+// 2 evaluation budget spent, 3 no acceptable step within the shrink limit
+__device__ int trj_step5(const GeomView &g, const TrjArgs &a, double *y, double *dydx, double *x, double htry,
+                         double *hdid, double *hnext, double *red, long long &ne)
+{
+  const double PGROW = -0.2, PSHRNK = -0.25, FCOR = 1.0 / 15.0, SAFETY = 0.9, ERRCON = 6.0e-04;
+  double xsav = *x, h = htry, ysav[4], dysav[4], ytemp[4];
+  for (int i = 0; i < 4; i++) { ysav[i] = y[i]; dysav[i] = dydx[i]; }
+  for (int it = 0; it < 200; it++) {
+    if (ne > a.max_evals) return 2;
+    double hh = 0.5 * h;
+    trj_rk4(g, a, ysav, dysav, xsav, hh, ytemp, red, ne);
+    *x = xsav + hh;
+    trj_eqs(g, a, *x, ytemp, dydx, red, ne);
+    trj_rk4(g, a, ytemp, dydx, *x, hh, y, red, ne);
+    *x = xsav + h;
+    if (*x == xsav) return 1;
+    trj_rk4(g, a, ysav, dysav, xsav, h, ytemp, red, ne);
+    double errmax = 0.0;
+    for (int i = 0; i < 4; i++) {
+      ytemp[i] = y[i] - ytemp[i];
+      double t = fabs(ytemp[i] / a.prec[i]);
+      if (errmax < t) errmax = t;
+    }
+    errmax /= a.eps_tol;
+    if (errmax <= 1.0) {
+      *hdid = h;
+      *hnext = (errmax > ERRCON ? SAFETY * h * exp(PGROW * log(errmax)) : 4.0 * h);
+      for (int i = 0; i < 4; i++) y[i] += ytemp[i] * FCOR;
+      return 0;
+    }
+    if (!(errmax < 1e300)) return 3;  // non-finite error: no step will be accepted
+    h *= SAFETY * exp(PSHRNK * log(errmax));
+  }
+  return 3;
+}
+
+// adaptive propagation of y from x1 to x2; 0 ok, 1 step too small, 2 step limit, 3 failure
+__device__ int trj_propagate(const GeomView &g, const TrjArgs &a, double *ystart, double x1, double x2, double h1,
+                             double hmin, double *red, long long &ne)
+{
+  double x = x1, h = (x2 > x1) ? fabs(h1) : -fabs(h1), y[4], dydx[4], hdid, hnext;
+  for (int i = 0; i < 4; i++) y[i] = ystart[i];
+  for (int n = 1; n <= a.max_steps; n++) {
+    trj_eqs(g, a, x, y, dydx, red, ne);
+    if ((x + h - x2) * (x + h - x1) > 0.0) h = x2 - x;
+    int rc = trj_step5(g, a, y, dydx, &x, h, &hdid, &hnext, red, ne);
+    if (rc) return rc;
+    if ((x - x2) * (x2 - x1) >= 0.0) {
+      for (int i = 0; i < 4; i++) ystart[i] = y[i];
+      return 0;
+    }
+    if (fabs(hnext) <= hmin) return 1;
+    h = hnext;
+  }
+  return 2;
+}
+
+// out[(b * np + i) * 5 + (y, x, x', z, z')]; status[b]: 0 ok, else the failure code
+__global__ void __launch_bounds__(TRJ_THREADS) trajectory_kernel(GeomView g, TrjArgs a, const double *__restrict__ init,
+                                                                double *__restrict__ out, int *__restrict__ status)
+{
+  __shared__ double red[3 * (TRJ_THREADS / 32)];
+  int b = blockIdx.x;
+  double Y[4], dY[4];
+  for (int k = 0; k < 4; k++) Y[k] = init[4 * b + k];
+  double x = a.y0, hmin = 1e-10 * a.step;
+  int rc = 0;
+  long long ne = 0;
+  for (int i = 0; i < a.np; i++) {
+    if (!a.adaptive) trj_eqs(g, a, x, Y, dY, red, ne);
+    if (threadIdx.x == 0) {
+      double *o = out + ((size_t)b * a.np + i) * 5;
+      o[0] = x;
+      for (int k = 0; k < 4; k++) o[1 + k] = Y[k];
+    }
+    if (i == a.np - 1 || rc) break;
+    double x1 = x + a.step;
+    if (a.adaptive) rc = trj_propagate(g, a, Y, x, x1, a.step, hmin, red, ne);
+    else trj_rk4(g, a, Y, dY, x, a.step, Y, red, ne);
+    x = x1;
+    if (rc) {
+      // rows after a failed interval repeat the last good state's position with NaN
+      for (int j = i + 1; j < a.np && threadIdx.x == 0; j++) {
+        double *o = out + ((size_t)b * a.np + j) * 5;
+        for (int k = 0; k < 5; k++) o[k] = __longlong_as_double(0x7ff8000000000000LL);
+      }
+      break;
+    }
+  }
+  if (threadIdx.x == 0) status[b] = rc;
+}
+
+int launch_trajectories(const GeomView &g, double energy_gev, const double *d_init, int n_traj, double y0, double y1,
+                        int np, const double *prec, double *d_out, int *d_status, cudaStream_t st)
+{
+  if (n_traj <= 0) return 0;
+  TrjArgs a;
+  a.y0 = y0;
+  a.np = np;
+  a.step = (np > 1) ? (y1 - y0) / (double)(np - 1) : 0.0;
+  a.ctm = -2.99792458e+05 / (1.e+09 * energy_gev);  // electron charge over momentum
+  a.adaptive = prec != nullptr;
+  a.max_steps = 5000;
+  a.max_evals = 40LL * np + 40000;
+  a.eps_tol = 1.0;
+  for (int k = 0; k < 4; k++) a.prec[k] = prec ? (prec[k] == 0.0 ? 1e23 : prec[k]) : 1.0;
+  trajectory_kernel<<<n_traj, TRJ_THREADS, 0, st>>>(g, a, d_init, d_out, d_status);
+  return check_launch("trajectory_kernel");
+}
+
 }  // namespace rb

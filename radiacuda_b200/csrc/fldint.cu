@@ -568,6 +568,8 @@ int field_int_impl(const RadB200Geom *g, const PointField &fld, const double *P1
 // device point field: points uploaded per refinement level, one launch per quantity
 DevGeom g_int_geom;
 DBuf g_int_pts, g_int_out, g_int_scratch;
+DevGeom g_trj_geom;
+DBuf g_trj_init, g_trj_out, g_trj_status;
 
 }  // namespace
 }  // namespace rb
@@ -623,6 +625,40 @@ int radb200_field_int_cb(const RadB200Geom *g, RadB200PointField fn, void *ctx, 
   if (status) {
     for (int d = 0; d < 5; d++) status[d] = st[d];
     status[5] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return 0;
+}
+
+int radb200_trajectories(const RadB200Geom *g, double energy_gev, int n_traj, const double *init, double y0, double y1,
+                         int np, const double *prec, double *out, int *status)
+{
+  if (!g || !init || !out || n_traj < 0 || np < 1 || !(energy_gev > 0) || !std::isfinite(y0) || !std::isfinite(y1)) {
+    set_error("bad trajectory arguments");
+    return RADB200_E_ARG;
+  }
+  if (n_traj == 0) return 0;
+  if ((size_t)n_traj * (size_t)np * 5 > ((size_t)1 << 31)) { set_error("too many trajectory points"); return RADB200_E_ARG; }
+  RB_TRY(g_trj_geom.upload(g));
+  RB_TRY(g_trj_init.upload(init, (size_t)n_traj * 4 * sizeof(double)));
+  size_t ob = (size_t)n_traj * np * 5 * sizeof(double);
+  RB_TRY(g_trj_out.alloc(ob));
+  RB_TRY(g_trj_status.alloc((size_t)n_traj * sizeof(int)));
+  RB_TRY(launch_trajectories(g_trj_geom.view(0), energy_gev, g_trj_init.as<double>(), n_traj, y0, y1, np, prec,
+                             g_trj_out.as<double>(), g_trj_status.as<int>(), 0));
+  RB_CUDA(cudaMemcpy(out, g_trj_out.p, ob, cudaMemcpyDeviceToHost));
+  std::vector<int> st(n_traj);
+  RB_CUDA(cudaMemcpy(st.data(), g_trj_status.p, (size_t)n_traj * sizeof(int), cudaMemcpyDeviceToHost));
+  int bad = 0, code = 0;
+  for (int b = 0; b < n_traj; b++) {
+    if (status) status[b] = st[b];
+    if (st[b] && !bad) { bad = b + 1; code = st[b]; }
+  }
+  if (bad) {
+    // the reference's messages (radiobuf.cpp:153-154)
+    set_error("trajectory %d: %s", bad - 1,
+              code == 1 ? "Radia::Error200: Step size is too small in automatic Runge-Kutta integration routine."
+                        : "Radia::Error201: Maximum number of steps exceeded in automatic Runge-Kutta integration routine.");
+    return RADB200_E_NOCONV;
   }
   return 0;
 }

@@ -199,5 +199,9 @@ int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what,
 int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int n,
                     int ld, float *N32, double *N64, cudaStream_t st);
 int launch_rowtrans_vec(const double *rowT, const double *in, double *out, int n, cudaStream_t st);
+// electron trajectories, one CTA each (field.cu); prec NULL: one RK4 step per
+// tabulation interval, else step-doubling control with these [4] accuracies
+int launch_trajectories(const GeomView &g, double energy_gev, const double *d_init, int n_traj, double y0, double y1,
+                        int np, const double *prec, double *d_out, int *d_status, cudaStream_t st);
 
 }  // namespace rb

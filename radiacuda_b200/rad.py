@@ -28,7 +28,7 @@ __all__ = [
     "ObjCnt", "ObjAddToCnt", "ObjCntStuf", "ObjCntSize", "ObjDivMag", "ObjM", "ObjSetM",
     "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
     "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
-    "RlxPre", "RlxAuto", "Solve", "Fld", "FldLst", "FldInt", "FldCmpCrt", "FldCmpPrc", "FldLenRndSw", "FldLenTol",
+    "RlxPre", "RlxAuto", "Solve", "Fld", "FldLst", "FldInt", "FldPtcTrj", "FldCmpCrt", "FldCmpPrc", "FldLenRndSw", "FldLenTol",
     "UtiDel", "UtiDelAll", "UtiVer", "UtiFldLastBackend", "UtiAsmLastBackend", "UtiGpuFallback",
 ]
 
@@ -704,6 +704,43 @@ def FldInt(obj: int, inf_or_fin: str, cmpn: str, P1, P2, precision: str = "doubl
         v = out[0:3] if q == "b" else out[3:6]
         vals.extend(float(x) for x in (v if comp is None else v[comp:comp + 1]))
     return vals[0] if len(vals) == 1 else vals
+
+
+def FldPtcTrj(obj: int, E: float, init, lims, np_: int):
+    """Relativistic electron trajectory in the field of obj (radpy FldPtcTrj,
+    radpy.cpp:2537-2569; radTApplication::ComputeParticleTrajectory,
+    radapl3.cpp:639-672): energy E (GeV), init [x0, dx/dy0, z0, dz/dy0] at
+    y = lims[0], tabulated at np_ points to lims[1].  Returns np_ lists
+    [y, x, dx/dy, z, dz/dy] (one flat list when np_ == 1).  With PrcCoord or
+    PrcAngle set positive (FldCmpCrt / FldCmpPrc) every interval is
+    integrated with step-doubling control, else with one fourth-order
+    Runge-Kutta step, as in the reference.  An extension: init given as an
+    [n, 4] array runs n trajectories at once (one CTA each) and returns an
+    [n, np_, 5] array."""
+    ini = np.asarray(init, dtype=np.float64)
+    lim = np.asarray(lims, dtype=np.float64).reshape(-1)
+    if lim.size != 2:
+        raise RadiaError("Radia::Error000: FldPtcTrj, incorrect definition of Y range")
+    batch = ini.ndim == 2
+    if (batch and ini.shape[1] != 4) or (not batch and ini.size != 4):
+        raise RadiaError("Radia::Error000: FldPtcTrj, incorrect definition of initial conditions")
+    n = int(np_)
+    if n < 1 or not (float(E) > 0):
+        raise RadiaError("Radia::Error000: FldPtcTrj: incorrect or missing function argument")
+    on = _prc["PrcCoord"] > 0 or _prc["PrcAngle"] > 0
+    prec = [_prc["PrcCoord"], _prc["PrcAngle"], _prc["PrcCoord"], _prc["PrcAngle"]] if on else None
+    geom = pack_sources(_objs, int(obj), tuple(_rand))
+    try:
+        out = _native.trajectories(geom, float(E), ini.reshape(-1, 4), lim[0], lim[1], n, prec)
+    except RuntimeError as e:
+        msg = str(e)
+        k = msg.find("Radia::Error")
+        raise RadiaError(msg[k:] if k >= 0 else msg) from None
+    _last_fld[0] = "gpu"
+    if batch:
+        return out
+    rows = [[float(v) for v in r] for r in out[0]]
+    return rows[0] if n == 1 else rows
 
 
 def FldCmpCrt(prcB: float, prcA: float, prcBint: float, prcFrc: float, prcTrjCrd: float, prcTrjAng: float) -> int:
