@@ -241,6 +241,21 @@ RADB200_API int radb200_field_int_cb(const RadB200Geom *g, RadB200PointField fn,
 RADB200_API int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r,
                          const RadB200Geom *ext, int storage, int64_t *handle);
 RADB200_API int radb200_intrc_free(int64_t handle);
+/* Save / restore the device state of an interaction (the solution state that
+ * UtiDmp / UtiDmpPrs would carry across processes, radintrc.cpp:1516,1946 of
+ * the reference dump the object tree only): the matrix as stored, the
+ * external field, the current and last converged magnetization and, when
+ * valid, the LU factors with their diagonal-block inverses.
+ * radb200_intrc_save: *bytes = size of the state; with buf != NULL and
+ * capacity >= that size the state is written there (host memory).
+ * radb200_intrc_restore: creates a new interaction from the same geometry,
+ * relaxation records, external sources and storage flags WITHOUT assembling
+ * and loads the state into it; the geometry stamp (a hash of element centres,
+ * frames, sources and materials) and the sizes must match the saved ones,
+ * else RADB200_E_ARG.                                                        */
+RADB200_API int radb200_intrc_save(int64_t handle, void *buf, int64_t capacity, int64_t *bytes);
+RADB200_API int radb200_intrc_restore(const RadB200Geom *elems, const RadB200Relax *r, const RadB200Geom *ext,
+                                      int storage, const void *buf, int64_t bytes, int64_t *handle);
 RADB200_API int radb200_intrc_size(int64_t handle, int32_t *n_elem, int32_t *storage);
 /* Copy the interaction matrix (row major, 3N x 3N) to a host buffer, as FP32
  * or FP64 (dtype 0 / 1), and the external field H_ext [3N].                 */

@@ -37,6 +37,8 @@ def lib():
         L.radb200_field_dev.argtypes = [_vp, C.c_void_p, _i64, C.c_int, C.c_int, C.c_void_p]
         L.radb200_intrc_create.argtypes = [_vp, _vp, _vp, C.c_int, C.POINTER(C.c_int64)]
         L.radb200_intrc_free.argtypes = [_i64]
+        L.radb200_intrc_save.argtypes = [_i64, C.c_void_p, _i64, C.POINTER(C.c_int64)]
+        L.radb200_intrc_restore.argtypes = [_vp, _vp, _vp, C.c_int, C.c_void_p, _i64, C.POINTER(C.c_int64)]
         L.radb200_intrc_size.argtypes = [_i64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.radb200_intrc_matrix.argtypes = [_i64, C.c_int, C.c_void_p]
         L.radb200_intrc_extfield.argtypes = [_i64, _dp]
@@ -141,17 +143,33 @@ def field_dev(geom: Dict[str, np.ndarray], d_pts_ptr: int, npts: int, what: int,
 class NativeInteraction:
     """Owner of a device-resident interaction (radb200_intrc_*)."""
 
-    def __init__(self, pack, storage: int = 0):
+    def __init__(self, pack, storage: int = 0, state: bytes = None):
+        """Assembles the interaction of pack on the device, or, given a state
+        saved by save(), restores it without assembling."""
         self.pack = pack
+        self.storage = storage
         self._g = GeomHolder(pack.elems)
         self._r = RelaxHolder(pack.elem_src, pack.mat_kind, pack.mat, pack.mh)
         self._x = GeomHolder(pack.ext) if pack.ext is not None else None
         h = C.c_int64(0)
-        check(lib().radb200_intrc_create(C.cast(self._g.ptr, _vp), C.cast(self._r.ptr, _vp),
-                                         C.cast(self._x.ptr, _vp) if self._x else None, storage, C.byref(h)),
-              "radb200_intrc_create")
+        xg = C.cast(self._x.ptr, _vp) if self._x else None
+        if state is None:
+            check(lib().radb200_intrc_create(C.cast(self._g.ptr, _vp), C.cast(self._r.ptr, _vp), xg, storage,
+                                             C.byref(h)), "radb200_intrc_create")
+        else:
+            buf = C.create_string_buffer(bytes(state), len(state))
+            check(lib().radb200_intrc_restore(C.cast(self._g.ptr, _vp), C.cast(self._r.ptr, _vp), xg, storage, buf,
+                                              len(state), C.byref(h)), "radb200_intrc_restore")
         self.handle = h.value
         self.n = pack.elem_src.shape[0]
+
+    def save(self) -> bytes:
+        """The interaction's device state (radb200_intrc_save)."""
+        n = C.c_int64(0)
+        check(lib().radb200_intrc_save(self.handle, None, 0, C.byref(n)), "radb200_intrc_save")
+        buf = C.create_string_buffer(n.value)
+        check(lib().radb200_intrc_save(self.handle, buf, n.value, C.byref(n)), "radb200_intrc_save")
+        return buf.raw[:n.value]
 
     def free(self):
         if self.handle:

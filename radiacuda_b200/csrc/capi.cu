@@ -368,8 +368,18 @@ int radb200_field(const RadB200Geom *g, const double *pts, int64_t npts, int wha
   return 0;
 }
 
-int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const RadB200Geom *ext, int storage,
-                         int64_t *handle)
+// FNV-1a over raw bytes: the interaction's geometry stamp
+static uint64_t fnv1a(uint64_t h, const void *p, size_t n)
+{
+  const unsigned char *b = (const unsigned char *)p;
+  for (size_t k = 0; k < n; k++) { h ^= b[k]; h *= 1099511628211ULL; }
+  return h;
+}
+
+// assemble = false builds everything but leaves the matrix zero (a restored
+// state fills it)
+static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, const RadB200Geom *ext, int storage,
+                             int64_t *handle, bool assemble)
 {
   int fast = (storage & RADB200_ASM_FAST) ? 1 : 0;
   storage &= ~RADB200_ASM_FAST;
@@ -416,6 +426,17 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   }
   RB_TRY(I->obs.upload(obs.data(), obs.size() * sizeof(double)));
   RB_TRY(I->rowT.upload(rowT.data(), rowT.size() * sizeof(double)));
+  {
+    uint64_t st = 1469598103934665603ULL;
+    int32_t hdr[3] = {n, storage, fast};
+    st = fnv1a(st, hdr, sizeof(hdr));
+    st = fnv1a(st, obs.data(), obs.size() * sizeof(double));
+    st = fnv1a(st, rowT.data(), rowT.size() * sizeof(double));
+    st = fnv1a(st, r->elem_src, 2 * (size_t)n * sizeof(int32_t));
+    st = fnv1a(st, r->mat_kind, (size_t)n * sizeof(int32_t));
+    st = fnv1a(st, r->mat, (size_t)n * RADB200_MAT_STRIDE * sizeof(double));
+    I->stamp = st;
+  }
   RB_TRY(I->elem_src.upload(r->elem_src, 2 * (size_t)n * sizeof(int)));
   RB_TRY(I->mat_kind.upload(r->mat_kind, (size_t)n * sizeof(int)));
   RB_TRY(I->mat.upload(r->mat, (size_t)n * RADB200_MAT_STRIDE * sizeof(double)));
@@ -426,8 +447,9 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   if (storage == RADB200_STORE_F32 || storage == RADB200_STORE_MIXED) RB_TRY(I->N32.alloc(nn * sizeof(float)));
   if (I->N64.p) RB_CUDA(cudaMemsetAsync(I->N64.p, 0, nn * sizeof(double)));
   if (I->N32.p) RB_CUDA(cudaMemsetAsync(I->N32.p, 0, nn * sizeof(float)));
-  RB_TRY(launch_assemble(I->geom.view(fast), I->elem_src.as<int>(), I->obs.as<double>(), I->rowT.as<double>(), n, I->ld,
-                         I->N32.as<float>(), I->N64.as<double>(), 0));
+  if (assemble)
+    RB_TRY(launch_assemble(I->geom.view(fast), I->elem_src.as<int>(), I->obs.as<double>(), I->rowT.as<double>(), n, I->ld,
+                           I->N32.as<float>(), I->N64.as<double>(), 0));
   // external field at element centres, in element frames
   size_t vb = (size_t)I->ld * sizeof(double);
   RB_TRY(I->hext.alloc(vb));
@@ -448,6 +470,138 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   int64_t h = g_next_handle++;
   g_intrc[h] = std::move(I);
   *handle = h;
+  return 0;
+}
+
+int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const RadB200Geom *ext, int storage,
+                         int64_t *handle)
+{
+  return intrc_create_impl(elems, r, ext, storage, handle, true);
+}
+
+// ---- saving and restoring the device state of an interaction --------------
+namespace {
+const char STATE_MAGIC[8] = {'R', 'B', '2', '0', '0', 'I', 'S', '1'};
+struct StateHeader {
+  char magic[8];
+  int32_t n, ld, storage, fast;
+  uint64_t stamp;
+  int32_t lu_mode, lu_tc, lu_of_d, last_kind;
+  int64_t solve_id, lu_solve_id;
+  int32_t nsec, pad;
+};
+enum { SEC_N64 = 1, SEC_N32, SEC_HEXT, SEC_M, SEC_LASTM, SEC_LU64, SEC_LU32, SEC_LUINV };
+struct Sec {
+  int64_t tag;
+  DBuf *buf;
+  int64_t bytes;
+};
+
+std::vector<Sec> state_sections(Intrc &I)
+{
+  const int64_t nn = (int64_t)I.n3 * I.ld, vb = (int64_t)I.ld * 8;
+  std::vector<Sec> v;
+  if (I.N64.p) v.push_back({SEC_N64, &I.N64, nn * 8});
+  if (I.N32.p) v.push_back({SEC_N32, &I.N32, nn * 4});
+  v.push_back({SEC_HEXT, &I.hext, vb});
+  v.push_back({SEC_M, &I.M, vb});
+  if (I.last_kind >= 0 && I.lastM.p) v.push_back({SEC_LASTM, &I.lastM, vb});
+  if (I.lu_mode >= 0) {
+    const int64_t es = (I.lu_mode == RADB200_LU_F64) ? 8 : 4;
+    if (I.LU64.p && es == 8) v.push_back({SEC_LU64, &I.LU64, nn * 8});
+    if (I.LU32.p && es == 4) v.push_back({SEC_LU32, &I.LU32, nn * 4});
+    v.push_back({SEC_LUINV, &I.LUinv, 2 * (int64_t)I.n3 * 128 * es});
+  }
+  return v;
+}
+}  // namespace
+
+int radb200_intrc_save(int64_t handle, void *buf, int64_t capacity, int64_t *bytes)
+{
+  Intrc *I = find_intrc(handle);
+  if (!I) return RADB200_E_HANDLE;
+  if (!bytes) { set_error("bad arguments"); return RADB200_E_ARG; }
+  std::vector<Sec> secs = state_sections(*I);
+  int64_t total = sizeof(StateHeader);
+  for (auto &x : secs) total += 16 + x.bytes;
+  *bytes = total;
+  if (!buf) return 0;
+  if (capacity < total) { set_error("state buffer too small: %lld bytes needed", (long long)total); return RADB200_E_ARG; }
+  StateHeader h{};
+  memcpy(h.magic, STATE_MAGIC, 8);
+  h.n = I->n; h.ld = I->ld; h.storage = I->storage; h.fast = I->fast; h.stamp = I->stamp;
+  h.lu_mode = I->lu_mode; h.lu_tc = I->lu_tc; h.lu_of_d = I->lu_of_d; h.last_kind = I->last_kind;
+  h.solve_id = I->solve_id; h.lu_solve_id = I->lu_solve_id; h.nsec = (int32_t)secs.size();
+  char *o = (char *)buf;
+  memcpy(o, &h, sizeof(h));
+  o += sizeof(h);
+  RB_CUDA(cudaDeviceSynchronize());
+  for (auto &x : secs) {
+    memcpy(o, &x.tag, 8);
+    memcpy(o + 8, &x.bytes, 8);
+    RB_CUDA(cudaMemcpy(o + 16, x.buf->p, (size_t)x.bytes, cudaMemcpyDeviceToHost));
+    o += 16 + x.bytes;
+  }
+  return 0;
+}
+
+int radb200_intrc_restore(const RadB200Geom *elems, const RadB200Relax *r, const RadB200Geom *ext, int storage,
+                          const void *buf, int64_t bytes, int64_t *handle)
+{
+  if (!buf || !handle || bytes < (int64_t)sizeof(StateHeader)) { set_error("bad state buffer"); return RADB200_E_ARG; }
+  StateHeader h;
+  memcpy(&h, buf, sizeof(h));
+  if (memcmp(h.magic, STATE_MAGIC, 8) != 0) { set_error("not a saved interaction state"); return RADB200_E_ARG; }
+  int64_t nh = 0;
+  RB_TRY(intrc_create_impl(elems, r, ext, storage, &nh, false));
+  Intrc *I = find_intrc(nh);
+  auto fail = [&](const char *why) {
+    g_intrc.erase(nh);
+    set_error("saved interaction state: %s", why);
+    return RADB200_E_ARG;
+  };
+  if (h.n != I->n || h.ld != I->ld || h.storage != I->storage || h.fast != I->fast)
+    return fail("sizes or storage differ from this geometry");
+  if (h.stamp != I->stamp) return fail("geometry stamp differs (other elements, images or materials)");
+  const char *p = (const char *)buf + sizeof(h), *end = (const char *)buf + bytes;
+  const int64_t nn = (int64_t)I->n3 * I->ld;
+  for (int k = 0; k < h.nsec; k++) {
+    if (end - p < 16) return fail("truncated");
+    int64_t tag, nb;
+    memcpy(&tag, p, 8);
+    memcpy(&nb, p + 8, 8);
+    p += 16;
+    if (nb < 0 || end - p < nb) return fail("truncated");
+    DBuf *dst = nullptr;
+    int64_t want = -1;
+    switch (tag) {
+      case SEC_N64: dst = &I->N64; want = nn * 8; break;
+      case SEC_N32: dst = &I->N32; want = nn * 4; break;
+      case SEC_HEXT: dst = &I->hext; want = (int64_t)I->ld * 8; break;
+      case SEC_M: dst = &I->M; want = (int64_t)I->ld * 8; break;
+      case SEC_LASTM: dst = &I->lastM; want = (int64_t)I->ld * 8; break;
+      case SEC_LU64: dst = &I->LU64; want = nn * 8; break;
+      case SEC_LU32: dst = &I->LU32; want = nn * 4; break;
+      case SEC_LUINV: dst = &I->LUinv; want = 2 * (int64_t)I->n3 * 128 * ((h.lu_mode == RADB200_LU_F64) ? 8 : 4); break;
+      default: return fail("unknown section");
+    }
+    if (nb != want) return fail("section size differs");
+    if (dst->alloc((size_t)nb) != 0) { g_intrc.erase(nh); return RADB200_E_NOMEM; }
+    if (cudaMemcpy(dst->p, p, (size_t)nb, cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      g_intrc.erase(nh);
+      set_error("saved interaction state: upload failed");
+      return RADB200_E_CUDA;
+    }
+    p += nb;
+  }
+  I->lu_mode = h.lu_mode;
+  I->lu_tc = h.lu_tc;
+  I->lu_of_d = h.lu_of_d;
+  I->last_kind = h.last_kind;
+  I->solve_id = (int)h.solve_id;
+  I->lu_solve_id = (int)h.lu_solve_id;
+  *handle = nh;
   return 0;
 }
 

@@ -130,6 +130,7 @@ struct Intrc {
   int lu_of_d = 0;                    // 1: the factors are of I - D N at the converged state of solve lu_solve_id
   int lu_solve_id = -1;
   int solve_id = 0;                   // counts relaxations / direct solves on this interaction
+  uint64_t stamp = 0;                 // hash of the element records, frames and materials
   DBuf lastM, lastH;                  // converged state of the last solve
   int last_kind = -1;                 // 0 relax, 1 direct
   // adjoint: external sources (kept for the gradient of H_ext at the centres),

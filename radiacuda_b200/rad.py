@@ -13,7 +13,9 @@ there is no CPU fallback -- a missing library or device raises.
 """
 from __future__ import annotations
 
+import io
 import math
+import pickle
 from typing import Any, Dict, List, Optional, Sequence
 
 import numpy as np
@@ -29,7 +31,7 @@ __all__ = [
     "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
     "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
     "RlxPre", "RlxAuto", "Solve", "Fld", "FldLst", "FldInt", "FldPtcTrj", "FldCmpCrt", "FldCmpPrc", "FldLenRndSw", "FldLenTol",
-    "UtiDel", "UtiDelAll", "UtiVer", "UtiFldLastBackend", "UtiAsmLastBackend", "UtiGpuFallback",
+    "UtiDel", "UtiDelAll", "UtiDmp", "UtiDmpPrs", "UtiVer", "UtiFldLastBackend", "UtiAsmLastBackend", "UtiGpuFallback",
 ]
 
 # --------------------------------------------------------------------------
@@ -809,6 +811,123 @@ def UtiDelAll() -> int:
         UtiDel(h)
     _next[0] = 1
     return 0
+
+
+_DMP_MAGIC = b"RADB200DMP\x01"
+
+
+def _dmp_closure(handles: Sequence[int]) -> Dict[int, Any]:
+    """Every object reachable from the handles (container members)."""
+    out: Dict[int, Any] = {}
+    stack = [int(h) for h in handles]
+    while stack:
+        h = stack.pop()
+        if h in out:
+            continue
+        o = _get(h)
+        out[h] = o
+        if isinstance(o, Container):
+            stack.extend(o.members)
+    return out
+
+
+def _dmp_asc(h: int, o) -> str:
+    lines = [f"Index: {h}"]
+    if isinstance(o, Interaction):
+        lines.append(f"   Relaxation interaction of {len(o.pack.leaves)} elements (device-resident)")
+    elif isinstance(o, Container):
+        lines.append(f"   Container of {len(o.members)} objects: {o.members}")
+    elif isinstance(o, RecMag):
+        lines.append("   Rectangular parallelepiped with " + ("current" if np.any(o.j != 0) else "magnetization"))
+        lines.append(f"   {{x,y,z}}= {{{o.c[0]},{o.c[1]},{o.c[2]}}}")
+        lines.append(f"   {{wx,wy,wz}}= {{{o.d[0]},{o.d[1]},{o.d[2]}}}")
+        lines.append(f"   {{mx,my,mz}}= {{{o.m[0]},{o.m[1]},{o.m[2]}}}")
+    elif isinstance(o, Polyhedron):
+        lines.append(f"   Polyhedron: {len(o.v)} vertices, {len(o.faces)} faces")
+        lines.append(f"   {{mx,my,mz}}= {{{o.m[0]},{o.m[1]},{o.m[2]}}}")
+    elif isinstance(o, ArcCur):
+        lines.append(f"   Arc current: centre {list(o.c)}, r {o.rmin}..{o.rmax}, phi {o.phimin}..{o.phimax}, "
+                     f"h {o.h}, j {o.j}, {o.nseg} segments")
+    elif isinstance(o, Bckg):
+        lines.append(f"   Uniform background field source {{bx,by,bz}}= {{{o.b[0]},{o.b[1]},{o.b[2]}}}")
+    elif isinstance(o, Material):
+        lines.append(f"   Material (kind {o.kind})")
+    elif isinstance(o, Trf):
+        lines.append("   Space transformation")
+    if isinstance(o, Obj) and o.trfs:
+        lines.append(f"   {len(o.trfs)} transformation(s) attached")
+    return "\n".join(lines)
+
+
+def UtiDmp(elem, fmt: str = "asc"):
+    """Dump of objects (radpy UtiDmp; the reference's dump,
+    radintrc.cpp:1516, covers the object tree).  'asc': a text description.
+    'bin': bytes that UtiDmpPrs turns back into objects in this or another
+    process -- every object reachable from elem (containers, materials,
+    transformations) and, for an interaction from RlxPre, its device state
+    (matrix, external field, magnetization, LU factors) so that the solution
+    state survives a restart without reassembly.  The binary form is this
+    library's own (not the reference's byte layout); load only dumps you
+    made, like any pickle-based format."""
+    handles = [int(x) for x in (elem if isinstance(elem, (list, tuple)) else [elem])]
+    f = str(fmt).lower()
+    if f.startswith("asc"):
+        return "\n".join(_dmp_asc(h, _get(h)) for h in handles)
+    if not f.startswith("bin"):
+        raise RadiaError("Radia::Error000: UtiDmp: format must be 'asc' or 'bin'")
+    objs: Dict[int, Any] = {}
+    intrc: Dict[int, Any] = {}
+    for h in handles:
+        o = _get(h)
+        if isinstance(o, Interaction):
+            intrc[h] = {"pack": o.pack, "storage": o.native.storage, "state": o.native.save(), "M": o.M}
+        else:
+            objs.update(_dmp_closure([h]))
+    payload = {"roots": handles, "single": not isinstance(elem, (list, tuple)), "objs": objs, "intrc": intrc}
+    return _DMP_MAGIC + pickle.dumps(payload, protocol=4)
+
+
+class _DmpUnpickler(pickle.Unpickler):
+    """Only this package's model classes, numpy arrays and builtins."""
+    _ok_modules = ("radiacuda_b200.model", "numpy", "numpy.core.multiarray", "numpy._core.multiarray",
+                   "numpy.core.numeric", "numpy._core.numeric", "builtins", "collections")
+
+    def find_class(self, module, name):
+        if module in self._ok_modules and not name.startswith("_") or (module.endswith("multiarray") and
+                                                                       name == "_reconstruct"):
+            if module == "builtins" and name not in ("list", "dict", "tuple", "set", "frozenset", "int", "float",
+                                                     "complex", "bool", "str", "bytes", "slice", "range"):
+                raise pickle.UnpicklingError(f"UtiDmpPrs: {module}.{name} not allowed")
+            return super().find_class(module, name)
+        raise pickle.UnpicklingError(f"UtiDmpPrs: {module}.{name} not allowed")
+
+
+def UtiDmpPrs(bstr: bytes):
+    """Instantiates the objects (and interactions) of a UtiDmp(..., 'bin')
+    dump under new handles (radpy UtiDmpPrs); returns the new handle of the
+    dumped element, or a list for a dumped list."""
+    b = bytes(bstr)
+    if not b.startswith(_DMP_MAGIC):
+        raise RadiaError("Radia::Error000: UtiDmpPrs: not a dump made by UtiDmp(..., 'bin')")
+    payload = _DmpUnpickler(io.BytesIO(b[len(_DMP_MAGIC):])).load()
+    remap: Dict[int, int] = {}
+    # new handles in the old handles' order: containers iterate their members
+    # by handle, so the traversal order (and every result) is preserved
+    for old in sorted(payload["objs"]):
+        remap[int(old)] = _add(payload["objs"][old])
+    for o in payload["objs"].values():
+        if isinstance(o, Container):
+            o.members = sorted(remap.get(m, m) for m in o.members)
+    for old, rec in payload["intrc"].items():
+        pack = rec["pack"]
+        for lf in pack.leaves:
+            lf.handle = remap.get(lf.handle, lf.handle)
+        nat = _native.NativeInteraction(pack, rec["storage"], state=rec["state"])
+        it = Interaction(pack, nat)
+        it.M = rec["M"]
+        remap[int(old)] = _add(it)
+    out = [remap[int(h)] for h in payload["roots"]]
+    return out[0] if payload["single"] else out
 
 
 def UtiVer() -> float:
