@@ -238,7 +238,6 @@ int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs)
 {
   RB_TRY(validate_geom(G));
   all_tets = 0;
-  tets_identity = 0;
   if (G->n_poly > 0) {
     HostTopo h;
     build_topo(G, tensor_coeffs, h);
@@ -256,35 +255,6 @@ int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs)
     RB_TRY(tetidx.upload(h.tetidx.data(), h.tetidx.size() * sizeof(int)));
     RB_TRY(tetrec.upload(h.tetrec.data(), h.tetrec.size() * sizeof(double)));
     all_tets = std::all_of(h.tetidx.begin(), h.tetidx.end(), [](int t) { return t >= 0; }) ? 1 : 0;
-    if (all_tets && !tensor_coeffs) {
-      bool ident = true;
-      for (int i = 0; i < G->n_poly && ident; i++) {
-        if (G->poly_info[4 * i + 3] != 1) { ident = false; break; }
-        const double *T = G->trf + (size_t)G->poly_info[4 * i + 2] * RADB200_TRF_STRIDE;
-        for (int k = 0; k < 21 && ident; k++) {
-          // [0, 9) M^-1 and [12, 21) sM the identity, [9, 12) V zero
-          double want = (k < 9) ? ((k % 4 == 0) ? 1.0 : 0.0) : (k < 12 ? 0.0 : (((k - 12) % 4 == 0) ? 1.0 : 0.0));
-          if (T[k] != want) ident = false;
-        }
-      }
-      if (ident) {
-        std::vector<float> f((size_t)G->n_poly * TET_REC_FIELD);
-        std::vector<double> c((size_t)G->n_poly * 3);
-        for (int i = 0; i < G->n_poly; i++) {
-          const double *r = h.tetrec.data() + (size_t)h.tetidx[i] * TET_REC_FIELD;
-          double cc[3] = {0, 0, 0};
-          for (int k = 0; k < 4; k++)
-            for (int d = 0; d < 3; d++) cc[d] += 0.25 * r[3 * k + d];
-          for (int d = 0; d < 3; d++) c[3 * (size_t)i + d] = cc[d];
-          float *o = f.data() + (size_t)i * TET_REC_FIELD;
-          for (int k = 0; k < 12; k++) o[k] = (float)(r[k] - cc[k % 3]);
-          for (int k = 12; k < TET_REC_FIELD; k++) o[k] = (float)r[k];
-        }
-        RB_TRY(tetf.upload(f.data(), f.size() * sizeof(float)));
-        RB_TRY(tetc.upload(c.data(), c.size() * sizeof(double)));
-        tets_identity = 1;
-      }
-    }
   }
   RB_TRY(trf.upload(G->trf, (size_t)G->n_trf * RADB200_TRF_STRIDE * sizeof(double)));
   RB_TRY(rec.upload(G->rec, (size_t)G->n_rec * RADB200_REC_STRIDE * sizeof(double)));
@@ -334,9 +304,6 @@ GeomView DevGeom::view(int fast) const
   v.tetidx = tetidx.as<int>();
   v.tetrec = tetrec.as<double>();
   v.all_tets = all_tets;
-  v.tets_identity = tets_identity;
-  v.tetf = tetf.as<float>();
-  v.tetc = tetc.as<double>();
   return v;
 }
 

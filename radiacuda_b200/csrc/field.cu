@@ -263,134 +263,6 @@ static int launch_tet_ppt(const GeomView &g, const double *d_pts, int64_t npts, 
   return check_launch("chunk_reduce_kernel");
 }
 
-// FP32 terms for tetrahedra whose image is the identity: vertex offsets from
-// the tetrahedron's centroid, distances, edge logarithms and solid angles are
-// FP32 (the point enters through one FP64 difference, point - centroid); the
-// logarithms and angles are weighted by the FP64 edge / face vectors and
-// summed in FP64, because those sums cancel to the order of (size / distance)
-// of their terms and FP32 weights would carry that amplification.
-constexpr int T32_TILE = 64;
-constexpr int T32_F = 30;  // floats per unit: offsets (12), edge lengths (6), m_t (12)
-constexpr int T32_D = 36;  // doubles per unit: centroid (3), M (3), a_f (12), g_e (18)
-
-__device__ __forceinline__ void tet32_unit(const float *__restrict__ r, const double *__restrict__ w, V3<double> P,
-                                           int what, double *acc)
-{
-  const double C = 1.0 / (4.0 * 3.141592653589793238);
-  const float qx = (float)(P.x - w[0]), qy = (float)(P.y - w[1]), qz = (float)(P.z - w[2]);
-  float rx[4], ry[4], rz[4], R[4];
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    rx[k] = r[3 * k] - qx;
-    ry[k] = r[3 * k + 1] - qy;
-    rz[k] = r[3 * k + 2] - qz;
-    R[k] = sqrtf(rx[k] * rx[k] + ry[k] * ry[k] + rz[k] * rz[k]);
-  }
-  float d[6];
-#pragma unroll
-  for (int e = 0; e < 6; e++) {
-    const int a = tet_edge_a(e), b = tet_edge_b(e);
-    d[e] = rx[a] * rx[b] + ry[a] * ry[b] + rz[a] * rz[b];
-  }
-  double ax = 0.0, ay = 0.0, az = 0.0;
-#pragma unroll
-  for (int e = 0; e < 6; e++) {
-    const int a = tet_edge_a(e), b = tet_edge_b(e);
-    const float l = r[12 + e];
-    float D;
-    if (d[e] >= 0.f) D = R[a] * R[b] + d[e];
-    else {
-      float cx = ry[a] * rz[b] - rz[a] * ry[b], cy = rz[a] * rx[b] - rx[a] * rz[b], cz = rx[a] * ry[b] - ry[a] * rx[b];
-      D = (cx * cx + cy * cy + cz * cz) / (R[a] * R[b] - d[e]);
-    }
-    const double L = (double)log1pf(l * (R[a] + R[b] + l) / D);
-    ax += L * w[18 + 3 * e]; ay += L * w[19 + 3 * e]; az += L * w[20 + 3 * e];
-  }
-  double omega_tot = 0.0;
-#pragma unroll
-  for (int f = 0; f < 4; f++) {
-    const int a = tet_face_a(f), b = tet_face_b(f), c = tet_face_c(f);
-    const float num = rx[a] * r[18 + 3 * f] + ry[a] * r[19 + 3 * f] + rz[a] * r[20 + 3 * f];
-    const float den = R[a] * R[b] * R[c] + d[tet_pair(a, b)] * R[c] + d[tet_pair(a, c)] * R[b] + d[tet_pair(b, c)] * R[a];
-    const double om = 2.0 * (double)atan2f(-num, den);
-    omega_tot += om;
-    ax += om * w[6 + 3 * f]; ay += om * w[7 + 3 * f]; az += om * w[8 + 3 * f];
-  }
-  const bool in = omega_tot < -6.283185307179586;
-  if (what == 2) {
-    if (in) { acc[0] += w[3]; acc[1] += w[4]; acc[2] += w[5]; }
-    return;
-  }
-  acc[0] += C * ax;
-  acc[1] += C * ay;
-  acc[2] += C * az;
-  if (what == 0 && in) { acc[0] += w[3]; acc[1] += w[4]; acc[2] += w[5]; }
-}
-
-__global__ void __launch_bounds__(128) field_tet32_kernel(GeomView g, const double *__restrict__ pts, int64_t npts,
-                                                          int what, double *__restrict__ out, int ub, int ue, int chunk,
-                                                          int accumulate)
-{
-  __shared__ float sf[T32_TILE * T32_F];
-  __shared__ double sw[T32_TILE * T32_D];
-  const int tid = threadIdx.x;
-  const int64_t i0 = (int64_t)blockIdx.x * 128 + tid;
-  const int u0 = ub + blockIdx.y * chunk, u1 = min(ue, u0 + chunk);
-  V3<double> P = mk3<double>(0, 0, 0);
-  if (i0 < npts) P = mk3<double>(pts[3 * i0], pts[3 * i0 + 1], pts[3 * i0 + 2]);
-  double a[3] = {0, 0, 0};
-  for (int base = u0; base < u1; base += T32_TILE) {
-    const int cnt = min(T32_TILE, u1 - base);
-    __syncthreads();
-    for (int e = tid; e < cnt * T32_F; e += 128) {
-      const int k = e / T32_F, f = e - k * T32_F;
-      const int p = __ldg(&g.units[base + k].y);
-      sf[e] = __ldg(g.tetf + (size_t)p * TET_REC_FIELD + f);
-    }
-    for (int e = tid; e < cnt * T32_D; e += 128) {
-      const int k = e / T32_D, f = e - k * T32_D;
-      const int p = __ldg(&g.units[base + k].y);
-      double v;
-      if (f < 3) v = __ldg(g.tetc + 3 * (size_t)p + f);
-      else if (f < 6) v = __ldg(g.poly + (size_t)p * RADB200_POLY_STRIDE + f);
-      else v = __ldg(g.tetrec + (size_t)__ldg(g.tetidx + p) * TET_REC_FIELD + 24 + f);  // record [30, 60)
-      sw[e] = v;
-    }
-    __syncthreads();
-    for (int k = 0; k < cnt; k++) tet32_unit(sf + k * T32_F, sw + k * T32_D, P, what, a);
-  }
-  if (i0 < npts) {
-    double *o = out + ((size_t)blockIdx.y * npts + i0) * 3;
-    if (accumulate) { o[0] += a[0]; o[1] += a[1]; o[2] += a[2]; }
-    else { o[0] = a[0]; o[1] = a[1]; o[2] = a[2]; }
-  }
-}
-
-static int launch_tet32(const GeomView &g, const double *d_pts, int64_t npts, int what, double *d_out, int ub, int ue,
-                        int accumulate, DBuf &scratch, cudaStream_t st)
-{
-  int64_t nblk = (npts + 127) / 128;
-  int nu = ue - ub;
-  int nchunk = 1;
-  const int64_t target = 148 * 6;
-  if (nblk < target) nchunk = (int)((target + nblk - 1) / nblk);
-  if (nchunk > nu) nchunk = nu;
-  if (nchunk > 65535) nchunk = 65535;
-  int chunk = (nu + nchunk - 1) / nchunk;
-  nchunk = (nu + chunk - 1) / chunk;
-  dim3 grid((unsigned)nblk, (unsigned)nchunk);
-  if (nchunk == 1) {
-    field_tet32_kernel<<<grid, 128, 0, st>>>(g, d_pts, npts, what, d_out, ub, ue, chunk, accumulate);
-    return check_launch("field_tet32_kernel");
-  }
-  RB_TRY(scratch.alloc((size_t)nchunk * npts * 3 * sizeof(double)));
-  field_tet32_kernel<<<grid, 128, 0, st>>>(g, d_pts, npts, what, scratch.as<double>(), ub, ue, chunk, 0);
-  RB_TRY(check_launch("field_tet32_kernel"));
-  int64_t n3 = npts * 3;
-  chunk_reduce_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(scratch.as<double>(), nchunk, n3, d_out, accumulate);
-  return check_launch("chunk_reduce_kernel");
-}
-
 // points per thread: 1 (more resident warps) or 2 (two interleaved chains);
 // RADB200_TET_PPT overrides the default for tuning
 template <typename T>
@@ -451,8 +323,6 @@ int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what,
     int rc;
     if (kind == 0)
       rc = launch_kind<double, UK_REC>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
-    else if (kind == 1 && g.fast && g.all_tets && precision == 1 && g.tets_identity)
-      rc = launch_tet32(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
     else if (kind == 1 && g.fast && g.all_tets)
       rc = (precision == 1) ? launch_tet<float>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st)
                             : launch_tet<double>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);

@@ -91,11 +91,6 @@ struct GeomView {
   const double *tetrec;
   int all_tets;       // every polyhedron has a tetrahedron record
   int fast;           // 1: evaluate polyhedra in the vertex/edge form
-  // every polyhedron unit is a tetrahedron with the identity image: FP32
-  // vertex offsets from each tetrahedron's vertex centroid (tet32 kernel)
-  int tets_identity;
-  const float *tetf;   // [n_poly * TET_REC_FIELD] offsets [0, 12), then the record's [12, 60) as floats
-  const double *tetc;  // [n_poly * 3] vertex centroid
 };
 
 struct DevGeom {
@@ -103,10 +98,9 @@ struct DevGeom {
   // polyhedron topology (vertex/edge form), see TopoView in formulas.cuh
   DBuf tinfo, tinfo2, tv, te, tel, teg, teG, tt, ttm, tfn, tfa;
   DBuf tetidx, tetrec;  // fixed-topology tetrahedron records (tet_fast)
-  DBuf tetf, tetc;      // FP32 centroid-relative records (identity images only)
   int n_units = 0, n_rec = 0, n_poly = 0;
   int ustart[5] = {0, 0, 0, 0, 0};
-  int all_tets = 0, tets_identity = 0;
+  int all_tets = 0;
   Guard g{0, 0, 0};
   int upload(const RadB200Geom *G, bool tensor_coeffs = false);
   GeomView view(int fast = 0) const;

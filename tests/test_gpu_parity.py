@@ -208,28 +208,6 @@ def test_fast_polyhedron_fp32_field(cuda, rad):
     assert rel_err(_native.field(g, P, 0, 1), O.field(g, P, 0)) < 5e-5
 
 
-def test_tet32_field_inside_outside_and_images(cuda, rad):
-    """FP32 terms for tetrahedra with identity images (centroid-relative
-    records) against the oracle: B and H outside and inside the mesh, M at the
-    points; a mesh whose tetrahedra carry symmetry images takes the general
-    FP32 path."""
-    h, c = _build(rad, "tet_mesh_150")
-    _randomize_m(rad, h, 9)
-    g = model.pack_sources(rad._objs, h, tuple(rad._rand))
-    rng = np.random.default_rng(12)
-    P = np.concatenate([np.array(c["points"]), rng.uniform(0.1, 5.9, size=(400, 3)) + 0.00137])
-    for what in (0, 1):
-        assert rel_err(_native.field(g, P, what, 1), O.field(g, P, what)) < 5e-5
-    assert np.array_equal(_native.field(g, P, 2, 1), O.field(g, P, 2))
-    Po = np.array(c["points"])
-    assert rel_err(_native.field(g, Po, 0, 1), O.field(g, Po, 0)) < 2e-6
-    hm, cm = _build(rad, "mixed_sym")
-    _randomize_m(rad, hm, 3)
-    gm = model.pack_sources(rad._objs, hm, tuple(rad._rand))
-    Pm = np.array(cm["points"])
-    assert rel_err(_native.field(gm, Pm, 0, 1), O.field(gm, Pm, 0)) < 5e-5
-
-
 @pytest.mark.parametrize("name", ["tet_mesh_150", "mixed_sym"])
 def test_fast_polyhedron_assembly_matches_oracle(cuda, rad, name):
     h, c = _build(rad, name)
