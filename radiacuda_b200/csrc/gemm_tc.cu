@@ -564,7 +564,9 @@ __global__ void tc_transpose_kernel(const float *__restrict__ B, int ldb, int k,
   }
 }
 
-static DBuf g_tc_bt;   // B^T scratch, [n x ldbt] floats, ldbt = k rounded up to 4
+// B^T scratch, [n x ldbt] floats, ldbt = k rounded up to 4; one per slot so
+// that updates on two streams (the LU's look-ahead) never share it
+static DBuf g_tc_bt_slots[2];
 
 // max_ctas > 0 caps the persistent grid (the self-test uses it to make every
 // CTA loop over several tiles)
@@ -610,8 +612,9 @@ static int encode_map(CUtensorMap *map, const float *base, int rows, int cols, i
 }
 
 static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb,
-                     cudaStream_t st, int overwrite = 0, int max_ctas = 0, int use_tma = -1)
+                     cudaStream_t st, int overwrite = 0, int max_ctas = 0, int use_tma = -1, int slot = 0)
 {
+  DBuf &g_tc_bt = g_tc_bt_slots[slot & 1];
   if (use_tma < 0) use_tma = g_tc_tma;
   long long tiles = (long long)((n + TC_BN - 1) / TC_BN) * ((m + TC_BM - 1) / TC_BM);
   if (tiles > (1ll << 30) || k < 1 || k > (1 << 20)) { set_error("tensor-core update shape out of range"); return RADB200_E_ARG; }
@@ -727,7 +730,7 @@ static int tc_selftest()
 }
 
 int tc_gemm_f32(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb, cudaStream_t st,
-                int *used, int overwrite)
+                int *used, int overwrite, int slot, int max_ctas)
 {
   *used = 0;
   if (getenv("RADB200_NO_TC")) return 0;
@@ -737,7 +740,7 @@ int tc_gemm_f32(float *C, int ldc, int m, int n, int k, float *A, int lda, const
   if (g_tc_state < 0) RB_TRY(tc_selftest());
   if (g_tc_state <= 0) return 0;
   RB_TRY(g_tc_err_flag.alloc(sizeof(int)));
-  RB_TRY(launch_tc(C, ldc, m, n, k, A, lda, B, ldb, st, overwrite));
+  RB_TRY(launch_tc(C, ldc, m, n, k, A, lda, B, ldb, st, overwrite, max_ctas, -1, slot));
   *used = 1;
   return 0;
 }

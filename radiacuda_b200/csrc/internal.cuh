@@ -190,8 +190,10 @@ int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_sec
 // C[m x n] -= A[m x k] B[k x n] (overwrite != 0: C = A B), FP32 row-major,
 // any k, leading dimensions multiples of 4, 16-byte aligned pointers, C not
 // aliasing A or B.  A is rounded to TF32 in place.
+// slot selects one of two B^T scratch buffers (updates on two streams must use
+// different slots); max_ctas > 0 caps the persistent grid
 int tc_gemm_f32(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb, cudaStream_t st,
-                int *used, int overwrite = 0);
+                int *used, int overwrite = 0, int slot = 0, int max_ctas = 0);
 int tc_error_flag(int *flag);  // 2 when a tensor-core CTA hit its wait limit
 
 // ---- kernels (launch wrappers) ---------------------------------------------

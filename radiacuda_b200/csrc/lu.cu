@@ -393,74 +393,149 @@ static double g_upd_bytes = 0.0, g_upd_flops = 0.0;
 // drops by LU_OUTER / 128 against 128-wide steps.
 constexpr int LU_OUTER = 512;
 
+// One-panel look-ahead: the trailing update of outer step k is split into the
+// columns of panel k+1 (on the main stream, first) and the rest (on a side
+// stream, its grid capped to leave LU_SIDE_FREE_SMS multiprocessors free), so
+// that panel k+1 -- its single-CTA diagonal factorizations, narrow GEMMs and
+// copies -- is factored on the main stream while the rest of the update runs.
+// The main stream waits for the side stream before the U block row of step
+// k+1, the only later work that reads or writes the columns the side stream
+// updates.  Events order the two streams; nothing waits on the device.
+constexpr int LU_SIDE_FREE_SMS = 12;  // swept 4-74 on the 60,000^2 factorization: 12 was fastest
+
+struct LuStreams {
+  cudaStream_t main = nullptr, side = nullptr;
+  cudaEvent_t in = nullptr, upd = nullptr, side_done = nullptr, out = nullptr;
+  int init()
+  {
+    if (main) return 0;
+    RB_CUDA(cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking));
+    RB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&in, &upd, &side_done, &out}) RB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return 0;
+  }
+};
+static LuStreams g_lu_streams;
+
 template <typename T>
 static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaStream_t st, int *tc_used)
 {
   const int n3 = I.n3, ld = I.ld;
   const int smax = LU_NB * (LU_NB + 1) * (int)sizeof(double);
   RB_CUDA(cudaFuncSetAttribute(diag_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-  // RADB200_LU_TIMING=1 prints the time of each phase (synchronizes per phase)
+  // RADB200_LU_TIMING=1 prints the time of each phase (synchronizes per phase);
+  // RADB200_LU_LOOKAHEAD=0 runs every phase on the caller's stream
   const bool timing = getenv("RADB200_LU_TIMING") != nullptr;
+  const char *la = getenv("RADB200_LU_LOOKAHEAD");
+  const bool lookahead = !(la && atoi(la) == 0);
   double tph[4] = {0, 0, 0, 0};
   auto t_last = std::chrono::steady_clock::now();
   auto phase = [&](int p) -> int {
     if (!timing) return 0;
-    RB_CUDA(cudaStreamSynchronize(st));
+    RB_CUDA(cudaDeviceSynchronize());
     auto t = std::chrono::steady_clock::now();
     tph[p] += std::chrono::duration<double>(t - t_last).count();
     t_last = t;
     return 0;
   };
+  cudaStream_t sm = st, ss = st;
+  int side_ctas = 0;
+  if (lookahead) {
+    RB_TRY(g_lu_streams.init());
+    sm = g_lu_streams.main;
+    ss = g_lu_streams.side;
+    RB_CUDA(cudaEventRecord(g_lu_streams.in, st));
+    RB_CUDA(cudaStreamWaitEvent(sm, g_lu_streams.in, 0));
+    RB_CUDA(cudaStreamWaitEvent(ss, g_lu_streams.in, 0));
+    int dev = 0, nsm = 0;
+    RB_CUDA(cudaGetDevice(&dev));
+    RB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const char *fs = getenv("RADB200_LU_FREE_SMS");  // tuning override
+    side_ctas = std::max(1, nsm - ((fs && atoi(fs) > 0) ? atoi(fs) : LU_SIDE_FREE_SMS));
+  }
+  bool side_pending = false;
   auto at = [&](int r, int c) { return A + (size_t)r * ld + c; };
+  // C[m x n] -= A B with the update's timing events on stream q
+  auto update = [&](T *C, int m, int n, int k, T *Ap, const T *Bp, cudaStream_t q, int slot, int cap) -> int {
+    if (m <= 0 || n <= 0) return 0;
+    if (g_update_timing) {
+      RB_TRY(g_upd_ev.grow());
+      RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used], q));
+    }
+    int used = 0;
+    if (sizeof(T) == 4) {
+      RB_TRY(tc_gemm_f32((float *)C, ld, m, n, k, (float *)Ap, ld, (const float *)Bp, ld, q, &used, 0, slot, cap));
+      if (used) *tc_used = 1;
+    }
+    if (!used) RB_TRY(gemm<T>(C, ld, m, n, k, Ap, ld, Bp, ld, 0, q, tc_used));
+    if (g_update_timing) {
+      RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used + 1], q));
+      g_upd_ev.used++;
+      // algorithmic bytes: C read + written, the L and U panels read once
+      g_upd_bytes += (double)sizeof(T) * (2.0 * m * n + (double)m * k + (double)k * n);
+      g_upd_flops += 2.0 * m * n * k;
+    }
+    return 0;
+  };
   for (int K0 = 0; K0 < n3; K0 += LU_OUTER) {
     const int NBe = std::min(LU_OUTER, n3 - K0);
     const int pend = K0 + NBe;  // end of the panel's columns
-    // ---- factor the panel columns [K0, pend) over rows [K0, n3)
+    // ---- factor the panel columns [K0, pend) over rows [K0, n3) (main stream;
+    // the previous step updated these columns there first)
     for (int j0 = K0; j0 < pend; j0 += LU_NB) {
       const int jb = std::min(LU_NB, pend - j0);
-      diag_factor_kernel<T><<<1, DIAG_T, (size_t)jb * (jb + 1) * sizeof(double), st>>>(A, ld, j0, jb, Linv, Uinv, d_err);
+      diag_factor_kernel<T><<<1, DIAG_T, (size_t)jb * (jb + 1) * sizeof(double), sm>>>(A, ld, j0, jb, Linv, Uinv, d_err);
       RB_TRY(check_launch("diag_factor_kernel"));
       RB_TRY(phase(0));
       const int rest = j0 + jb, m = n3 - rest;
       if (m <= 0) break;
       // L21 = A21 U_jj^-1   (tmp: m x LU_NB)
-      RB_TRY(gemm<T>(tmp, LU_NB, m, jb, jb, at(rest, j0), ld, Uinv + (size_t)j0 * LU_NB, LU_NB, 1, st, tc_used));
-      RB_TRY(copy2d<T>(at(rest, j0), ld, tmp, LU_NB, m, jb, st));
+      RB_TRY(gemm<T>(tmp, LU_NB, m, jb, jb, at(rest, j0), ld, Uinv + (size_t)j0 * LU_NB, LU_NB, 1, sm, tc_used));
+      RB_TRY(copy2d<T>(at(rest, j0), ld, tmp, LU_NB, m, jb, sm));
       const int w = pend - rest;  // panel columns right of this step
       if (w > 0) {
         // U12 inside the panel = L_jj^-1 A12   (tmp: jb x w)
-        RB_TRY(gemm<T>(tmp, ld, jb, w, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, rest), ld, 1, st, tc_used));
-        RB_TRY(copy2d<T>(at(j0, rest), ld, tmp, ld, jb, w, st));
+        RB_TRY(gemm<T>(tmp, ld, jb, w, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, rest), ld, 1, sm, tc_used));
+        RB_TRY(copy2d<T>(at(j0, rest), ld, tmp, ld, jb, w, sm));
         // narrow update of the panel: A[rest:, rest:pend] -= L21 U12
-        RB_TRY(gemm<T>(at(rest, rest), ld, m, w, jb, at(rest, j0), ld, at(j0, rest), ld, 0, st, tc_used));
+        RB_TRY(gemm<T>(at(rest, rest), ld, m, w, jb, at(rest, j0), ld, at(j0, rest), ld, 0, sm, tc_used));
       }
       RB_TRY(phase(1));
     }
     const int T0 = pend, mT = n3 - pend;
     if (mT <= 0) break;
+    // the columns right of this panel must carry the previous step's update
+    if (side_pending) {
+      RB_CUDA(cudaEventRecord(g_lu_streams.side_done, ss));
+      RB_CUDA(cudaStreamWaitEvent(sm, g_lu_streams.side_done, 0));
+      side_pending = false;
+    }
     // ---- U block row of the trailing columns: forward substitution with the
     // panel's unit-lower diagonal block, 128 rows at a time
     for (int j0 = K0; j0 < pend; j0 += LU_NB) {
       const int jb = std::min(LU_NB, pend - j0);
-      if (j0 > K0) RB_TRY(gemm<T>(at(j0, T0), ld, jb, mT, j0 - K0, at(j0, K0), ld, at(K0, T0), ld, 0, st, tc_used));
-      RB_TRY(gemm<T>(tmp, ld, jb, mT, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, T0), ld, 1, st, tc_used));
-      RB_TRY(copy2d<T>(at(j0, T0), ld, tmp, ld, jb, mT, st));
+      if (j0 > K0) RB_TRY(gemm<T>(at(j0, T0), ld, jb, mT, j0 - K0, at(j0, K0), ld, at(K0, T0), ld, 0, sm, tc_used));
+      RB_TRY(gemm<T>(tmp, ld, jb, mT, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, T0), ld, 1, sm, tc_used));
+      RB_TRY(copy2d<T>(at(j0, T0), ld, tmp, ld, jb, mT, sm));
     }
     RB_TRY(phase(2));
-    // ---- trailing update A22 -= L21 U12 with K = NBe
-    if (g_update_timing) {
-      RB_TRY(g_upd_ev.grow());
-      RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used], st));
-    }
-    RB_TRY(gemm<T>(at(T0, T0), ld, mT, mT, NBe, at(T0, K0), ld, at(K0, T0), ld, 0, st, tc_used));
-    if (g_update_timing) {
-      RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used + 1], st));
-      g_upd_ev.used++;
-      // algorithmic bytes: C read + written, the L and U panels read once
-      g_upd_bytes += (double)sizeof(T) * (2.0 * mT * mT + 2.0 * mT * NBe);
-      g_upd_flops += 2.0 * mT * mT * NBe;
+    // ---- trailing update A22 -= L21 U12 with K = NBe: the next panel's
+    // columns on the main stream, the rest on the side stream
+    const int nxt = lookahead ? std::min(LU_OUTER, mT) : mT;
+    RB_TRY(update(at(T0, T0), mT, nxt, NBe, at(T0, K0), at(K0, T0), sm, 0, 0));
+    if (mT > nxt) {
+      RB_CUDA(cudaEventRecord(g_lu_streams.upd, sm));
+      RB_CUDA(cudaStreamWaitEvent(ss, g_lu_streams.upd, 0));
+      RB_TRY(update(at(T0, T0 + nxt), mT, mT - nxt, NBe, at(T0, K0), at(K0, T0 + nxt), ss, 1, side_ctas));
+      side_pending = true;
     }
     RB_TRY(phase(3));
+  }
+  if (lookahead) {
+    RB_CUDA(cudaEventRecord(g_lu_streams.side_done, ss));
+    RB_CUDA(cudaStreamWaitEvent(sm, g_lu_streams.side_done, 0));
+    RB_CUDA(cudaEventRecord(g_lu_streams.out, sm));
+    RB_CUDA(cudaStreamWaitEvent(st, g_lu_streams.out, 0));
   }
   if (timing)
     fprintf(stderr, "[radb200 LU n=%d %s] diag %.3f s, panel %.3f s, U block rows %.3f s, trailing %.3f s\n", n3,
