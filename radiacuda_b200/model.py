@@ -494,12 +494,60 @@ class InteractionPack:
     main: List[Trf] = field(default_factory=list)
 
 
+# Packed sources of recent (handle, rand) pairs.  Objects are immutable
+# through the API except for their magnetization (relaxation write-back,
+# ObjSetM), and transformations are only ever added; so an entry stays valid
+# while the walk meets the same objects with transformation lists of the same
+# lengths, and only the M columns are refreshed.  The entry holds the leaves, so no
+# object id it compares can be reused while it lives.
+_SRC_CACHE: Dict[Tuple[int, Tuple[float, ...]], tuple] = {}
+_SRC_CACHE_MAX = 4
+
+
+def _leaf_key(leaves: List[Leaf]) -> np.ndarray:
+    # object identity and the length of its transformation list (transforms
+    # are only ever added, at the front)
+    k = np.empty((len(leaves), 2), dtype=np.int64)
+    k[:, 0] = np.fromiter((id(lf.obj) for lf in leaves), dtype=np.int64, count=len(leaves))
+    k[:, 1] = np.fromiter((len(lf.trf_list) for lf in leaves), dtype=np.int64, count=len(leaves))
+    return k
+
+
+def clear_source_cache():
+    _SRC_CACHE.clear()
+
+
 def pack_sources(objs, handle, rand) -> Dict[str, np.ndarray]:
+    """Flat source arrays of the object tree under handle (RadB200Geom).
+    Returns fresh arrays: callers may modify them."""
+    leaves = collect_leaves(objs, handle)
+    key = (int(handle), tuple(float(x) for x in rand))
+    fp = _leaf_key(leaves)
+    hit = _SRC_CACHE.get(key)
+    if hit is not None and hit[0].shape == fp.shape and np.array_equal(hit[0], fp):
+        _, arrays, slots, _ = hit
+        for name, col, rows, objs_m in slots:
+            if rows.size:
+                arrays[name][rows, col:col + 3] = np.array([o.m for o in objs_m], dtype=np.float64)
+        return {k: v.copy() for k, v in arrays.items()}
     p = Packed()
     p.abs_rand, p.rel_rand, p.zero_rand = rand
-    for lf in collect_leaves(objs, handle):
-        p.add_leaf(lf)
-    return p.arrays()
+    rec_rows, rec_objs, poly_rows, poly_objs = [], [], [], []
+    for lf in leaves:
+        kind, idx = p.add_leaf(lf)
+        if kind == 0 and hasattr(lf.obj, "m"):
+            rec_rows.append(idx)
+            rec_objs.append(lf.obj)
+        elif kind == 1:
+            poly_rows.append(idx)
+            poly_objs.append(lf.obj)
+    arrays = p.arrays()
+    slots = [("rec", 6, np.array(rec_rows, dtype=np.int64), rec_objs),
+             ("poly", 3, np.array(poly_rows, dtype=np.int64), poly_objs)]
+    if len(_SRC_CACHE) >= _SRC_CACHE_MAX:
+        _SRC_CACHE.pop(next(iter(_SRC_CACHE)))
+    _SRC_CACHE[key] = (fp, arrays, slots, leaves)
+    return {k: v.copy() for k, v in arrays.items()}
 
 
 def pack_interaction(objs, handle, srcobj, rand) -> InteractionPack:

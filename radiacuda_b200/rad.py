@@ -20,7 +20,7 @@ from typing import Any, Dict, List, Optional, Sequence
 
 import numpy as np
 
-from . import _native
+from . import _native, model
 from .model import (ArcCur, Bckg, Container, InteractionPack, Material, Obj, Polyhedron, RadiaError,
                     RecMag, Trf, collect_leaves, images_of, pack_interaction, pack_sources, trf_field_inversion,
                     trf_plane_sym, trf_rotation, trf_translation)
@@ -810,6 +810,7 @@ def UtiDelAll() -> int:
     for h in list(_objs):
         UtiDel(h)
     _next[0] = 1
+    model.clear_source_cache()
     return 0
 
 

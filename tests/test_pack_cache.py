@@ -1,0 +1,38 @@
+"""The packed-source cache returns exactly what a fresh packing returns:
+after a magnetization change, after added transformations and container
+members, and with returned arrays that callers may modify."""
+import numpy as np
+
+import models as MD
+from radiacuda_b200 import model
+
+
+def _fresh(rad, h):
+    model.clear_source_cache()
+    return model.pack_sources(rad._objs, h, tuple(rad._rand))
+
+
+def _same(a, b):
+    return sorted(a) == sorted(b) and all(a[k].shape == b[k].shape and np.array_equal(a[k], b[k]) for k in a)
+
+
+def test_cache_follows_magnetization_transforms_and_members(rad):
+    h = MD.mixed_sym(rad)
+    g0 = model.pack_sources(rad._objs, h, tuple(rad._rand))
+    g0["poly"][:] = -7.0                         # callers may modify what they get
+    assert _same(model.pack_sources(rad._objs, h, tuple(rad._rand)), _fresh(rad, h))
+    leaves = model.collect_leaves(rad._objs, h)
+    for k, lf in enumerate(leaves):
+        if hasattr(lf.obj, "m"):
+            lf.obj.m = np.array([0.1 * k, -0.2, 0.3])
+    assert _same(model.pack_sources(rad._objs, h, tuple(rad._rand)), _fresh(rad, h))
+    rad.TrfOrnt(h, rad.TrfRot([1, 2, 3], [0, 1, 1], 0.4))
+    assert _same(model.pack_sources(rad._objs, h, tuple(rad._rand)), _fresh(rad, h))
+    extra = rad.ObjRecMag([90, 0, 0], [2, 2, 2], [0, 0, 1])
+    rad.ObjAddToCnt(h, [extra])
+    assert _same(model.pack_sources(rad._objs, h, tuple(rad._rand)), _fresh(rad, h))
+    rad.FldLenRndSw("on")
+    try:
+        assert _same(model.pack_sources(rad._objs, h, tuple(rad._rand)), _fresh(rad, h))
+    finally:
+        rad.FldLenRndSw("off")
