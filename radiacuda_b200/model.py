@@ -515,6 +515,7 @@ def _leaf_key(leaves: List[Leaf]) -> np.ndarray:
 
 def clear_source_cache():
     _SRC_CACHE.clear()
+    _INT_CACHE.clear()
 
 
 def pack_sources(objs, handle, rand) -> Dict[str, np.ndarray]:
@@ -550,16 +551,72 @@ def pack_sources(objs, handle, rand) -> Dict[str, np.ndarray]:
     return {k: v.copy() for k, v in arrays.items()}
 
 
+_INT_CACHE: Dict[tuple, tuple] = {}
+
+
+def _int_key(leaves: List[Leaf]) -> np.ndarray:
+    k = np.empty((len(leaves), 3), dtype=np.int64)
+    k[:, :2] = _leaf_key(leaves)
+    k[:, 2] = np.fromiter((id(getattr(lf.obj, "mat", None)) for lf in leaves), dtype=np.int64, count=len(leaves))
+    return k
+
+
+def _refresh_m(arrays, slots):
+    for name, col, rows, objs_m in slots:
+        if rows.size:
+            arrays[name][rows, col:col + 3] = np.array([o.m for o in objs_m], dtype=np.float64)
+
+
+def _m_slots(kinds_objs):
+    rec_rows, rec_objs, poly_rows, poly_objs = [], [], [], []
+    for (kind, idx), o in kinds_objs:
+        if kind == 0 and hasattr(o, "m"):
+            rec_rows.append(idx)
+            rec_objs.append(o)
+        elif kind == 1:
+            poly_rows.append(idx)
+            poly_objs.append(o)
+    return [("rec", 6, np.array(rec_rows, dtype=np.int64), rec_objs),
+            ("poly", 3, np.array(poly_rows, dtype=np.int64), poly_objs)]
+
+
 def pack_interaction(objs, handle, srcobj, rand) -> InteractionPack:
+    """Relaxable elements, their materials and the external sources of the
+    object tree under handle (plus srcobj).  Cached like pack_sources: the
+    entry is reused while the walk meets the same objects, transformation
+    list lengths and materials; magnetizations and the material records that
+    depend on them are refreshed."""
+    leaves = collect_leaves(objs, handle)
+    sleaves = collect_leaves(objs, srcobj) if srcobj else []
+    key = (int(handle), int(srcobj), tuple(float(x) for x in rand))
+    fp = _int_key(leaves + sleaves)
+    hit = _INT_CACHE.get(key)
+    if hit is not None and hit[0].shape == fp.shape and np.array_equal(hit[0], fp):
+        _, pack, eslots, xslots, _ = hit
+        _refresh_m(pack.elems, eslots)
+        if pack.ext is not None:
+            _refresh_m(pack.ext, xslots)
+        mats = pack.mat
+        for e, lf in enumerate(pack.leaves):
+            o = lf.obj
+            if o.mat.kind != 2:
+                mats[e] = o.mat.record(o.m)
+        return InteractionPack(
+            elems={k: v.copy() for k, v in pack.elems.items()},
+            ext=({k: v.copy() for k, v in pack.ext.items()} if pack.ext is not None else None),
+            elem_src=pack.elem_src.copy(), mat_kind=pack.mat_kind.copy(), mat=mats.copy(), mh=pack.mh.copy(),
+            leaves=list(pack.leaves), main=list(pack.main))
     pe, px = Packed(), Packed()
     pe.abs_rand, pe.rel_rand, pe.zero_rand = rand
     px.abs_rand, px.rel_rand, px.zero_rand = rand
     elem_src, mat_kind, mats, mh_rows, relax_leaves, mains = [], [], [], [], [], []
+    eko, xko = [], []
     n_ext = 0
-    for lf in collect_leaves(objs, handle):
+    for lf in leaves:
         o = lf.obj
         if getattr(o, "relaxable", False):
             kind, idx = pe.add_leaf(lf)
+            eko.append(((kind, idx), o))
             elem_src.append((kind, idx))
             mat = o.mat
             rec = mat.record(o.m)
@@ -573,15 +630,14 @@ def pack_interaction(objs, handle, srcobj, rand) -> InteractionPack:
             relax_leaves.append(lf)
             mains.append(pe.last_images[0])
         else:
-            px.add_leaf(lf)
+            xko.append((px.add_leaf(lf), o))
             n_ext += 1
-    if srcobj:
-        for lf in collect_leaves(objs, srcobj):
-            px.add_leaf(lf)
-            n_ext += 1
+    for lf in sleaves:
+        xko.append((px.add_leaf(lf), lf.obj))
+        n_ext += 1
     if not elem_src:
         raise RadiaError("Radia::Error118: no relaxable elements (apply a material first)")
-    return InteractionPack(
+    pack = InteractionPack(
         elems=pe.arrays(), ext=(px.arrays() if n_ext else None),
         elem_src=np.ascontiguousarray(np.array(elem_src, dtype=np.int32).reshape(-1, 2)),
         mat_kind=np.ascontiguousarray(np.array(mat_kind, dtype=np.int32)),
@@ -589,6 +645,14 @@ def pack_interaction(objs, handle, srcobj, rand) -> InteractionPack:
         mh=(np.ascontiguousarray(np.array(mh_rows, dtype=np.float64).reshape(-1, 3))
             if mh_rows else np.zeros((0, 3))),
         leaves=relax_leaves, main=mains)
+    if len(_INT_CACHE) >= _SRC_CACHE_MAX:
+        _INT_CACHE.pop(next(iter(_INT_CACHE)))
+    _INT_CACHE[key] = (fp, pack, _m_slots(eko), _m_slots(xko), leaves + sleaves)
+    return InteractionPack(
+        elems={k: v.copy() for k, v in pack.elems.items()},
+        ext=({k: v.copy() for k, v in pack.ext.items()} if pack.ext is not None else None),
+        elem_src=pack.elem_src.copy(), mat_kind=pack.mat_kind.copy(), mat=pack.mat.copy(), mh=pack.mh.copy(),
+        leaves=list(relax_leaves), main=list(mains))
 
 
 def element_centres(pack: InteractionPack) -> np.ndarray:

@@ -36,3 +36,28 @@ def test_cache_follows_magnetization_transforms_and_members(rad):
         assert _same(model.pack_sources(rad._objs, h, tuple(rad._rand)), _fresh(rad, h))
     finally:
         rad.FldLenRndSw("off")
+
+
+def _same_pack(a, b):
+    return (_same(a.elems, b.elems) and ((a.ext is None and b.ext is None) or _same(a.ext, b.ext))
+            and all(np.array_equal(getattr(a, k), getattr(b, k)) for k in ("elem_src", "mat_kind", "mat", "mh"))
+            and [id(lf.obj) for lf in a.leaves] == [id(lf.obj) for lf in b.leaves])
+
+
+def test_interaction_cache_follows_magnetization_and_materials(rad):
+    h = MD.mixed_sym(rad)
+    rand = tuple(rad._rand)
+    p0 = model.pack_interaction(rad._objs, h, 0, rand)
+    p0.mat[:] = 0.0
+    model.clear_source_cache()
+    assert _same_pack(model.pack_interaction(rad._objs, h, 0, rand), model.pack_interaction(rad._objs, h, 0, rand))
+    for k, lf in enumerate(model.collect_leaves(rad._objs, h)):
+        if hasattr(lf.obj, "m"):
+            lf.obj.m = np.array([0.2, 0.1 * k, -0.4])
+    cached = model.pack_interaction(rad._objs, h, 0, rand)
+    model.clear_source_cache()
+    assert _same_pack(cached, model.pack_interaction(rad._objs, h, 0, rand))
+    rad.MatApl(h, rad.MatLin([0.3, 0.1], [0.0, 0.0, 1.0]))
+    cached = model.pack_interaction(rad._objs, h, 0, rand)
+    model.clear_source_cache()
+    assert _same_pack(cached, model.pack_interaction(rad._objs, h, 0, rand))
