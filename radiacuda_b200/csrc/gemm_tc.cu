@@ -116,8 +116,25 @@ __device__ __forceinline__ void tc_issue_chunk(uint32_t sa, uint32_t sb, const f
 }
 
 // overwrite == 0: C -= A B;  overwrite == 1: C = A B.  C must not alias A or B.
+// Tile order of the persistent grid: bands of TC_TILE_GROUP n-tiles, and
+// inside a band the n-tiles fastest, then the rows.  The CTAs running at any
+// moment then cover about (grid / 16) row blocks of one 16-tile band, so the
+// band's B^T slice (16 x 256 x K) stays in L2 for the whole band and the A
+// panel is streamed once per band, instead of the whole B^T panel once per
+// row of tiles when a row is wider than L2 holds (60,000 columns: 120 MB).
+constexpr int TC_TILE_GROUP = 16;
+__device__ __forceinline__ void tile_rc(int t, int tiles_m, int tiles_n, int &row0, int &col0)
+{
+  const int band = t / (TC_TILE_GROUP * tiles_m);
+  const int n0 = band * TC_TILE_GROUP;
+  const int gw = min(TC_TILE_GROUP, tiles_n - n0);
+  const int r = t - band * TC_TILE_GROUP * tiles_m;
+  row0 = (r / gw) * TC_BM;
+  col0 = (n0 + r % gw) * TC_BN;
+}
+
 // Bt = B^T (n x ldbt, K contiguous).  Persistent: CTA b handles tiles b,
-// b + gridDim.x, ... (n-tiles fastest, so neighbouring CTAs share A rows in L2).
+// b + gridDim.x, ... in the banded order of tile_rc.
 // Every tile runs ceil(k / 64) chunks through a two-stage pipeline: chunk g+1
 // is copied into the other stage while the MMAs of chunk g run; the tile's C
 // values are loaded into registers at its first chunk and consumed at its
@@ -167,12 +184,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
 
   {  // chunk 0 into stage 0
     const int t0 = blockIdx.x;
-    tc_issue_chunk(s0, s0 + TC_STAGE_A, A, lda, Bt, ldbt, m, n, k, 0, (t0 / tiles_n) * TC_BM, (t0 % tiles_n) * TC_BN, tid);
+    int r0, c0;
+    tile_rc(t0, tiles_m, tiles_n, r0, c0);
+    tc_issue_chunk(s0, s0 + TC_STAGE_A, A, lda, Bt, ldbt, m, n, k, 0, r0, c0, tid);
   }
   for (int g = 0; g < G; g++) {
     const int i = g / nch, c = g - i * nch;
     const int tile = blockIdx.x + i * gridDim.x;
-    const int row0 = (tile / tiles_n) * TC_BM, col0 = (tile % tiles_n) * TC_BN;
+    int row0, col0;
+    tile_rc(tile, tiles_m, tiles_n, row0, col0);
     const int st = g & 1;
     unsigned char *sa = sbase + st * TC_STAGE, *sb = sa + TC_STAGE_A;
     // ---- this chunk's operands (already TF32 values): wait for the copies
@@ -203,8 +223,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_update_kernel(float *__restr
       const int i1 = (g + 1) / nch, c1 = (g + 1) - i1 * nch;
       const int t1 = blockIdx.x + i1 * gridDim.x;
       const uint32_t so = s0 + (st ^ 1) * TC_STAGE;
-      tc_issue_chunk(so, so + TC_STAGE_A, A, lda, Bt, ldbt, m, n, k, c1 * TC_KC, (t1 / tiles_n) * TC_BM,
-                     (t1 % tiles_n) * TC_BN, tid);
+      int r1, c1b;
+      tile_rc(t1, tiles_m, tiles_n, r1, c1b);
+      tc_issue_chunk(so, so + TC_STAGE_A, A, lda, Bt, ldbt, m, n, k, c1 * TC_KC, r1, c1b, tid);
     }
     // ---- first chunk of a tile: this thread's C values (row r, 128 columns)
     if (c == 0) {
@@ -407,8 +428,10 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
         const int tt = blockIdx.x + ii * gridDim.x;
         const uint32_t so = s0 + (gg % TM_NST) * TM_STAGE, fb = smem_u32(&full[gg % TM_NST]);
         mbar_expect_tx(fb, (uint32_t)TM_STAGE);
-        tma_load_2d(so, &tmA, cc * TM_KC, (tt / tiles_n) * TC_BM, fb);
-        tma_load_2d(so + TM_STAGE_A, &tmB, cc * TM_KC, (tt % tiles_n) * TC_BN, fb);
+        int rr, ccol;
+        tile_rc(tt, tiles_m, tiles_n, rr, ccol);
+        tma_load_2d(so, &tmA, cc * TM_KC, rr, fb);
+        tma_load_2d(so + TM_STAGE_A, &tmB, cc * TM_KC, ccol, fb);
       };
       for (; issued < TM_NST - 1 && issued < G; issued++) issue(issued);
       const uint32_t idesc = umma_idesc(0);
@@ -461,7 +484,8 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
     const int r = q * 32 + lane;
     for (int i = 0; i < my_tiles; i++) {
       const int tile = blockIdx.x + i * gridDim.x;
-      const int row0 = (tile / tiles_n) * TC_BM, col0 = (tile % tiles_n) * TC_BN;
+      int row0, col0;
+      tile_rc(tile, tiles_m, tiles_n, row0, col0);
       const int buf = i & 1;
       const int gr = row0 + r, gcb = col0 + hc * 128;
       float4 cv[32];
