@@ -25,6 +25,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -179,8 +180,10 @@ def run_ours(args, rank, world):
     err = float(np.abs(B_mixed - B_plain).max() / np.abs(B_plain).max()) if B_plain is not None else None
 
     times, t_asm, t_solve, t_fld = [], [], [], []
-    clocks = Clocks(os.path.join(ROOT, "gpurun_out", f"bench_clocks_r{rank}.csv") if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
-                    else f"/tmp/bench_clocks_r{rank}.csv")
+    # the raw samples go to BENCH_CLOCKS_DIR (default: the temp directory); the
+    # JSON line carries their summary
+    clocks = Clocks(os.path.join(os.environ.get("BENCH_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"bench_clocks_r{rank}.csv"))
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
