@@ -241,6 +241,12 @@ RADB200_API int radb200_field_int_cb(const RadB200Geom *g, RadB200PointField fn,
 RADB200_API int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r,
                          const RadB200Geom *ext, int storage, int64_t *handle);
 RADB200_API int radb200_intrc_free(int64_t handle);
+/* Device blocks of 256 MB and more (matrices, factors) are kept for reuse when
+ * released, up to RADB200_BUFCACHE_GB (environment; default 40% of the
+ * device's memory, 0 = off), so that repeated create / free cycles do not
+ * unmap and remap tens of GB each time.  No counterpart in the reference.
+ * This call returns every kept block to the driver.                         */
+RADB200_API int radb200_release_cached_memory(void);
 /* Save / restore the device state of an interaction (the solution state that
  * UtiDmp / UtiDmpPrs would carry across processes, radintrc.cpp:1516,1946 of
  * the reference dump the object tree only): the matrix as stored, the

@@ -34,6 +34,82 @@ int check_launch(const char *what)
   return 0;
 }
 
+// ---- reuse of large device blocks -----------------------------------------
+// Released blocks of BIG_BLOCK bytes and more wait here (after the device is
+// idle, so no kernel still uses them) until an allocation of at most 25% less
+// takes them, up to a cap of RADB200_BUFCACHE_GB (default: 40% of the device's
+// memory; 0 turns reuse off).  A failed cudaMalloc returns every cached block
+// to the driver and tries again; radb200_release_cached_memory does the same
+// on request.  The pool is never destroyed (blocks outlive static DBufs).
+namespace {
+struct BigPool {
+  std::multimap<size_t, void *> blocks;
+  size_t total = 0, cap = 0;
+  bool init = false;
+};
+BigPool &big_pool()
+{
+  static BigPool *bp = new BigPool();
+  if (!bp->init) {
+    bp->init = true;
+    const char *e = getenv("RADB200_BUFCACHE_GB");
+    if (e) bp->cap = (size_t)(atof(e) * 1073741824.0);
+    else {
+      size_t fr = 0, tot = 0;
+      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) bp->cap = tot / 10 * 4;
+      else cudaGetLastError();
+    }
+  }
+  return *bp;
+}
+void big_flush(BigPool &bp)
+{
+  for (auto &kv : bp.blocks) cudaFree(kv.second);
+  bp.blocks.clear();
+  bp.total = 0;
+}
+}  // namespace
+
+void big_release_all() { big_flush(big_pool()); }
+
+void *big_alloc(size_t b, size_t *got)
+{
+  BigPool &bp = big_pool();
+  auto it = bp.blocks.lower_bound(b);
+  if (it != bp.blocks.end() && it->first <= b + b / 4) {
+    void *p = it->second;
+    *got = it->first;
+    bp.total -= it->first;
+    bp.blocks.erase(it);
+    return p;
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, b) != cudaSuccess) {
+    cudaGetLastError();
+    big_flush(bp);
+    if (cudaMalloc(&p, b) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("device allocation of %zu bytes failed", b);
+      return nullptr;
+    }
+  }
+  *got = b;
+  return p;
+}
+
+void big_free(void *p, size_t b)
+{
+  BigPool &bp = big_pool();
+  if (bp.total + b <= bp.cap && cudaDeviceSynchronize() == cudaSuccess) {
+    bp.blocks.emplace(b, p);
+    bp.total += b;
+    return;
+  }
+  cudaGetLastError();
+  cudaFree(p);
+}
+
+
 static int validate_geom(const RadB200Geom *G)
 {
   if (!G) { set_error("null geometry"); return RADB200_E_ARG; }
@@ -602,6 +678,12 @@ int radb200_intrc_restore(const RadB200Geom *elems, const RadB200Relax *r, const
   I->solve_id = (int)h.solve_id;
   I->lu_solve_id = (int)h.lu_solve_id;
   *handle = nh;
+  return 0;
+}
+
+int radb200_release_cached_memory(void)
+{
+  rb::big_release_all();
   return 0;
 }
 

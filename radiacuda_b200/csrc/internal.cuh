@@ -32,6 +32,14 @@ int check_launch(const char *what);   // cudaGetLastError after a launch
   } while (0)
 
 // ---- device buffers ----------------------------------------------------------
+// Blocks of BIG_BLOCK bytes and more are kept for reuse when released (up to
+// a cap, see big_free in capi.cu): an interaction's 10-60 GB of matrix and
+// factors would otherwise be unmapped and mapped again by every create/free.
+constexpr size_t BIG_BLOCK = (size_t)256 << 20;
+void *big_alloc(size_t b, size_t *got);  // nullptr on failure (error set)
+void big_free(void *p, size_t b);
+void big_release_all();
+
 struct DBuf {
   void *p = nullptr;
   size_t bytes = 0;
@@ -41,7 +49,10 @@ struct DBuf {
   ~DBuf() { release(); }
   void release()
   {
-    if (p) cudaFree(p);
+    if (p) {
+      if (bytes >= BIG_BLOCK) big_free(p, bytes);
+      else cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
   }
@@ -50,6 +61,13 @@ struct DBuf {
     if (b <= bytes && p) return 0;
     release();
     if (b == 0) return 0;
+    if (b >= BIG_BLOCK) {
+      size_t got = 0;
+      p = big_alloc(b, &got);
+      if (!p) return RADB200_E_NOMEM;
+      bytes = got;
+      return 0;
+    }
     if (cudaMalloc(&p, b) != cudaSuccess) {
       cudaGetLastError();
       set_error("device allocation of %zu bytes failed", b);
