@@ -281,7 +281,7 @@ def run_ours(args, rank, world):
     return res
 
 
-def adjoint_ratio(reps=3):
+def adjoint_ratio(reps=5):
     """Second half of the metric: wall time of one full adjoint gradient over
     one forward solve, through radiacuda_b200.adjoint.FieldProblem (the public
     API: host parameters in, host field / gradients out), on
@@ -291,7 +291,9 @@ def adjoint_ratio(reps=3):
         about 6,000 elements, mirror plane (2 images), B at 1e5 points,
         Newton-Krylov relaxation.
     Forward = assembly + solve + field; adjoint = field VJP + transposed solve
-    + derivative contractions.  Median of `reps` after one warm-up."""
+    + derivative contractions.  Median of `reps` after one warm-up; every
+    rep's times and the SM clocks sampled over each case are kept, since a
+    single slow rep on a shared host moves a median of few."""
     import torch
 
     from radiacuda_b200 import adjoint as A
@@ -306,21 +308,26 @@ def adjoint_ratio(reps=3):
         prob = A.FieldProblem(h, pts, "b", prec=1e-12)
         W = np.random.default_rng(1).normal(size=pts.shape)
         tf, tb = [], []
-        for r in range(reps + 1):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            prob.forward()
-            torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            prob.backward(W)
-            torch.cuda.synchronize()
-            t2 = time.perf_counter()
-            if r:
-                tf.append(t1 - t0)
-                tb.append(t2 - t1)
+        clk = Clocks(os.path.join(os.environ.get("BENCH_CLOCKS_DIR", tempfile.gettempdir()),
+                                  f"radb200_adjoint_clocks_{os.getpid()}_{name}.csv"))
+        with clk:
+            for r in range(reps + 1):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                prob.forward()
+                torch.cuda.synchronize()
+                t1 = time.perf_counter()
+                prob.backward(W)
+                torch.cuda.synchronize()
+                t2 = time.perf_counter()
+                if r:
+                    tf.append(t1 - t0)
+                    tb.append(t2 - t1)
         f, b = float(np.median(tf)), float(np.median(tb))
         out[name] = {"n_elements": int(prob.n), "n_points": int(pts.shape[0]), "forward_s": round(f, 4),
                      "adjoint_s": round(b, 4), "adjoint_over_forward": round(b / f, 3),
+                     "forward_reps_s": [round(x, 4) for x in tf], "adjoint_reps_s": [round(x, 4) for x in tb],
+                     "clocks": clk.summary(int(os.environ.get("LOCAL_RANK", 0))),
                      "phases_s": {k: round(v, 4) for k, v in prob.last_timing.items()},
                      "adjoint_residual": float(prob.last_status["adjoint"][0]),
                      "adjoint_iterations": int(prob.last_status["adjoint"][1])}
