@@ -156,9 +156,12 @@ __device__ __forceinline__ void pair_adj(const GeomView &g, const SrcInfo &s, V3
 constexpr int ADJ_T = 128;
 
 // Thread per source j; observers [k0, k1) of chunk blockIdx.y staged in shared
-// memory.  part[chunk][j][9] = (aM, ac, ad).
+// memory.  part[chunk][j][9] = (aM, ac, ad).  The kernel waits on FP64
+// latency, so the M-gradient variant is held to 168 registers (3 blocks, 12
+// warps per SM, a few dozen bytes of spill) instead of 182 (8 warps); the
+// variant without it fits 4 blocks at 127.
 template <bool WANT_M, bool RECT_ONLY>
-__global__ void __launch_bounds__(ADJ_T) adj_src_kernel(GeomView g, const int *__restrict__ elem_src,
+__global__ void __launch_bounds__(ADJ_T, WANT_M ? 3 : 4) adj_src_kernel(GeomView g, const int *__restrict__ elem_src,
                                                         const double *__restrict__ m, int n, const double *__restrict__ X,
                                                         const double *__restrict__ U, int nobs, int per_chunk, int what,
                                                         double *__restrict__ part)
