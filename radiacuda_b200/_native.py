@@ -71,6 +71,14 @@ def kernel_launches() -> int:
     return int(lib().radb200_kernel_launches())
 
 
+def release_cached_memory() -> None:
+    """Return the device blocks kept for reuse (256 MB and more, released
+    interactions and factors) to the driver.  Nothing is cached before the
+    library is loaded, so this does not load it."""
+    if _lib is not None:
+        check(_lib.radb200_release_cached_memory(), "radb200_release_cached_memory")
+
+
 def field(geom: Dict[str, np.ndarray], pts: np.ndarray, what: int, precision: int = 0) -> np.ndarray:
     g = GeomHolder(geom)
     P = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)

@@ -807,10 +807,13 @@ def UtiDel(h: int) -> int:
 
 
 def UtiDelAll() -> int:
+    """Deletes every object; the device memory that freed interactions left
+    for reuse goes back to the driver."""
     for h in list(_objs):
         UtiDel(h)
     _next[0] = 1
     model.clear_source_cache()
+    _native.release_cached_memory()
     return 0
 
 
