@@ -341,8 +341,9 @@ def relax_matvec_timing():
     anisotropic MatLin, 3x3x3 subdivision, so 10,800 cuboids, N3 = 32,400 and
     an FP32 matrix of 4.2 GB, far larger than L2.  Every iteration reads N
     once, 4 N3^2 algorithmic bytes.  The marginal time per iteration between
-    runs of 20 and 60 iterations removes the fixed cost of the call; the host
-    round trip of the misfit and the Anderson vector work stay in it."""
+    runs of 20 and 60 iterations (the fastest of three each) removes the fixed
+    cost of the call; the host round trip of the misfit and the Anderson
+    vector work stay in it."""
     from radiacuda_b200 import _native, rad
     import models as MD
 
@@ -354,13 +355,18 @@ def relax_matvec_timing():
     L.radb200_device_sync()
     t, its = {}, {}
     for k in (20, 60):
-        t0 = time.perf_counter()
-        st = rad.RlxAuto(im, 1e-30, k, 4, "ZeroM->False")
-        L.radb200_device_sync()
-        t[k], its[k] = time.perf_counter() - t0, int(st[3])
+        best = float("inf")
+        for _ in range(3):  # the fastest of three: host stalls on a shared machine only add time
+            t0 = time.perf_counter()
+            st = rad.RlxAuto(im, 1e-30, k, 4, "ZeroM->False")
+            L.radb200_device_sync()
+            best = min(best, time.perf_counter() - t0)
+        t[k], its[k] = best, int(st[3])
     rad.UtiDel(im)
     per_iter = 4.0 * n3 * n3
     marginal = (t[60] - t[20]) / max(its[60] - its[20], 1)
+    if marginal <= 0.0:
+        marginal = t[60] / max(its[60], 1)
     hbm = float(_peaks().get("hbm_gbs", 6650.0))
     gbs = per_iter / marginal / 1e9
     return {"model": "magnet array 20x20 blocks, 3x3x3 subdivision (10,800 cuboids)", "n3": n3,
