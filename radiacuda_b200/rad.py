@@ -26,7 +26,7 @@ from .model import (ArcCur, Bckg, Container, InteractionPack, Material, Obj, Pol
                     trf_plane_sym, trf_rotation, trf_translation)
 
 __all__ = [
-    "ObjRecMag", "ObjRecCur", "ObjPolyhdr", "ObjThckPgn", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
+    "ObjRecMag", "ObjRecCur", "ObjPolyhdr", "ObjThckPgn", "ObjMltExtPgn", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
     "ObjCnt", "ObjAddToCnt", "ObjCntStuf", "ObjCntSize", "ObjDivMag", "ObjM", "ObjSetM",
     "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
     "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
@@ -175,6 +175,131 @@ def ObjThckPgn(x, lx, pts, a="x", M=(0.0, 0.0, 0.0)) -> int:
     o = Polyhedron(np.asarray(V), F, (t.Minv @ M) / t.s)
     o.add_transform(1, t)
     return _add(o)
+
+
+def _ccw(p: np.ndarray) -> np.ndarray:
+    """The polygon counter-clockwise (signed area >= 0)."""
+    x, y = p[:, 0], p[:, 1]
+    area2 = float(np.dot(x, np.roll(y, -1)) - np.dot(np.roll(x, -1), y))
+    return p if area2 >= 0.0 else p[::-1].copy()
+
+
+def _is_convex(p: np.ndarray, tol: float) -> bool:
+    """Every turn of the counter-clockwise polygon is a left turn or straight
+    (radTPolygon::CheckIfConvex, called from its constructors, radplnr1.cpp:136)."""
+    q = _ccw(p)
+    d = np.roll(q, -1, axis=0) - q
+    cr = d[:, 0] * np.roll(d, -1, axis=0)[:, 1] - d[:, 1] * np.roll(d, -1, axis=0)[:, 0]
+    return bool(np.all(cr >= -tol * tol))
+
+
+def _strictly_convex_crease(A: np.ndarray, B: np.ndarray, C: np.ndarray, za: float, zb: float, zc: float,
+                            tol: float) -> bool:
+    """Whether the two slabs A-B and B-C meet at every edge of B with a
+    strictly convex crease.  The section at zb of the hull of A and C is the
+    Minkowski combination t A + (1 - t) C; the crease at an edge of B is
+    convex when that section lies inside the edge's line by more than tol.
+    A flat crease counts as not convex, as in the reference's test
+    (SetUpOnePolyhedronSegment, radapl4.cpp:716-752)."""
+    t = (zc - zb) / (zc - za)
+    q = _ccw(B)
+    d = np.roll(q, -1, axis=0) - q
+    for k in range(q.shape[0]):
+        L = math.hypot(d[k, 0], d[k, 1])
+        if L <= tol:
+            continue
+        n = np.array([d[k, 1], -d[k, 0]]) / L        # outward normal of a CCW edge
+        hA, hC = float(np.max(A @ n)), float(np.max(C @ n))
+        if t * hA + (1.0 - t) * hC >= float(q[k] @ n) - tol:
+            return False
+    return True
+
+
+def _hull_faces(P: np.ndarray, tol: float) -> List[List[int]]:
+    """Faces of the convex hull of the points P: hull triangles of one plane
+    merged, each face's vertices ordered around it."""
+    from scipy.spatial import ConvexHull
+
+    try:
+        hull = ConvexHull(P)
+    except Exception as e:  # flat or degenerate set of points
+        raise RadiaError(f"Radia::Error063: the slices do not enclose a volume ({e.__class__.__name__})")
+    planes: List[List[Any]] = []
+    for s, eq in zip(hull.simplices, hull.equations):
+        for g in planes:
+            if float(np.dot(g[0], eq[:3])) > 1.0 - 1e-12 and abs(g[1] - eq[3]) <= tol:
+                g[2].update(int(i) for i in s)
+                break
+        else:
+            planes.append([eq[:3].copy(), float(eq[3]), {int(i) for i in s}])
+    faces = []
+    for n, _, idx in planes:
+        idx = sorted(idx)
+        c = P[idx].mean(axis=0)
+        u = P[idx[0]] - c
+        u /= np.linalg.norm(u)
+        w = np.cross(n, u)
+        ang = [math.atan2(float((P[i] - c) @ w), float((P[i] - c) @ u)) for i in idx]
+        faces.append([idx[k] for k in np.argsort(ang)])
+    return faces
+
+
+def ObjMltExtPgn(slices, M=(0.0, 0.0, 0.0)) -> int:
+    """Convex polyhedra from polygon slices (radpy ObjMltExtPgn,
+    radpy.cpp:358-410; radTApplication::SetMultGenExtrPolygon, radapl1.cpp:859;
+    SetUpPolyhedronsFromLayerPolygons / SetUpOnePolyhedronSegment,
+    radapl4.cpp:435-...; CheckLayerPolygonStructures, radapl4.cpp:1036).
+
+    slices = [[[[x, y], ...], z], ...] with z strictly increasing or strictly
+    decreasing; a slice of 3 points or more is a convex polygon, fewer points
+    are allowed (a pole, an edge).  Consecutive slabs stay in one polyhedron
+    while they meet with a strictly convex crease at every edge of the slice
+    between them; a flat or reflex crease, a slice of fewer than 3 points
+    between them, or a single-point slice above ends the polyhedron there.
+    Each polyhedron is built as the convex hull of its slices, so the solid
+    (and the field of a uniform M) is the reference's.  One polyhedron is
+    returned as itself, several in a container (CheckIfGroupIsNeeded,
+    radapl4.cpp:1069).  Lengths compare with 10 max(1e-9, relative
+    randomization) times the z extent, the reference's RelAbsTol."""
+    M = _v3(M)
+    try:
+        layers = [(np.asarray(s[0], dtype=np.float64).reshape(-1, 2), float(s[1])) for s in slices]
+    except Exception:
+        raise RadiaError("Radia::Error000: ObjMltExtPgn, incorrect slices / layers definition")
+    ns = len(layers)
+    if ns < 2:
+        raise RadiaError("Radia::Error063: ObjMltExtPgn, number of slices / layers should be >= 2")
+    z = np.array([zz for _, zz in layers])
+    dz = np.diff(z)
+    if not (np.all(dz > 0.0) or np.all(dz < 0.0)):
+        raise RadiaError("Radia::Error063: the slice attitudes must strictly increase or strictly decrease")
+    npt = [p.shape[0] for p, _ in layers]
+    if min(npt) < 1 or max(npt) < 2:
+        raise RadiaError("Radia::Error063: incorrect slices / layers definition")
+    tol = 10.0 * max(1e-9, _rand[1]) * abs(z[-1] - z[0])
+    for p, _ in layers:
+        if p.shape[0] >= 3 and not _is_convex(p, tol):
+            raise RadiaError("Radia::Error111: the slice polygons must be convex")
+    for i in range(1, ns):
+        if npt[i - 1] < 3 and npt[i] < 3 and not (npt[i - 1] == 2 and npt[i] == 2):
+            raise RadiaError("Radia::Error063: two neighbouring slices of fewer than 3 points must both be segments")
+    pieces, s = [], 0
+    for i in range(1, ns):
+        b = i - 1
+        if b > s:   # slice b lies between two slabs of the current piece
+            if npt[b] < 3 or not _strictly_convex_crease(layers[b - 1][0], layers[b][0], layers[i][0],
+                                                         z[b - 1], z[b], z[i], tol):
+                pieces.append((s, b))
+                s = b
+        if npt[i] == 1 or i == ns - 1:
+            pieces.append((s, i))
+            s = i
+    hs = []
+    for a, b in pieces:
+        P = np.concatenate([np.column_stack([layers[k][0], np.full(npt[k], z[k])]) for k in range(a, b + 1)])
+        faces = _hull_faces(P, tol)
+        hs.append(_add(Polyhedron(P, faces, M)))
+    return hs[0] if len(hs) == 1 else ObjCnt(hs)
 
 
 def _axis_trf(P, orient: str) -> Optional[Trf]:
