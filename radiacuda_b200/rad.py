@@ -224,16 +224,28 @@ def _hull_faces(P: np.ndarray, tol: float) -> List[List[int]]:
         hull = ConvexHull(P)
     except Exception as e:  # flat or degenerate set of points
         raise RadiaError(f"Radia::Error063: the slices do not enclose a volume ({e.__class__.__name__})")
-    planes: List[List[Any]] = []
-    for s, eq in zip(hull.simplices, hull.equations):
-        for g in planes:
-            if float(np.dot(g[0], eq[:3])) > 1.0 - 1e-12 and abs(g[1] - eq[3]) <= tol:
-                g[2].update(int(i) for i in s)
-                break
-        else:
-            planes.append([eq[:3].copy(), float(eq[3]), {int(i) for i in s}])
+    # neighbouring triangles of one plane belong to one face (union-find over
+    # the hull's triangle adjacency: linear in the number of triangles)
+    eqs = hull.equations
+    root = list(range(len(eqs)))
+
+    def find(i):
+        while root[i] != i:
+            root[i] = root[root[i]]
+            i = root[i]
+        return i
+
+    for i, nb in enumerate(hull.neighbors):
+        for j in nb:
+            j = int(j)
+            if j > i and float(np.dot(eqs[i, :3], eqs[j, :3])) > 1.0 - 1e-12 and abs(eqs[i, 3] - eqs[j, 3]) <= tol:
+                root[find(j)] = find(i)
+    planes: Dict[int, List[Any]] = {}
+    for i, s in enumerate(hull.simplices):
+        g = planes.setdefault(find(i), [eqs[i, :3].copy(), set()])
+        g[1].update(int(k) for k in s)
     faces = []
-    for n, _, idx in planes:
+    for n, idx in planes.values():
         idx = sorted(idx)
         c = P[idx].mean(axis=0)
         u = P[idx[0]] - c
