@@ -26,7 +26,7 @@ from .model import (ArcCur, Bckg, Container, InteractionPack, Material, Obj, Pol
                     trf_plane_sym, trf_rotation, trf_translation)
 
 __all__ = [
-    "ObjRecMag", "ObjRecCur", "ObjPolyhdr", "ObjThckPgn", "ObjMltExtPgn", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
+    "ObjRecMag", "ObjRecCur", "ObjPolyhdr", "ObjThckPgn", "ObjMltExtPgn", "ObjMltExtRtg", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
     "ObjCnt", "ObjAddToCnt", "ObjCntStuf", "ObjCntSize", "ObjDivMag", "ObjM", "ObjSetM",
     "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
     "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
@@ -312,6 +312,31 @@ def ObjMltExtPgn(slices, M=(0.0, 0.0, 0.0)) -> int:
         faces = _hull_faces(P, tol)
         hs.append(_add(Polyhedron(P, faces, M)))
     return hs[0] if len(hs) == 1 else ObjCnt(hs)
+
+
+def ObjMltExtRtg(layers, M=(0.0, 0.0, 0.0)) -> int:
+    """Convex polyhedra from rectangular slices (radpy ObjMltExtRtg,
+    radpy.cpp:428; radTApplication::SetMultGenExtrRectangle, radapl1.cpp:885;
+    SetUpPolyhedronsFromLayerRectangles, radapl4.cpp:1088;
+    CheckLayerRectangleStructures, radapl4.cpp:1161).
+
+    layers = [[[x, y, z], [wx, wy]], ...]: each rectangle becomes the slice
+    (x -/+ wx/2, y -/+ wy/2) at z, listed counter-clockwise from its
+    (xmin, ymin) corner, and the slices are built as by ObjMltExtPgn."""
+    try:
+        rects = [(np.asarray(l[0], dtype=np.float64).reshape(3), np.asarray(l[1], dtype=np.float64).reshape(2))
+                 for l in layers]
+    except Exception:
+        raise RadiaError("Radia::Error000: ObjMltExtRtg, incorrect rectangle definition")
+    if len(rects) < 2:
+        raise RadiaError("Radia::Error063: ObjMltExtRtg, number of slices / layers should be >= 2")
+    slices = []
+    for c, w in rects:
+        if w[0] <= 0.0 and w[1] <= 0.0:
+            raise RadiaError("Radia::Error064: Incorrect input: Rectangle dimensions should be positive.")
+        x0, x1, y0, y1 = c[0] - 0.5 * w[0], c[0] + 0.5 * w[0], c[1] - 0.5 * w[1], c[1] + 0.5 * w[1]
+        slices.append([[[x0, y0], [x1, y0], [x1, y1], [x0, y1]], float(c[2])])
+    return ObjMltExtPgn(slices, M)
 
 
 def _axis_trf(P, orient: str) -> Optional[Trf]:

@@ -1,4 +1,4 @@
-"""Golden vectors for ObjMltExtPgn from the compiled reference module.
+"""Golden vectors for ObjMltExtPgn and ObjMltExtRtg from the compiled reference module.
 
     make -f oracle/Makefile.ref REF=/root/reference -j8     # builds oracle/_ref
     python tests/golden/make_mltextpgn_golden.py            # writes tests/golden/mltextpgn.json
@@ -53,6 +53,16 @@ def cases():
     }
 
 
+def rectangle_cases():
+    """ObjMltExtRtg layers [[x, y, z], [wx, wy]]: a three-layer frustum and a waist."""
+    return {
+        "rtg_frustum": ([[[0.1, 0.2, 0.0], [4.0, 3.0]], [[0.3, 0.1, 2.0], [2.0, 1.5]], [[0.2, 0.3, 3.5], [0.6, 0.4]]],
+                        [0.2, 0.4, 1.0]),
+        "rtg_waist": ([[[0.0, 0.0, 0.0], [4.0, 4.0]], [[0.2, 0.0, 1.2], [1.0, 1.2]], [[0.0, 0.1, 2.5], [4.4, 3.9]]],
+                      [1.0, 0.0, 0.3]),
+    }
+
+
 def main():
     import radia as R
 
@@ -66,6 +76,14 @@ def main():
         P = np.vstack([P, [[0.001, 0.0007, 0.0013], [0.0123, 0.0211, 2.0137]]])
         B = np.array(R.Fld(h, "b", P.tolist()))
         out[name] = {"slices": sl, "M": M, "pieces": int(R.ObjCntSize(h)), "points": P.tolist(), "b": B.tolist()}
+    rng = np.random.default_rng(8)
+    for name, (layers, M) in rectangle_cases().items():
+        R.UtiDelAll()
+        R.FldLenRndSw("off")
+        h = R.ObjMltExtRtg(layers, M)
+        P = rng.uniform(-3.0, 3.0, size=(30, 3)) + np.array([0.0137, 0.0071, 1.5])
+        B = np.array(R.Fld(h, "b", P.tolist()))
+        out[name] = {"layers": layers, "M": M, "pieces": int(R.ObjCntSize(h)), "points": P.tolist(), "b": B.tolist()}
     with open(os.path.join(HERE, "mltextpgn.json"), "w") as f:
         json.dump(out, f)
 

@@ -1,4 +1,4 @@
-"""rad.ObjMltExtPgn against the reference's golden vectors
+"""rad.ObjMltExtPgn and rad.ObjMltExtRtg against the reference's golden vectors
 (tests/golden/make_mltextpgn_golden.py): the same pieces and the same field,
 through the CPU oracle on the packed geometry and through the device."""
 import json
@@ -17,6 +17,8 @@ GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "mltextp
 def _build(rad, case):
     rad.UtiDelAll()
     rad.FldLenRndSw("off")
+    if "layers" in case:
+        return rad.ObjMltExtRtg(case["layers"], case["M"])
     return rad.ObjMltExtPgn(case["slices"], case["M"])
 
 
@@ -65,6 +67,10 @@ def test_slice_order_does_not_change_the_solid(rad, name):
 
 
 def test_argument_errors(rad):
+    with pytest.raises(RuntimeError, match="Error064"):
+        rad.ObjMltExtRtg([[[0, 0, 0], [1, 1]], [[0, 0, 1], [0, 0]]])
+    with pytest.raises(RuntimeError, match="Error063"):
+        rad.ObjMltExtRtg([[[0, 0, 0], [1, 1]]])
     sq = [[-1, -1], [1, -1], [1, 1], [-1, 1]]
     with pytest.raises(RuntimeError, match="Error063"):
         rad.ObjMltExtPgn([[sq, 0.0]])
