@@ -26,7 +26,8 @@ from .model import (ArcCur, Bckg, Container, InteractionPack, Material, Obj, Pol
                     trf_plane_sym, trf_rotation, trf_translation)
 
 __all__ = [
-    "ObjRecMag", "ObjRecCur", "ObjPolyhdr", "ObjThckPgn", "ObjMltExtPgn", "ObjMltExtRtg", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
+    "ObjRecMag", "ObjRecCur", "ObjPolyhdr", "ObjThckPgn", "ObjMltExtPgn", "ObjMltExtRtg", "ObjFullMag",
+    "ObjDrwAtr", "ObjDegFre", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
     "ObjCnt", "ObjAddToCnt", "ObjCntStuf", "ObjCntSize", "ObjDivMag", "ObjM", "ObjSetM",
     "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
     "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
@@ -312,6 +313,49 @@ def ObjMltExtPgn(slices, M=(0.0, 0.0, 0.0)) -> int:
         faces = _hull_faces(P, tol)
         hs.append(_add(Polyhedron(P, faces, M)))
     return hs[0] if len(hs) == 1 else ObjCnt(hs)
+
+
+def ObjDrwAtr(obj: int, rgb=None, thcn: float = 0.001) -> int:
+    """Drawing attributes (radpy ObjDrwAtr, radpy.cpp:1422).  Nothing is
+    drawn here; the colour and line thickness are kept on the object so that
+    scripts which set them run unchanged."""
+    o = _get(obj)
+    if rgb is not None:
+        o.drw_rgb = [float(c) for c in np.asarray(rgb, dtype=np.float64).reshape(-1)]
+    o.drw_thcn = float(thcn)
+    return int(obj)
+
+
+def ObjFullMag(P, L, M, K, cnt: int, mat: int, rgb=None) -> int:
+    """Block, colour, material, subdivision and container in one call, in the
+    reference's order (RadObjFullMag, cpp/src/lib/radentry.cpp:1858-1885):
+    ObjRecMag, ObjDrwAtr, MatApl when mat > 0, ObjDivMag by K, ObjAddToCnt
+    when cnt > 0."""
+    h = ObjRecMag(P, L, M)
+    ObjDrwAtr(h, rgb, 0.001)
+    if int(mat) > 0:
+        h = MatApl(h, int(mat))
+    h = ObjDivMag(h, K)
+    if int(cnt) > 0:
+        ObjAddToCnt(int(cnt), [h])
+    return h
+
+
+def ObjDegFre(obj: int) -> int:
+    """Degrees of freedom of the relaxation (radpy ObjDegFre;
+    radTApplication::ComputeNumberOfDegOfFreedom, radapl1.cpp:2017): 3 for a
+    block with a material (radrec.h:206), 3 for every polyhedron whether or
+    not it has one (radvlpgn.h:229), the sum over the members of a container
+    or a subdivided block (radgroup.h:149-156), 0 for currents and
+    backgrounds.  Symmetry images add nothing."""
+    o = _get(obj)
+    if isinstance(o, Container):
+        return int(sum(ObjDegFre(m) for m in o.members))
+    if isinstance(o, Polyhedron):
+        return 3
+    if isinstance(o, RecMag):
+        return 3 if getattr(o, "mat", None) is not None else 0
+    return 0
 
 
 def ObjMltExtRtg(layers, M=(0.0, 0.0, 0.0)) -> int:
