@@ -27,7 +27,7 @@ from .model import (ArcCur, Bckg, Container, InteractionPack, Material, Obj, Pol
 
 __all__ = [
     "ObjRecMag", "ObjRecCur", "ObjPolyhdr", "ObjThckPgn", "ObjMltExtPgn", "ObjMltExtRtg", "ObjFullMag",
-    "ObjDrwAtr", "ObjDegFre", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
+    "ObjCylMag", "ObjDrwAtr", "ObjDegFre", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
     "ObjCnt", "ObjAddToCnt", "ObjCntStuf", "ObjCntSize", "ObjDivMag", "ObjM", "ObjSetM",
     "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
     "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
@@ -313,6 +313,29 @@ def ObjMltExtPgn(slices, M=(0.0, 0.0, 0.0)) -> int:
         faces = _hull_faces(P, tol)
         hs.append(_add(Polyhedron(P, faces, M)))
     return hs[0] if len(hs) == 1 else ObjCnt(hs)
+
+
+def ObjCylMag(P, r: float, h: float, nseg: int, a: str = "z", M=(0.0, 0.0, 0.0)) -> int:
+    """Cylinder as a prism on a regular nseg-gon (radpy ObjCylMag;
+    radTApplication::SetCylMag, radapl1.cpp:1425-1482): vertices at angles
+    2 pi k / nseg from the first one, at radius r about the axis through P
+    along a, extruded over h about P; built as ObjThckPgn builds it, with the
+    polygon's (u, v) in the plane (y, z), (z, x) or (x, y) for a = x, y, z."""
+    P = _v3(P, "centre")
+    r, h, nseg = float(r), float(h), int(nseg)
+    if r <= 0.0:
+        raise RadiaError("Radia::Error089: the radius must be positive")
+    if h <= 0.0:
+        raise RadiaError("Radia::Error012: the height must be positive")
+    if nseg <= 0:
+        raise RadiaError("Radia::Error090: the number of segments must be positive")
+    ax = str(a)[:1].lower()
+    if ax not in ("x", "y", "z"):
+        raise RadiaError("Radia::Error000: ObjCylMag: orientation definition should be 'x', 'y' or 'z'")
+    iu, iv, ia = {"x": (1, 2, 0), "y": (2, 0, 1), "z": (0, 1, 2)}[ax]
+    ang = 2.0 * math.pi / nseg * np.arange(nseg)
+    pts = np.column_stack([P[iu] + r * np.cos(ang), P[iv] + r * np.sin(ang)])
+    return ObjThckPgn(P[ia], h, pts, ax, M)
 
 
 def ObjDrwAtr(obj: int, rgb=None, thcn: float = 0.001) -> int:

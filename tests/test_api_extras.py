@@ -1,7 +1,8 @@
-"""rad.ObjFullMag, rad.ObjDegFre and rad.ObjDrwAtr: the reference's counts
+"""rad.ObjFullMag, rad.ObjDegFre, rad.ObjDrwAtr and rad.ObjCylMag: the reference's counts
 and return values, and the same model as the reference builds (its field
 through the oracle against the compiled reference module, when present)."""
 import numpy as np
+import pytest
 
 from radiacuda_b200 import model
 
@@ -40,3 +41,34 @@ def test_full_magnet_model_matches_reference(rad, ref):
     Br = np.array(ref.Fld(hr[0], "b", P.tolist()))
     Bo = O.field(model.pack_sources(rad._objs, ho[0], tuple(rad._rand)), P, 0)
     assert np.abs(Br - Bo).max() / np.abs(Br).max() < 1e-10
+
+
+CYLINDERS = [([1.1, -0.3, 2.2], 3.0, 5.0, 12, "z", [0.1, 0.2, 1.0]), ([0.2, 0.4, -1.0], 2.0, 4.0, 7, "x", [1.0, 0.3, 0.0]),
+             ([-1.0, 2.0, 0.5], 2.5, 3.0, 9, "y", [0.2, 1.0, 0.4])]
+
+
+def test_cylinder_errors_and_axial_field(rad):
+    for bad, code in (((0, 0, 0), 0.0, 1.0, 8), "Error089"), (((0, 0, 0), 1.0, 0.0, 8), "Error012"), \
+            (((0, 0, 0), 1.0, 1.0, 0), "Error090"):
+        with pytest.raises(RuntimeError, match=code):
+            rad.ObjCylMag(*bad)
+    # a long 64-gon prism magnetized along its axis: B at the centre is close
+    # to M (1 - cos of the half-angle seen from the centre)
+    rad.UtiDelAll()
+    rad.FldLenRndSw("off")
+    h = rad.ObjCylMag([0, 0, 0], 1.0, 200.0, 64, "z", [0, 0, 1.0])
+    b = O.field(model.pack_sources(rad._objs, h, tuple(rad._rand)), np.array([[0.01, 0.007, 0.013]]), 0)[0]
+    assert abs(b[2] - 100.0 / np.hypot(100.0, 1.0)) < 2e-3
+
+
+def test_cylinders_match_reference(rad, ref):
+    rng = np.random.default_rng(5)
+    for args in CYLINDERS:
+        for X in (ref, rad):
+            X.UtiDelAll()
+            X.FldLenRndSw("off")
+        hr, ho = ref.ObjCylMag(*args), rad.ObjCylMag(*args)
+        P = rng.uniform(-6, 6, size=(30, 3)) + np.array([0.0137, 0.0071, 0.0113])
+        Br = np.array(ref.Fld(hr, "b", P.tolist()))
+        Bo = O.field(model.pack_sources(rad._objs, ho, tuple(rad._rand)), P, 0)
+        assert np.abs(Br - Bo).max() / np.abs(Br).max() < 1e-10
