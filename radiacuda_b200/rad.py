@@ -32,7 +32,8 @@ __all__ = [
     "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
     "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
     "RlxPre", "RlxAuto", "Solve", "Fld", "FldLst", "FldInt", "FldPtcTrj", "FldCmpCrt", "FldCmpPrc", "FldLenRndSw", "FldLenTol",
-    "UtiDel", "UtiDelAll", "UtiDmp", "UtiDmpPrs", "UtiVer", "UtiFldLastBackend", "UtiAsmLastBackend", "UtiGpuFallback",
+    "UtiDel", "UtiDelAll", "UtiDmp", "UtiDmpPrs", "UtiMPI", "UtiVer", "UtiFldLastBackend", "UtiAsmLastBackend",
+    "UtiGpuFallback",
 ]
 
 # --------------------------------------------------------------------------
@@ -1161,6 +1162,53 @@ def UtiDmpPrs(bstr: bytes):
         remap[int(old)] = _add(it)
     out = [remap[int(h)] for h in payload["roots"]]
     return out[0] if payload["single"] else out
+
+
+def _flat_floats(data) -> List[float]:
+    """Nested lists / arrays flattened to floats, as the reference copies them
+    into its share buffer (CopyPyNestedListElemsToNumAr)."""
+    if isinstance(data, (list, tuple)):
+        out: List[float] = []
+        for d in data:
+            out.extend(_flat_floats(d))
+        return out
+    return [float(v) for v in np.asarray(data, dtype=np.float64).reshape(-1)]
+
+
+def UtiMPI(mode: str, data=None, rankFrom: int = 0, rankTo: int = -1):
+    """Parallel-process control (radpy UtiMPI, radpy.cpp:3280-3335), on the
+    torch.distributed default process group in place of MPI (one process
+    per GPU).  'on' and 'in' return this process's rank (0 when no group is
+    initialized: this library does not start one), 'off' returns it and
+    leaves the group to its owner, 'barrier' waits for every rank.  'share'
+    sends data, flattened to floats as the reference does, from rankFrom to
+    every rank (rankTo = -1) or to rankTo, and returns the flat list; a rank
+    that receives nothing gets its own data back.  Without data the rank is
+    returned, as in the reference."""
+    m = str(mode).strip().lower()
+    if m not in ("on", "in", "off", "share", "barrier"):
+        raise RadiaError("Radia::Error000: UtiMPI: the first argument should be 'on', 'in', 'off', 'share' or "
+                         "'barrier'")
+    dist = None
+    try:
+        import torch.distributed as _dist
+        if _dist.is_available() and _dist.is_initialized():
+            dist = _dist
+    except ImportError:
+        pass
+    rank = dist.get_rank() if dist is not None else 0
+    if m == "barrier" and dist is not None:
+        dist.barrier()
+    if m != "share" or data is None:
+        return rank
+    flat = _flat_floats(data)
+    if dist is None:
+        return flat
+    box = [flat if rank == int(rankFrom) else None]
+    dist.broadcast_object_list(box, src=int(rankFrom))
+    if int(rankTo) < 0 or rank == int(rankTo):
+        return [float(v) for v in box[0]]
+    return flat
 
 
 def UtiVer() -> float:

@@ -139,3 +139,52 @@ def test_sharded_fld_over_nccl_equals_fld(cuda):
         p.join(timeout=300)
         assert p.exitcode == 0
         assert out[0]
+
+
+def _utimpi_main(rank, world, port, out):
+    import sys
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from radiacuda_b200 import rad
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        res = {"on": rad.UtiMPI("on"), "barrier": rad.UtiMPI("barrier")}
+        mine = [[10.0 * rank, 1.0], [2.0]]
+        res["all"] = rad.UtiMPI("share", mine, 1)
+        res["to0"] = rad.UtiMPI("share", mine, 1, 0)
+        res["off"] = rad.UtiMPI("off")
+        out[rank] = res
+    finally:
+        dist.destroy_process_group()
+
+
+def test_utimpi_over_two_gloo_ranks():
+    """rad.UtiMPI on the default group: the rank, a barrier, and 'share' from
+    rank 1 to every rank and to rank 0 only (data flattened to floats)."""
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    with ctx.Manager() as m:
+        out = m.dict()
+        procs = [ctx.Process(target=_utimpi_main, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=120)
+            assert p.exitcode == 0
+        res = dict(out)
+    for r in (0, 1):
+        assert res[r]["on"] == r and res[r]["barrier"] == r and res[r]["off"] == r
+        assert res[r]["all"] == [10.0, 1.0, 2.0]
+    assert res[0]["to0"] == [10.0, 1.0, 2.0]
+    assert res[1]["to0"] == [10.0, 1.0, 2.0]
+
+
+def test_utimpi_without_a_process_group(rad):
+    assert rad.UtiMPI("on") == 0 and rad.UtiMPI("barrier") == 0 and rad.UtiMPI("off") == 0
+    assert rad.UtiMPI("share", [[1, 2], [3]]) == [1.0, 2.0, 3.0]
+    with pytest.raises(RuntimeError, match="Error000"):
+        rad.UtiMPI("start")
