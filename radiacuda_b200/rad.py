@@ -27,7 +27,7 @@ from .model import (ArcCur, Bckg, Container, InteractionPack, Material, Obj, Pol
 
 __all__ = [
     "ObjRecMag", "ObjRecCur", "ObjPolyhdr", "ObjThckPgn", "ObjMltExtPgn", "ObjMltExtRtg", "ObjFullMag",
-    "ObjCylMag", "ObjDrwAtr", "ObjDegFre", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
+    "ObjCylMag", "ObjArcPgnMag", "ObjDrwAtr", "ObjDegFre", "ObjArcCur", "ObjRaceTrk", "ObjBckg",
     "ObjCnt", "ObjAddToCnt", "ObjCntStuf", "ObjCntSize", "ObjDivMag", "ObjM", "ObjSetM",
     "TrfTrsl", "TrfRot", "TrfPlSym", "TrfInv", "TrfCmbL", "TrfCmbR", "TrfMlt", "TrfOrnt",
     "TrfZerPara", "TrfZerPerp", "MatLin", "MatSatIsoFrm", "MatApl",
@@ -339,6 +339,87 @@ def ObjCylMag(P, r: float, h: float, nseg: int, a: str = "z", M=(0.0, 0.0, 0.0))
     return ObjThckPgn(P[ia], h, pts, ax, M)
 
 
+def ObjArcPgnMag(P, a, pgn, phi, nseg: int, sym: str = "nosym", M=(0.0, 0.0, 0.0)) -> int:
+    """Arc of polygonal cross-section (radpy ObjArcPgnMag, radpy.cpp:314-345;
+    radTApplication::SetArcPolygon, radapl1.cpp:1027-1370).
+
+    The axis runs along a through the 2-D point P ((y, z), (z, x) or (x, y)
+    for a = x, y, z); the cross-section points [r, z] lie in the half-plane
+    of the radial direction y, z or x, rotated about the axis by phi[0].
+    The first sector is the polyhedron swept from phi[0] to
+    phi[0] + (phi[1] - phi[0]) / nseg: the cross-section at both ends and one
+    planar face per cross-section edge (a triangle where one end has r = 0,
+    none where both have).  With nseg > 1 the sector is repeated by the
+    rotation through the sector angle: 'sym' as nseg symmetry images of one
+    element (their magnetizations rotate with them), 'nosym' as a container
+    of nseg elements that each carry the rotation as their own transform and
+    have the lab-frame magnetization M."""
+    p2 = np.asarray(P, dtype=np.float64).reshape(-1)
+    if p2.size != 2:
+        raise RadiaError("Radia::Error000: ObjArcPgnMag, incorrect definition of initial center point")
+    ax = str(a)[:1].lower()
+    if ax not in ("x", "y", "z"):
+        raise RadiaError("Radia::Error092: the orientation should be 'x', 'y' or 'z'")
+    pts = np.asarray(pgn, dtype=np.float64).reshape(-1, 2)
+    ph = np.asarray(phi, dtype=np.float64).reshape(-1)
+    if pts.shape[0] < 3 or ph.size != 2:
+        raise RadiaError("Radia::Error000: ObjArcPgnMag, incorrect definition of cross-section polygon or angles")
+    if ph[1] <= ph[0] or ph[1] - ph[0] > 2.0 * math.pi:
+        raise RadiaError("Radia::Error011: incorrect angles")
+    nseg = int(nseg)
+    if nseg <= 0:
+        raise RadiaError("Radia::Error090: the number of segments must be positive")
+    dphi = (ph[1] - ph[0]) / nseg
+    if dphi <= 0.0 or dphi >= math.pi:
+        raise RadiaError("Radia::Error094: the segment angle must be below pi")
+    if str(sym) not in ("sym", "SYM", "nosym", "NOSYM"):
+        raise RadiaError("Radia::Error093: the symmetry switch should be 'sym' or 'nosym'")
+    M = _v3(M)
+    cen = {"x": [0.0, p2[0], p2[1]], "y": [p2[1], 0.0, p2[0]], "z": [p2[0], p2[1], 0.0]}[ax]
+    cen = np.array(cen)
+    axis = np.eye(3)[{"x": 0, "y": 1, "z": 2}[ax]]
+    rad0 = np.eye(3)[{"x": 1, "y": 2, "z": 0}[ax]]
+
+    def radial(ang):   # rad0 rotated about the axis by ang (right-handed)
+        return math.cos(ang) * rad0 + math.sin(ang) * np.cross(axis, rad0)
+
+    r1, r2 = radial(ph[0]), radial(ph[0] + dphi)
+    r = pts[:, 0]
+    if np.any(r < 0.0) or int(np.sum(r == 0.0)) > 2:
+        raise RadiaError("Radia::Error095: the cross-section must not cross the axis")
+    n = pts.shape[0]
+    V = [cen + pts[i, 0] * r1 + pts[i, 1] * axis for i in range(n)]
+    idx2 = []
+    for i in range(n):        # second base: points on the axis are shared
+        if r[i] == 0.0:
+            idx2.append(i)
+        else:
+            idx2.append(len(V))
+            V.append(cen + pts[i, 0] * r2 + pts[i, 1] * axis)
+    F = [list(range(n)), list(idx2)]
+    for j in range(n):
+        k = (j + 1) % n
+        if r[j] <= 0.0 and r[k] <= 0.0:
+            continue
+        f = [j, k, idx2[k], idx2[j]]
+        F.append([v for q, v in enumerate(f) if v not in f[:q]])
+    V = np.array(V)
+    if nseg == 1:
+        return _add(Polyhedron(V, F, M))
+    rot = trf_rotation(cen, axis, dphi)
+    if str(sym).lower() == "sym":
+        o = Polyhedron(V, F, M)
+        o.add_transform(nseg, rot)
+        return _add(o)
+    hs = [_add(Polyhedron(V, F, M))]
+    for k in range(1, nseg):
+        t = trf_rotation(cen, axis, k * dphi)
+        o = Polyhedron(V, F, (t.Minv @ M) / t.s)
+        o.add_transform(1, t)
+        hs.append(_add(o))
+    return ObjCnt(hs)
+
+
 def ObjDrwAtr(obj: int, rgb=None, thcn: float = 0.001) -> int:
     """Drawing attributes (radpy ObjDrwAtr, radpy.cpp:1422).  Nothing is
     drawn here; the colour and line thickness are kept on the object so that
@@ -498,7 +579,10 @@ def ObjCntStuf(obj: int) -> List[int]:
 
 
 def ObjCntSize(obj: int) -> int:
-    return len(collect_leaves(_objs, obj))
+    """Number of direct members of a container or a subdivided block, 0 for
+    any other object (radpy ObjCntSize: the size of the radTGroup)."""
+    o = _get(obj)
+    return len(o.members) if isinstance(o, Container) else 0
 
 
 def ObjDivMag(obj: int, k, *args, **kw) -> int:

@@ -31,6 +31,8 @@ def test_degrees_of_freedom_and_drawing_attributes(rad):
     assert [rad.ObjDegFre(h) for h in (top, cnt, b1, b2, tet)] == [21, 21, 18, 0, 3]
     assert rad.ObjDrwAtr(b1, [0, 0, 1], 0.002) == b1
     assert rad.ObjCntSize(b1) == 6
+    # the reference's sizes: direct members of a container, 0 for one element
+    assert rad.ObjCntSize(top) == 2 and rad.ObjCntSize(cnt) == 3 and rad.ObjCntSize(tet) == 0
 
 
 def test_full_magnet_model_matches_reference(rad, ref):
@@ -69,6 +71,41 @@ def test_cylinders_match_reference(rad, ref):
             X.FldLenRndSw("off")
         hr, ho = ref.ObjCylMag(*args), rad.ObjCylMag(*args)
         P = rng.uniform(-6, 6, size=(30, 3)) + np.array([0.0137, 0.0071, 0.0113])
+        Br = np.array(ref.Fld(hr, "b", P.tolist()))
+        Bo = O.field(model.pack_sources(rad._objs, ho, tuple(rad._rand)), P, 0)
+        assert np.abs(Br - Bo).max() / np.abs(Br).max() < 1e-10
+
+
+ARCS = [([1.0, 2.0], "z", [[3, -1], [5, -1.5], [6, 1], [3.5, 1.2]], [0.2, 2.4], 5, "nosym", [0.3, 1.0, 0.2]),
+        ([1.0, 2.0], "z", [[3, -1], [5, -1.5], [6, 1], [3.5, 1.2]], [0.2, 2.4], 5, "sym", [0.3, 1.0, 0.2]),
+        ([0.5, -0.3], "x", [[0, -1], [2, -1], [2, 1], [0, 1]], [0.0, 3.0], 4, "nosym", [0, 0.5, 1.0]),
+        ([0.5, -0.3], "y", [[0, -1], [2, 0], [0, 1]], [-1.0, 1.5], 3, "sym", [1.0, 0.2, 0.1])]
+
+
+def test_arc_structure_and_errors(rad):
+    rad.UtiDelAll()
+    sizes = [(rad.ObjCntSize(h), rad.ObjDegFre(h)) for h in (rad.ObjArcPgnMag(*c) for c in ARCS)]
+    # 'nosym' makes one element per sector, 'sym' one element with images
+    assert sizes == [(5, 15), (0, 3), (4, 12), (0, 3)]
+    sq = [[1, 0], [2, 0], [2, 1], [1, 1]]
+    for args, code in ((([0, 0], "w", sq, [0, 1], 2), "Error092"), (([0, 0], "z", sq, [1, 0], 2), "Error011"),
+                       (([0, 0], "z", sq, [0, 1], 0), "Error090"), (([0, 0], "z", sq, [0, 6.5], 2), "Error094"),
+                       (([0, 0], "z", [[-1, 0], [2, 0], [2, 1]], [0, 1], 2), "Error095")):
+        with pytest.raises(RuntimeError, match=code):
+            rad.ObjArcPgnMag(*args)
+    with pytest.raises(RuntimeError, match="Error093"):
+        rad.ObjArcPgnMag([0, 0], "z", sq, [0, 1], 2, "both")
+
+
+def test_arcs_match_reference(rad, ref):
+    rng = np.random.default_rng(9)
+    for args in ARCS:
+        for X in (ref, rad):
+            X.UtiDelAll()
+            X.FldLenRndSw("off")
+        hr, ho = ref.ObjArcPgnMag(*args), rad.ObjArcPgnMag(*args)
+        assert (ref.ObjCntSize(hr), ref.ObjDegFre(hr)) == (rad.ObjCntSize(ho), rad.ObjDegFre(ho))
+        P = rng.uniform(-7, 7, size=(40, 3)) + np.array([0.0137, 0.0071, 0.0113])
         Br = np.array(ref.Fld(hr, "b", P.tolist()))
         Bo = O.field(model.pack_sources(rad._objs, ho, tuple(rad._rand)), P, 0)
         assert np.abs(Br - Bo).max() / np.abs(Br).max() < 1e-10

@@ -23,8 +23,7 @@ def _build(rad, case):
 
 
 def _pieces(rad, h):
-    o = rad._objs[h]
-    return rad.ObjCntSize(h) if hasattr(o, "members") else 0
+    return rad.ObjCntSize(h)
 
 
 def _rel(a, b):
