@@ -89,7 +89,7 @@ def test_arc_structure_and_errors(rad):
     assert sizes == [(5, 15), (0, 3), (4, 12), (0, 3)]
     sq = [[1, 0], [2, 0], [2, 1], [1, 1]]
     for args, code in ((([0, 0], "w", sq, [0, 1], 2), "Error092"), (([0, 0], "z", sq, [1, 0], 2), "Error011"),
-                       (([0, 0], "z", sq, [0, 1], 0), "Error090"), (([0, 0], "z", sq, [0, 6.5], 2), "Error094"),
+                       (([0, 0], "z", sq, [0, 1], 0), "Error090"), (([0, 0], "z", sq, [0, 3.5], 1), "Error094"),
                        (([0, 0], "z", [[-1, 0], [2, 0], [2, 1]], [0, 1], 2), "Error095")):
         with pytest.raises(RuntimeError, match=code):
             rad.ObjArcPgnMag(*args)
