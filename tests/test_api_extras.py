@@ -1,6 +1,8 @@
-"""rad.ObjFullMag, rad.ObjDegFre, rad.ObjDrwAtr and rad.ObjCylMag: the reference's counts
-and return values, and the same model as the reference builds (its field
-through the oracle against the compiled reference module, when present)."""
+"""rad.ObjFullMag, rad.ObjDegFre, rad.ObjDrwAtr, rad.ObjCylMag,
+rad.ObjArcPgnMag and rad.ObjCntSize: the reference's counts, sizes, errors
+and return values, the same models as the reference builds (their field
+through the oracle against the compiled reference module, when present), and
+a relaxed model of these constructors against committed golden vectors."""
 import numpy as np
 import pytest
 
@@ -109,3 +111,24 @@ def test_arcs_match_reference(rad, ref):
         Br = np.array(ref.Fld(hr, "b", P.tolist()))
         Bo = O.field(model.pack_sources(rad._objs, ho, tuple(rad._rand)), P, 0)
         assert np.abs(Br - Bo).max() / np.abs(Br).max() < 1e-10
+
+
+def test_relaxed_constructor_model_matches_reference_golden(rad):
+    """Arcs ('nosym' elements carry their own rotation, 'sym' ones are
+    images), an x-axis cylinder and rectangle slices with anisotropic and
+    saturating materials, relaxed by the oracle's method 4 to 1e-8 like the
+    reference's Solve: B agrees to 1e-8 (tests/golden/make_constructors_golden.py)."""
+    import json
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_constructors_golden import build
+    from test_oracle_pin import oracle_solve
+
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "constructors.json")))
+    h = build(rad)
+    _, _, st = oracle_solve(rad, h, 1e-8, 5000)
+    assert int(st[3]) == int(gold["status"][3])
+    B = O.field(model.pack_sources(rad._objs, h, tuple(rad._rand)), np.array(gold["points"]), 0)
+    assert np.abs(B - np.array(gold["b"])).max() / np.abs(np.array(gold["b"])).max() < 1e-8
