@@ -91,3 +91,37 @@ def test_device_field_matches_reference(rad, cuda, name):
     c = GOLD[name]
     h = _build(rad, c)
     assert _rel(rad.Fld(h, "b", c["points"]), c["b"]) < 1e-9
+
+
+def test_crease_rule_on_convex_flat_and_reflex_slices(rad):
+    """The piece rule on its own: a section of the outer slices strictly
+    inside the middle one is a convex crease, equal to it is flat, and
+    outside it is reflex (the two latter end a piece)."""
+    from radiacuda_b200.rad import _strictly_convex_crease
+
+    sq = lambda a: np.array([[-a, -a], [a, -a], [a, a], [-a, a]], dtype=float)
+    tol = 1e-8
+    assert _strictly_convex_crease(sq(1.0), sq(2.0), sq(1.0), 0.0, 1.0, 2.0, tol)        # bulge
+    assert not _strictly_convex_crease(sq(1.0), sq(1.5), sq(2.0), 0.0, 1.0, 2.0, tol)    # straight taper
+    assert not _strictly_convex_crease(sq(2.0), sq(1.0), sq(2.0), 0.0, 1.0, 2.0, tol)    # waist
+    assert _strictly_convex_crease(sq(1.0), sq(1.6), sq(2.0), 0.0, 1.0, 2.0, tol)        # widening less fast
+    # the middle slice only partly outside the hull section: reflex at one edge
+    assert not _strictly_convex_crease(sq(1.0), sq(1.4) + [0.5, 0.0], sq(1.0), 0.0, 1.0, 2.0, tol)
+
+
+def test_finely_sliced_sphere_is_one_polyhedron(rad):
+    import math
+
+    rad.UtiDelAll()
+    rad.FldLenRndSw("off")
+    nz, nphi = 40, 24
+    sl = [[[[0.0, 0.0]], -1.0]]
+    for i in range(1, nz):
+        z = -1.0 + 2.0 * i / nz
+        ct = math.sqrt(1.0 - z * z)
+        sl.append([[[ct * math.cos(2 * math.pi * k / nphi), ct * math.sin(2 * math.pi * k / nphi)] for k in range(nphi)], z])
+    sl.append([[[0.0, 0.0]], 1.0])
+    h = rad.ObjMltExtPgn(sl, [0.0, 0.0, 1.0])
+    assert rad.ObjCntSize(h) == 0
+    b = O.field(model.pack_sources(rad._objs, h, tuple(rad._rand)), np.array([[0.01, 0.02, 0.03]]), 0)[0]
+    assert abs(b[2] - 2.0 / 3.0) < 5e-3
