@@ -245,8 +245,8 @@ def run_ours(args, rank, world):
                                 "fallback bf16 / 2"),
                 "hbm_achieved_gbs": round(upd_gbs, 1), "hbm_peak_gbs": hbm, "hbm_frac": round(upd_gbs / hbm, 4),
                 "traffic": round(TC_TRAFFIC_OVER_ALGORITHMIC * upd_bytes_per_launch),
-                "traffic_note": "ncu dram bytes / algorithmic bytes (0.92) of the same kernel on a 9,000^2 LU "
-                                "(profiles/tc_update_tma_kernel_lu9000.md), times the algorithmic bytes per launch",
+                "traffic_note": "ncu dram bytes / algorithmic bytes (0.92) of the same kernel on a 9,000^2 LU, "
+                                "times the algorithmic bytes per launch",
                 "launches_per_step": int(upd_n.value // max(args.steps, 1)),
                 "seconds_per_step": round(upd_s.value / max(args.steps, 1), 4),
                 "algorithmic": "2 m^2 K flops; 8 m^2 + 8 m K bytes per launch (FP32 C read + written, panels read once)"}
@@ -471,8 +471,7 @@ def trajectory_timing(reps=3):
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum over the algorithmic bytes of the
-# trailing-update kernel (561 MB / 611 MB), from the ncu capture summarised in
-# profiles/tc_update_tma_kernel_lu9000.md
+# trailing-update kernel (561 MB / 611 MB), from an ncu capture of a 9,000^2 LU
 TC_TRAFFIC_OVER_ALGORITHMIC = 0.92
 
 

@@ -161,11 +161,13 @@ RADB200_API int radb200_field(const RadB200Geom *g, const double *pts, int64_t n
  * memory: the pointer fields of *g, pts and out; the struct itself and its
  * counts are on the host.  FP64, face-by-face polyhedron form.  The call
  * allocates nothing: its only scratch is a static 3 MiB device array that
- * every GPU loading the library keeps until exit (its address is looked up
- * on the first call on each device; make that first call outside any stream
- * capture).  At most 16,384 points per call; larger counts are rejected with
- * RADB200_E_ARG.  Calls that overlap on the GPU share the scratch and race:
- * serialize them.  Synchronizes stream 0 before returning.                   */
+ * every GPU it runs on keeps until exit.  The driver maps that array when the
+ * first call on a device looks up its address (lazy module loading), so the
+ * first call can fail for lack of device memory: make it at set-up, outside
+ * any stream capture.  At most 16,384 points per call; larger counts are
+ * rejected with RADB200_E_ARG.  Calls that overlap on the GPU share the
+ * scratch and race: serialize them.  Runs on the calling thread's per-thread
+ * default stream (cudaStreamPerThread) and synchronizes it before returning. */
 RADB200_API int radb200_field_noalloc(const RadB200Geom *g, const double *d_pts, int64_t npts,
                                       int what, double *d_out);
 /* Same, with pts/out already in device memory (cudaStream 0 ordering).      */
@@ -269,6 +271,20 @@ RADB200_API int radb200_intrc_matrix(int64_t handle, int dtype, void *out);
 RADB200_API int radb200_intrc_extfield(int64_t handle, double *out);
 /* Replace the external field (e.g. after a source update, RlxUpdSrc).       */
 RADB200_API int radb200_intrc_set_extfield(int64_t handle, const double *h_ext);
+/* Create an interaction from a matrix assembled elsewhere: replaces the
+ * host flatten + upload of radGPU_PackInteractionData (radgpurlx.cpp:25-62,
+ * radgpurlx.h:90-96), used when Radia's CPU assembly built the matrix.
+ * N: host [3N x 3N] FP32 row major (radTInteraction::mAsmMatrix layout,
+ * radintrc.h:99-115); h_ext: host [3N] or NULL (zero).  The interaction has
+ * no element geometry: relaxation and direct solves work, the geometric
+ * adjoint terms (dL_dc, dL_dd, radb200_field_vjp) return
+ * RADB200_E_UNSUPPORTED.                                                     */
+RADB200_API int radb200_intrc_load(const RadB200Relax *r, const float *N, const double *h_ext, int64_t *handle);
+/* Replace the materials of an interaction (same elements); drops its LU
+ * factors.  The reference re-reads each element's material at every
+ * relaxation (radgpurlx.cpp:104-196), so a MatApl between RlxPre and RlxAuto
+ * takes effect; this is the device side of that.                            */
+RADB200_API int radb200_intrc_set_materials(int64_t handle, const RadB200Relax *r);
 
 /* ---- relaxation ------------------------------------------------------------
  * Replaces radGPU_AutoRelax (method 9) and radGPU_AutoRelaxNK (method 11),

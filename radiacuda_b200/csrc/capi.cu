@@ -7,6 +7,7 @@
 #include <cmath>
 #include <map>
 #include <memory>
+#include <mutex>
 
 #include "internal.cuh"
 
@@ -37,56 +38,84 @@ int check_launch(const char *what)
 // ---- reuse of large device blocks -----------------------------------------
 // Released blocks of BIG_BLOCK bytes and more wait here (after the device is
 // idle, so no kernel still uses them) until an allocation of at most 25% less
-// takes them, up to a cap of RADB200_BUFCACHE_GB (default: 40% of the device's
-// memory; 0 turns reuse off).  A failed cudaMalloc returns every cached block
-// to the driver and tries again; radb200_release_cached_memory does the same
-// on request.  The pool is never destroyed (blocks outlive static DBufs).
+// on the same device takes them, up to a cap of RADB200_BUFCACHE_GB (default:
+// 40% of the first device's memory; 0 turns reuse off).  A failed cudaMalloc
+// returns every cached block of that device to the driver and tries again;
+// radb200_release_cached_memory returns all of them.  Blocks are keyed by
+// device ordinal and the pool is guarded by a mutex, so host threads and
+// device switches do not mix blocks up.  The pool is never destroyed (blocks
+// outlive static DBufs).
 namespace {
 struct BigPool {
-  std::multimap<size_t, void *> blocks;
+  std::map<int, std::multimap<size_t, void *>> blocks;  // device -> size -> block
   size_t total = 0, cap = 0;
   bool init = false;
+  std::mutex mu;
 };
 BigPool &big_pool()
 {
   static BigPool *bp = new BigPool();
-  if (!bp->init) {
-    bp->init = true;
-    const char *e = getenv("RADB200_BUFCACHE_GB");
-    if (e) bp->cap = (size_t)(atof(e) * 1073741824.0);
-    else {
-      size_t fr = 0, tot = 0;
-      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) bp->cap = tot / 10 * 4;
-      else cudaGetLastError();
-    }
-  }
   return *bp;
 }
-void big_flush(BigPool &bp)
+void big_init(BigPool &bp)
 {
-  for (auto &kv : bp.blocks) cudaFree(kv.second);
-  bp.blocks.clear();
-  bp.total = 0;
+  if (bp.init) return;
+  bp.init = true;
+  const char *e = getenv("RADB200_BUFCACHE_GB");
+  if (e) bp.cap = (size_t)(atof(e) * 1073741824.0);
+  else {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) bp.cap = tot / 10 * 4;
+    else cudaGetLastError();
+  }
+}
+int current_device()
+{
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) { cudaGetLastError(); d = 0; }
+  return d;
+}
+// frees the cached blocks of device dev (all devices when dev < 0); caller holds mu
+void big_flush(BigPool &bp, int dev)
+{
+  int cur = current_device();
+  for (auto it = bp.blocks.begin(); it != bp.blocks.end();) {
+    if (dev >= 0 && it->first != dev) { ++it; continue; }
+    if (it->first != cur) cudaSetDevice(it->first);
+    for (auto &kv : it->second) { cudaFree(kv.second); bp.total -= kv.first; }
+    if (it->first != cur) cudaSetDevice(cur);
+    it = bp.blocks.erase(it);
+  }
+  cudaGetLastError();
 }
 }  // namespace
 
-void big_release_all() { big_flush(big_pool()); }
+void big_release_all()
+{
+  BigPool &bp = big_pool();
+  std::lock_guard<std::mutex> lk(bp.mu);
+  big_flush(bp, -1);
+}
 
 void *big_alloc(size_t b, size_t *got)
 {
   BigPool &bp = big_pool();
-  auto it = bp.blocks.lower_bound(b);
-  if (it != bp.blocks.end() && it->first <= b + b / 4) {
+  std::lock_guard<std::mutex> lk(bp.mu);
+  big_init(bp);
+  const int dev = current_device();
+  auto &mine = bp.blocks[dev];
+  auto it = mine.lower_bound(b);
+  if (it != mine.end() && it->first <= b + b / 4) {
     void *p = it->second;
     *got = it->first;
     bp.total -= it->first;
-    bp.blocks.erase(it);
+    mine.erase(it);
     return p;
   }
   void *p = nullptr;
   if (cudaMalloc(&p, b) != cudaSuccess) {
     cudaGetLastError();
-    big_flush(bp);
+    big_flush(bp, dev);
     if (cudaMalloc(&p, b) != cudaSuccess) {
       cudaGetLastError();
       set_error("device allocation of %zu bytes failed", b);
@@ -100,8 +129,10 @@ void *big_alloc(size_t b, size_t *got)
 void big_free(void *p, size_t b)
 {
   BigPool &bp = big_pool();
+  std::lock_guard<std::mutex> lk(bp.mu);
+  big_init(bp);
   if (bp.total + b <= bp.cap && cudaDeviceSynchronize() == cudaSuccess) {
-    bp.blocks.emplace(b, p);
+    bp.blocks[current_device()].emplace(b, p);
     bp.total += b;
     return;
   }
@@ -555,6 +586,76 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   return intrc_create_impl(elems, r, ext, storage, handle, true);
 }
 
+static int check_materials(const RadB200Relax *r)
+{
+  for (int e = 0; e < r->n_elem; e++)
+    if (r->mat_kind[e] < 0 || r->mat_kind[e] > 1) {
+      set_error("element %d: unsupported material kind %d", e, r->mat_kind[e]);
+      return RADB200_E_UNSUPPORTED;
+    }
+  return 0;
+}
+
+int radb200_intrc_load(const RadB200Relax *r, const float *N, const double *h_ext, int64_t *handle)
+{
+  if (!r || !N || !handle || r->n_elem <= 0 || !r->mat_kind || !r->mat) { set_error("bad arguments"); return RADB200_E_ARG; }
+  RB_TRY(check_materials(r));
+  std::unique_ptr<Intrc> I(new Intrc());
+  const int n = r->n_elem;
+  I->n = n;
+  I->n3 = 3 * n;
+  I->ld = (I->n3 + 31) / 32 * 32;
+  I->storage = RADB200_STORE_F32;
+  I->geom_ok = 0;
+  RB_TRY(I->mat_kind.upload(r->mat_kind, (size_t)n * sizeof(int)));
+  RB_TRY(I->mat.upload(r->mat, (size_t)n * RADB200_MAT_STRIDE * sizeof(double)));
+  I->h_mat_kind.assign(r->mat_kind, r->mat_kind + n);
+  I->h_mat.assign(r->mat, r->mat + (size_t)n * RADB200_MAT_STRIDE);
+  const size_t nn = (size_t)I->n3 * I->ld;
+  RB_TRY(I->N32.alloc(nn * sizeof(float)));
+  RB_CUDA(cudaMemset(I->N32.p, 0, nn * sizeof(float)));
+  RB_CUDA(cudaMemcpy2D(I->N32.p, (size_t)I->ld * sizeof(float), N, (size_t)I->n3 * sizeof(float),
+                       (size_t)I->n3 * sizeof(float), (size_t)I->n3, cudaMemcpyHostToDevice));
+  const size_t vb = (size_t)I->ld * sizeof(double);
+  RB_TRY(I->hext.alloc(vb));
+  RB_CUDA(cudaMemset(I->hext.p, 0, vb));
+  if (h_ext) RB_CUDA(cudaMemcpy(I->hext.p, h_ext, (size_t)I->n3 * sizeof(double), cudaMemcpyHostToDevice));
+  RB_TRY(I->M.alloc(vb)); RB_TRY(I->H.alloc(vb)); RB_TRY(I->Mp.alloc(vb)); RB_TRY(I->F.alloc(vb));
+  RB_CUDA(cudaMemset(I->M.p, 0, vb)); RB_CUDA(cudaMemset(I->H.p, 0, vb));
+  RB_CUDA(cudaMemset(I->Mp.p, 0, vb)); RB_CUDA(cudaMemset(I->F.p, 0, vb));
+  {
+    uint64_t st = 1469598103934665603ULL;
+    int32_t hdr[3] = {n, -1, 0};
+    st = fnv1a(st, hdr, sizeof(hdr));
+    st = fnv1a(st, r->mat_kind, (size_t)n * sizeof(int32_t));
+    st = fnv1a(st, r->mat, (size_t)n * RADB200_MAT_STRIDE * sizeof(double));
+    I->stamp = st;
+  }
+  RB_CUDA(cudaDeviceSynchronize());
+  int64_t h = g_next_handle++;
+  g_intrc[h] = std::move(I);
+  *handle = h;
+  return 0;
+}
+
+int radb200_intrc_set_materials(int64_t handle, const RadB200Relax *r)
+{
+  Intrc *I = find_intrc(handle);
+  if (!I) return RADB200_E_HANDLE;
+  if (!r || !r->mat_kind || !r->mat || r->n_elem != I->n) { set_error("bad arguments"); return RADB200_E_ARG; }
+  RB_TRY(check_materials(r));
+  RB_TRY(I->mat_kind.upload(r->mat_kind, (size_t)I->n * sizeof(int)));
+  RB_TRY(I->mat.upload(r->mat, (size_t)I->n * RADB200_MAT_STRIDE * sizeof(double)));
+  I->h_mat_kind.assign(r->mat_kind, r->mat_kind + I->n);
+  I->h_mat.assign(r->mat, r->mat + (size_t)I->n * RADB200_MAT_STRIDE);
+  // factors and the converged state belong to the old materials
+  I->drop_lu_graphs();
+  I->lu_mode = -1;
+  I->lu_of_d = 0;
+  I->last_kind = -1;
+  return 0;
+}
+
 // ---- saving and restoring the device state of an interaction --------------
 namespace {
 const char STATE_MAGIC[8] = {'R', 'B', '2', '0', '0', 'I', 'S', '1'};
@@ -800,6 +901,7 @@ int radb200_adjoint_grad(int64_t handle, const double *lambda, double *dL_dMr, d
   if (!I) return RADB200_E_HANDLE;
   if (!lambda) { set_error("bad adjoint arguments"); return RADB200_E_ARG; }
   if (I->last_kind < 0) { set_error("adjoint: no converged solve on this interaction"); return RADB200_E_ARG; }
+  if (!I->geom_ok && (dL_dc || dL_dd)) { set_error("adjoint: no element geometry (interaction loaded from a matrix)"); return RADB200_E_UNSUPPORTED; }
   return adjoint_grad(*I, lambda, dL_dMr, dL_dchi, dL_dc, dL_dd);
 }
 
@@ -809,6 +911,7 @@ int radb200_field_vjp(int64_t handle, const double *M, const double *pts, int64_
   Intrc *I = find_intrc(handle);
   if (!I) return RADB200_E_HANDLE;
   if (!M || !pts || !W || npts < 0 || what < 0 || what > 1) { set_error("bad field_vjp arguments"); return RADB200_E_ARG; }
+  if (!I->geom_ok) { set_error("field_vjp: no element geometry (interaction loaded from a matrix)"); return RADB200_E_UNSUPPORTED; }
   return field_vjp(*I, M, pts, npts, what, W, g_M, g_c, g_d);
 }
 

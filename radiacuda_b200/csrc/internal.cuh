@@ -131,6 +131,7 @@ struct Intrc {
   int ld = 0;       // padded leading dimension of N (multiple of 32)
   int storage = 0;
   int fast = 0;     // polyhedra in the vertex/edge form
+  int geom_ok = 1;  // 0: loaded from a matrix assembled elsewhere (no element geometry)
   DevGeom geom;     // relaxable elements (object frames, images)
   DBuf elem_src, obs, rowT;           // [2n] int, [3n] obs points, [9n] s*Minv of main image
   DBuf N32, N64;                      // [n3 x ld]

@@ -8,13 +8,20 @@
 // radb200_field_noalloc evaluates B / H / M like radb200_field_dev but takes
 // EVERY array in device memory -- the geometry arrays of RadB200Geom included
 // -- and keeps its only scratch (per-chunk partial sums) in the file-scope
-// array below, reserved when the library is loaded.
+// array below.
 //
 // The scratch holds RADB200_NOALLOC_MAX_CHUNKS x RADB200_NOALLOC_MAX_POINTS x 3
-// doubles (3 MiB) on every GPU that loads the library, until the process
-// exits.  Every call shares it and it keeps the last call's contents; each
-// call overwrites the slices it reads.  Calls that overlap on the GPU (two
-// host threads, or two streams) race on it: serialize them.
+// doubles (3 MiB) on every GPU this entry point runs on, until the process
+// exits.  With lazy module loading (the CUDA default since 12.2) the driver
+// maps it on the first call on each device, when this file looks up its
+// address: that first call can fail for lack of device memory, so make it at
+// set-up, outside any stream capture.  Every call shares the scratch and it
+// keeps the last call's contents; each call overwrites the slices it reads.
+// Calls that overlap on the GPU (two host threads, or two streams) race on
+// it: serialize them.  The work runs on the calling thread's per-thread
+// default stream, which does not synchronize with other blocking streams
+// (a capture running on one of them elsewhere in the process is not
+// disturbed), and the call waits for it before returning.
 #include "internal.cuh"
 
 #define RADB200_NOALLOC_MAX_POINTS 16384
@@ -25,7 +32,9 @@ namespace rb {
 static __device__ __align__(256) double g_noalloc_scratch[RADB200_NOALLOC_MAX_CHUNKS * RADB200_NOALLOC_MAX_POINTS * 3];
 
 // device address of g_noalloc_scratch per device ordinal (host-side symbols are
-// stand-ins, not device addresses); filled by the first call on each device
+// stand-ins, not device addresses); filled by the first call on each device,
+// and looked up again if the cached address no longer belongs to this device
+// (a caller that reset the device with cudaDeviceReset)
 static double *g_noalloc_addr[64];
 
 // Field of source s of the concatenated list [cuboids, polyhedra, arcs,
@@ -61,6 +70,7 @@ __device__ V3<double> noalloc_source(const RadB200Geom &G, const Guard &gd, int 
       }
     } else if (kind == 1) {
       const double *pr = G.poly + (size_t)idx * RADB200_POLY_STRIDE;
+      // the reference's polygon face form uses this 15-digit pi (radplnr2.cpp:32)
       const double C = 1.0 / (4.0 * 3.14159265358979);
       int f0 = G.poly_info[4 * idx], nf = G.poly_info[4 * idx + 1], inside = 1;
       double hx = 0, hy = 0, hz = 0;
@@ -147,18 +157,27 @@ extern "C" RADB200_API int radb200_field_noalloc(const RadB200Geom *g, const dou
   int dev = 0;
   RB_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) { set_error("radb200_field_noalloc: device ordinal out of range"); return RADB200_E_ARG; }
+  if (g_noalloc_addr[dev]) {
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, g_noalloc_addr[dev]) != cudaSuccess || pa.type != cudaMemoryTypeDevice ||
+        pa.device != dev) {
+      cudaGetLastError();
+      g_noalloc_addr[dev] = nullptr;
+    }
+  }
   if (!g_noalloc_addr[dev]) {
     // set-up, once per device, with that device current: the device address of the scratch
     void *p = nullptr;
     RB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     g_noalloc_addr[dev] = (double *)p;
   }
+  const cudaStream_t st = cudaStreamPerThread;
   double *scratch = g_noalloc_addr[dev];
   int nsrc = g->n_rec + g->n_poly + g->n_arc + g->n_bkg;
   int n3 = (int)npts * 3;
   if (nsrc == 0) {
-    RB_CUDA(cudaMemsetAsync(d_out, 0, (size_t)n3 * sizeof(double), 0));
-    RB_CUDA(cudaStreamSynchronize(0));
+    RB_CUDA(cudaMemsetAsync(d_out, 0, (size_t)n3 * sizeof(double), st));
+    RB_CUDA(cudaStreamSynchronize(st));
     return 0;
   }
   // as many source chunks as fit the scratch, up to ~8 CTAs per SM in total
@@ -168,10 +187,10 @@ extern "C" RADB200_API int radb200_field_noalloc(const RadB200Geom *g, const dou
   int chunk = (nsrc + nchunk - 1) / nchunk;
   nchunk = (nsrc + chunk - 1) / chunk;
   Guard gd{g->abs_rand, g->rel_rand, g->zero_rand};
-  noalloc_field_kernel<<<dim3(nblk, nchunk), 128>>>(*g, gd, d_pts, (int)npts, what, nsrc, chunk, scratch);
+  noalloc_field_kernel<<<dim3(nblk, nchunk), 128, 0, st>>>(*g, gd, d_pts, (int)npts, what, nsrc, chunk, scratch);
   RB_TRY(check_launch("noalloc_field_kernel"));
-  noalloc_reduce_kernel<<<(n3 + 255) / 256, 256>>>(scratch, nchunk, n3, d_out);
+  noalloc_reduce_kernel<<<(n3 + 255) / 256, 256, 0, st>>>(scratch, nchunk, n3, d_out);
   RB_TRY(check_launch("noalloc_reduce_kernel"));
-  RB_CUDA(cudaStreamSynchronize(0));
+  RB_CUDA(cudaStreamSynchronize(st));
   return 0;
 }

@@ -1264,11 +1264,15 @@ def UtiMPI(mode: str, data=None, rankFrom: int = 0, rankTo: int = -1):
     torch.distributed default process group in place of MPI (one process
     per GPU).  'on' and 'in' return this process's rank (0 when no group is
     initialized: this library does not start one), 'off' returns it and
-    leaves the group to its owner, 'barrier' waits for every rank.  'share'
-    sends data, flattened to floats as the reference does, from rankFrom to
-    every rank (rankTo = -1) or to rankTo, and returns the flat list; a rank
-    that receives nothing gets its own data back.  Without data the rank is
-    returned, as in the reference."""
+    leaves the group to its owner, 'barrier' waits for every rank.
+
+    'share' follows radTApplication's MPI share (radapl1.cpp:2345-2440):
+    with rankTo < 0 every rank joins a broadcast from rankFrom, whether or
+    not it passes data; with rankTo >= 0 only rankFrom and rankTo take part,
+    rankFrom sending the count and then the values.  A rank that passed data
+    gets the shared values back, flattened to floats (its own data when it
+    received nothing); a rank without data gets its rank, as in the
+    reference.  rankFrom must pass data."""
     m = str(mode).strip().lower()
     if m not in ("on", "in", "off", "share", "barrier"):
         raise RadiaError("Radia::Error000: UtiMPI: the first argument should be 'on', 'in', 'off', 'share' or "
@@ -1283,16 +1287,34 @@ def UtiMPI(mode: str, data=None, rankFrom: int = 0, rankTo: int = -1):
     rank = dist.get_rank() if dist is not None else 0
     if m == "barrier" and dist is not None:
         dist.barrier()
-    if m != "share" or data is None:
+    if m != "share":
         return rank
-    flat = _flat_floats(data)
+    flat = _flat_floats(data) if data is not None else None
     if dist is None:
+        return rank if flat is None else flat
+    src, dst = int(rankFrom), int(rankTo)
+    if rank == src and flat is None:
+        raise RadiaError("Radia::Error601: UtiMPI share: the sending rank has no data")
+    if dst < 0:
+        box = [flat if rank == src else None]
+        dist.broadcast_object_list(box, src=src)
+        return rank if flat is None else [float(v) for v in box[0]]
+    if rank not in (src, dst):
+        return rank if flat is None else flat
+    import torch
+    dev = (torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl"
+           else torch.device("cpu"))
+    if rank == src:
+        dist.send(torch.tensor([len(flat)], dtype=torch.int64, device=dev), dst)
+        if flat:
+            dist.send(torch.tensor(flat, dtype=torch.float64, device=dev), dst)
         return flat
-    box = [flat if rank == int(rankFrom) else None]
-    dist.broadcast_object_list(box, src=int(rankFrom))
-    if int(rankTo) < 0 or rank == int(rankTo):
-        return [float(v) for v in box[0]]
-    return flat
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    dist.recv(cnt, src)
+    buf = torch.empty(int(cnt.item()), dtype=torch.float64, device=dev)
+    if buf.numel():
+        dist.recv(buf, src)
+    return rank if flat is None else [float(v) for v in buf.cpu().tolist()]
 
 
 def UtiVer() -> float:

@@ -45,7 +45,7 @@ def _points(name, pts):
     return rng.uniform(-60, 80, size=(60, 3)) + np.array([0.0137, 0.0291, 0.0413])
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=os.environ.get("RADIA_REFERENCE", "/root/reference")):
     out = {"provenance": "reference Radia CPU module built by oracle/Makefile.ref, FldLenRndSw('off')"}
     # known answer: reference example 1 (cube 1 mm, M = [-0.5, 1, 0.7], B at [0.52, 0.6, 0.7])
     R.UtiDelAll()

@@ -1,10 +1,10 @@
 """Small, self-contained launches of the hot kernels for profiling.
 
-    python -m radiacuda_b200.profile_cases field    [--tets N] [--points P] [--precision double|single|fast]
-    python -m radiacuda_b200.profile_cases assemble [--tets N]
-    python -m radiacuda_b200.profile_cases lu       [--tets N] [--mode 0|1]
-    python -m radiacuda_b200.profile_cases relax    [--blocks N]
-    python -m radiacuda_b200.profile_cases adjoint  [--pairs N] [--points P]
+    python tests/profile_cases.py field    [--tets N] [--points P] [--precision double|single|fast]
+    python tests/profile_cases.py assemble [--tets N]
+    python tests/profile_cases.py lu       [--tets N] [--mode 0|1]
+    python tests/profile_cases.py relax    [--blocks N]
+    python tests/profile_cases.py adjoint  [--pairs N] [--points P]
 
 Each case builds a seeded model of the benchmark's shapes (tetrahedral mesh
 of chi = 1000 material, magnet array) at a size that keeps one launch of the
@@ -21,11 +21,11 @@ import time
 import numpy as np
 
 
-def _models():
-    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    sys.path.insert(0, os.path.join(here, "tests"))
-    import models
-    return models
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.dirname(HERE))
+
+import models as MD  # noqa: E402
 
 
 def main(argv=None):
@@ -38,8 +38,7 @@ def main(argv=None):
     ap.add_argument("--mode", type=int, default=1)
     ap.add_argument("--precision", default="double", choices=["double", "single", "fast"])
     a = ap.parse_args(argv)
-    from . import _native, model, rad
-    MD = _models()
+    from radiacuda_b200 import _native, model, rad
     t0 = time.perf_counter()
     if a.case in ("field", "assemble", "lu"):
         ncell = int(np.ceil((a.tets / 6) ** (1 / 3)))
@@ -61,7 +60,7 @@ def main(argv=None):
             st = rad.RlxAuto(im, 1e-13, 200, 12 if a.mode == 0 else 13)
             print("lu mode", a.mode, time.perf_counter() - t0, "s", st)
     elif a.case == "adjoint":
-        from .adjoint import FieldProblem
+        from radiacuda_b200.adjoint import FieldProblem
         h = MD.hybrid_undulator(rad, n_pairs=a.pairs)[0]
         P = MD.hybrid_points(a.points, n_pairs=a.pairs)
         prob = FieldProblem(h, P, "b", prec=1e-12)

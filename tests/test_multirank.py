@@ -183,6 +183,51 @@ def test_utimpi_over_two_gloo_ranks():
     assert res[1]["to0"] == [10.0, 1.0, 2.0]
 
 
+def _utimpi_partial_main(rank, world, port, out):
+    import sys
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from radiacuda_b200 import rad
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        res = {}
+        # broadcast from rank 2: the receivers pass no data but still join
+        res["bcast"] = rad.UtiMPI("share", [[7.0, 8.0]] if rank == 2 else None, 2)
+        # point to point from rank 1 to rank 0: rank 2 does not call share at all
+        if rank in (0, 1):
+            res["p2p"] = rad.UtiMPI("share", [[1.5 + rank, 2.5]] if rank == 1 else None, 1, 0)
+        res["barrier"] = rad.UtiMPI("barrier")
+        out[rank] = res
+    finally:
+        dist.destroy_process_group()
+
+
+def test_utimpi_share_with_receivers_without_data_over_three_gloo_ranks():
+    """'share' as the reference's MPI share: receivers that pass no data join
+    the broadcast and get their rank back; a rankTo >= 0 share involves only
+    the sending and the receiving rank."""
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    with ctx.Manager() as m:
+        out = m.dict()
+        procs = [ctx.Process(target=_utimpi_partial_main, args=(r, 3, port, out)) for r in range(3)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=120)
+            assert p.exitcode == 0
+        res = dict(out)
+    assert res[0]["bcast"] == 0 and res[1]["bcast"] == 1 and res[2]["bcast"] == [7.0, 8.0]
+    assert res[1]["p2p"] == [2.5, 2.5]
+    assert res[0]["p2p"] == 0
+    assert "p2p" not in res[2]
+    assert [res[r]["barrier"] for r in range(3)] == [0, 1, 2]
+
+
 def test_utimpi_without_a_process_group(rad):
     assert rad.UtiMPI("on") == 0 and rad.UtiMPI("barrier") == 0 and rad.UtiMPI("off") == 0
     assert rad.UtiMPI("share", [[1, 2], [3]]) == [1.0, 2.0, 3.0]

@@ -59,7 +59,9 @@ def test_field_noalloc_matches_allocating_entry_point(cuda, rad):
 
     L = _native.lib()
     L.radb200_field_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
-    h = MD.mixed_sym(rad)
+    # mixed cuboids, tetrahedra, arcs and a racetrack, plus a uniform
+    # background (a source kind with no M and no inside test)
+    h = rad.ObjCnt([MD.mixed_sym(rad), rad.ObjBckg([0.11, -0.07, 0.23])])
     rng = np.random.default_rng(21)
     for lf in model.collect_leaves(rad._objs, h):
         if hasattr(lf.obj, "m") and not (hasattr(lf.obj, "j") and np.any(lf.obj.j != 0)):
@@ -68,7 +70,9 @@ def test_field_noalloc_matches_allocating_entry_point(cuda, rad):
     g, keep = _device_geom(arrs, torch, cuda)
     P = rng.uniform(-90, 90, size=(3000, 3))
     d_pts = torch.from_numpy(P).to(cuda)
-    for what in (0, 1):
+    # sample points inside the magnets too, so the M path (what == 2) sees both sides
+    P[:200] = [c for c in _inside_points(arrs, 200, rng)]
+    for what in (0, 1, 2):
         ref = _native.field(arrs, P, what, 0)
         for call in range(2):
             d_out = torch.full((P.shape[0], 3), float("nan"), dtype=torch.float64, device=cuda)
@@ -76,8 +80,28 @@ def test_field_noalloc_matches_allocating_entry_point(cuda, rad):
                                          C.c_void_p(d_out.data_ptr()))
             _native.check(rc, "radb200_field_noalloc")
             got = d_out.cpu().numpy()
+            if what == 2:
+                assert np.array_equal(got, ref), (what, call)
+                assert np.abs(ref).max() > 0
+                continue
             err = np.abs(got - ref).max() / np.abs(ref).max()
             assert err < 1e-10, (what, call, err)
+
+
+def _inside_points(arrs, n, rng):
+    """Points inside the cuboids (centre + a fraction of the half widths),
+    mapped by each cuboid's first image."""
+    rec, img, trf = arrs["rec"], arrs["rec_img"], arrs["trf"]
+    out = []
+    for k in range(n):
+        i = k % rec.shape[0]
+        if np.any(rec[i, 9:12] != 0):
+            i = 0
+        q = rec[i, 0:3] + rng.uniform(-0.4, 0.4, 3) * rec[i, 3:6]
+        T = trf[img[i, 0]]
+        M = np.linalg.inv(T[0:9].reshape(3, 3))
+        out.append(M @ q + T[9:12])
+    return np.array(out)
 
 
 def test_field_noalloc_rejects_oversized_calls(cuda, rad):
