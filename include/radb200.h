@@ -107,7 +107,9 @@ typedef struct RadB200Geom {
  *   kind 0 (linear):   [0..8] chi tensor, [9..11] Mr          (radmater.h:164-362)
  *   kind 1 (tanh):     [0..2] ksi_i, [3..5] ms_i, [6] count, [9..11] Mr
  *                      |M| = sum ms_i tanh(ksi_i |H| / ms_i)  (radmater.h:417-600)
- *   kind 2 (table):    [0] first point, [1] count into mh_table (H, M, dM/dH)  */
+ *   kind 2 (table):    [0] first row, [1] rows (>= 2, H ascending) of
+ *                      mh_table (H, M, dM/dH), [9..11] Mr; |M|(|H|) cubic
+ *                      between the rows (radmater.cpp:618-710), M || H     */
 #define RADB200_MAT_STRIDE 12
 #define RADB200_MAT_LINEAR 0
 #define RADB200_MAT_TANH   1
@@ -231,7 +233,11 @@ RADB200_API int radb200_field_int_cb(const RadB200Geom *g, RadB200PointField fn,
  * radintrc.cpp:831-877) and the external field from every non-relaxable
  * source (radintrc.cpp:1208-1234) into device memory, where it stays for the
  * solves.  storage: 0 = FP32 matrix (the reference's layout),
- * 1 = FP64 matrix, 2 = FP32 matrix plus an FP64 copy of the near blocks.
+ * 1 = FP64 matrix, 2 = mixed: every block in FP32 and, for the near pairs
+ * (an image of element j within RADB200_NEAR_FACTOR (default 1.5) times the
+ * sum of the two elements' radii of element i's centre; the self block
+ * always), the FP64 residue of the block, which the refinement residual,
+ * the relaxation and the adjoint's transposed products add back in FP64.
  * ext may be NULL (no external sources).                                     */
 #define RADB200_STORE_F32   0
 #define RADB200_STORE_F64   1

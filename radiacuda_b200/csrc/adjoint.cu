@@ -288,13 +288,13 @@ __global__ void __launch_bounds__(ADJ_T) matvec_t_kernel(const MT *__restrict__ 
 // coef[e] = B^T (9), P^-T (9), Qd^T (9); lu != 0: B^T = chi^T, P^-T = I, Qd^T = 0.
 template <typename MT>
 __global__ void adj_prep_kernel(const MT *__restrict__ N, int ld, int n, const double *__restrict__ H,
-                                const int *__restrict__ kind, const double *__restrict__ mat, int lu,
-                                double *__restrict__ coef)
+                                const int *__restrict__ kind, const double *__restrict__ mat,
+                                const double *__restrict__ mh, int lu, double *__restrict__ coef)
 {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
   double D[9], *c = coef + (size_t)e * 27;
-  mat_D(kind[e], mat + (size_t)e * RADB200_MAT_STRIDE, mk3<double>(H[3 * e], H[3 * e + 1], H[3 * e + 2]), D);
+  mat_D(kind[e], mat + (size_t)e * RADB200_MAT_STRIDE, mk3<double>(H[3 * e], H[3 * e + 1], H[3 * e + 2]), D, mh);
   if (lu) {
     for (int a = 0; a < 3; a++)
       for (int b = 0; b < 3; b++) {
@@ -359,12 +359,12 @@ __global__ void adj_finish_kernel(const double *__restrict__ part, int nchunk, i
 
 // X_e = D_e = dM/dH at H_e, in the layout of a material record's chi slots
 __global__ void adj_dmat_kernel(const double *__restrict__ H, const int *__restrict__ kind, const double *__restrict__ mat,
-                                int n, double *__restrict__ X)
+                                const double *__restrict__ mh, int n, double *__restrict__ X)
 {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
   double D[9];
-  mat_D(kind[e], mat + (size_t)e * RADB200_MAT_STRIDE, mk3<double>(H[3 * e], H[3 * e + 1], H[3 * e + 2]), D);
+  mat_D(kind[e], mat + (size_t)e * RADB200_MAT_STRIDE, mk3<double>(H[3 * e], H[3 * e + 1], H[3 * e + 2]), D, mh);
   for (int k = 0; k < 9; k++) X[(size_t)e * RADB200_MAT_STRIDE + k] = D[k];
   for (int k = 9; k < RADB200_MAT_STRIDE; k++) X[(size_t)e * RADB200_MAT_STRIDE + k] = 0.0;
 }
@@ -372,12 +372,13 @@ __global__ void adj_dmat_kernel(const double *__restrict__ H, const int *__restr
 // u_e = rowT_e^T D_e^T lambda_e (lab-frame weight of element e's field row)
 __global__ void adj_weight_kernel(const double *__restrict__ lambda, const double *__restrict__ H,
                                   const int *__restrict__ kind, const double *__restrict__ mat,
-                                  const double *__restrict__ rowT, int n, double *__restrict__ u)
+                                  const double *__restrict__ mh, const double *__restrict__ rowT, int n,
+                                  double *__restrict__ u)
 {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
   double D[9];
-  mat_D(kind[e], mat + (size_t)e * RADB200_MAT_STRIDE, mk3<double>(H[3 * e], H[3 * e + 1], H[3 * e + 2]), D);
+  mat_D(kind[e], mat + (size_t)e * RADB200_MAT_STRIDE, mk3<double>(H[3 * e], H[3 * e + 1], H[3 * e + 2]), D, mh);
   double l0 = lambda[3 * e], l1 = lambda[3 * e + 1], l2 = lambda[3 * e + 2];
   double mu[3];
   for (int b = 0; b < 3; b++) mu[b] = D[b] * l0 + D[3 + b] * l1 + D[6 + b] * l2;
@@ -393,12 +394,19 @@ static int matvec_t(Intrc &I, const double *x, DBuf &part, int *nchunk_out, cuda
   int nchunk = std::max(1, std::min(64, (148 * 4 + tiles - 1) / tiles));
   int rows = (I.n3 + nchunk - 1) / nchunk;
   nchunk = (I.n3 + rows - 1) / rows;
-  RB_TRY(part.alloc((size_t)nchunk * I.ld * sizeof(double)));
+  // mixed storage: one more partial slice holds the near residue's D^T x
+  const int extra = I.near_nnz > 0 ? 1 : 0;
+  RB_TRY(part.alloc((size_t)(nchunk + extra) * I.ld * sizeof(double)));
   dim3 grid(tiles, nchunk);
   if (I.N64.p) matvec_t_kernel<double><<<grid, ADJ_T, 0, st>>>(I.N64.as<double>(), I.ld, I.n3, x, rows, part.as<double>());
   else matvec_t_kernel<float><<<grid, ADJ_T, 0, st>>>(I.N32.as<float>(), I.ld, I.n3, x, rows, part.as<double>());
   RB_TRY(check_launch("matvec_t_kernel"));
-  *nchunk_out = nchunk;
+  if (extra) {
+    double *slice = part.as<double>() + (size_t)nchunk * I.ld;
+    RB_CUDA(cudaMemsetAsync(slice, 0, (size_t)I.ld * sizeof(double), st));
+    RB_TRY(launch_near_t(I, x, slice, st));
+  }
+  *nchunk_out = nchunk + extra;
   return 0;
 }
 
@@ -459,17 +467,17 @@ int adjoint_solve(Intrc &I, const double *dLdM, double rtol, int max_iter, doubl
     } else {
       DBuf X;
       RB_TRY(X.alloc((size_t)n * RADB200_MAT_STRIDE * sizeof(double)));
-      adj_dmat_kernel<<<nb, 128>>>(H, I.mat_kind.as<int>(), I.mat.as<double>(), n, X.as<double>());
+      adj_dmat_kernel<<<nb, 128>>>(H, I.mat_kind.as<int>(), I.mat.as<double>(), I.mh.as<double>(), n, X.as<double>());
       RB_TRY(check_launch("adj_dmat_kernel"));
       const int mode = n3 >= 3072 ? RADB200_LU_TF32 : RADB200_LU_F64;
       if (lu_build_x(I, mode, X.as<double>(), 1, &tfac) == 0) use_lu = 1;
     }
   }
   if (I.N64.p)
-    adj_prep_kernel<double><<<nb, 128>>>(I.N64.as<double>(), ld, n, H, I.mat_kind.as<int>(), I.mat.as<double>(), use_lu,
+    adj_prep_kernel<double><<<nb, 128>>>(I.N64.as<double>(), ld, n, H, I.mat_kind.as<int>(), I.mat.as<double>(), I.mh.as<double>(), use_lu,
                                          coef.as<double>());
   else
-    adj_prep_kernel<float><<<nb, 128>>>(I.N32.as<float>(), ld, n, H, I.mat_kind.as<int>(), I.mat.as<double>(), use_lu,
+    adj_prep_kernel<float><<<nb, 128>>>(I.N32.as<float>(), ld, n, H, I.mat_kind.as<int>(), I.mat.as<double>(), I.mh.as<double>(), use_lu,
                                         coef.as<double>());
   RB_TRY(check_launch("adj_prep_kernel"));
   AdjOp op(I, coef.as<double>(), t, part, use_lu);
@@ -548,7 +556,7 @@ int adjoint_grad(Intrc &I, const double *lambda, double *dMr, double *dchi, doub
   }
   if (!dc && !dd) return 0;
   int nb = (n + 127) / 128;
-  adj_weight_kernel<<<nb, 128>>>(lam, H, I.mat_kind.as<int>(), I.mat.as<double>(), I.rowT.as<double>(), n, u);
+  adj_weight_kernel<<<nb, 128>>>(lam, H, I.mat_kind.as<int>(), I.mat.as<double>(), I.mh.as<double>(), I.rowT.as<double>(), n, u);
   RB_TRY(check_launch("adj_weight_kernel"));
   // sources: every element at its converged M; observers: the element centres
   DBuf srcout, obsout, part;

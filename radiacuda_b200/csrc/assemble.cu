@@ -106,6 +106,37 @@ int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, c
   return 0;
 }
 
+// FP64 residue of the near pairs of mixed storage: the block computed again
+// in FP64 minus its stored FP32 rounding (read back, so the residue is exact
+// whatever the compiler did with the first evaluation).
+__global__ void __launch_bounds__(128) assemble_near_kernel(GeomView g, const int *__restrict__ elem_src,
+                                                            const double *__restrict__ obs, const double *__restrict__ rowT,
+                                                            int ld, const float *__restrict__ N32,
+                                                            const int *__restrict__ row, const int *__restrict__ col,
+                                                            int64_t nnz, double *__restrict__ D)
+{
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nnz) return;
+  const int i = row[k], j = col[k];
+  V3<double> o = mk3<double>(__ldg(obs + 3 * i), __ldg(obs + 3 * i + 1), __ldg(obs + 3 * i + 2));
+  double R[9], blk[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) R[q] = __ldg(rowT + 9 * (size_t)i + q);
+  pair_block(g, elem_src, o, R, j, blk);
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) D[9 * k + 3 * a + b] = blk[3 * a + b] - (double)N32[(size_t)(3 * i + a) * ld + 3 * j + b];
+}
+
+int launch_assemble_near(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int ld,
+                         const float *N32, const int *row, const int *col, int64_t nnz, double *D, cudaStream_t st)
+{
+  if (nnz == 0) return 0;
+  assemble_near_kernel<<<(unsigned)((nnz + 127) / 128), 128, 0, st>>>(g, elem_src, obs, rowT, ld, N32, row, col, nnz, D);
+  return check_launch("assemble_near_kernel");
+}
+
 __global__ void round_f32_kernel(const double *__restrict__ a, float *__restrict__ b, size_t n)
 {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -483,6 +483,45 @@ static uint64_t fnv1a(uint64_t h, const void *p, size_t n)
   return h;
 }
 
+// Material records: linear and tanh laws, and tables whose rows lie inside
+// mh_table with H ascending (the reference's MatSatIsoTab check,
+// radapl2.cpp:152-166) and at least two points.
+static int check_materials(const RadB200Relax *r)
+{
+  for (int e = 0; e < r->n_elem; e++) {
+    const int k = r->mat_kind[e];
+    if (k < 0 || k > 2) {
+      set_error("element %d: unsupported material kind %d", e, k);
+      return RADB200_E_UNSUPPORTED;
+    }
+    if (k != RADB200_MAT_TABLE) continue;
+    const double *m = r->mat + (size_t)e * RADB200_MAT_STRIDE;
+    const double f = m[0], c = m[1];
+    if (!(f >= 0) || !(c >= 2) || f != floor(f) || c != floor(c) || f + c > (double)r->n_mh || !r->mh_table) {
+      set_error("element %d: M(H) table rows outside the table array", e);
+      return RADB200_E_ARG;
+    }
+    for (int q = 1; q < (int)c; q++)
+      if (!(r->mh_table[3 * ((size_t)f + q)] > r->mh_table[3 * ((size_t)f + q - 1)])) {
+        set_error("element %d: M(H) table not ascending in H", e);
+        return RADB200_E_ARG;
+      }
+  }
+  return 0;
+}
+
+// device copies of the material records and tables
+static int upload_materials(Intrc &I, const RadB200Relax *r)
+{
+  RB_TRY(I.mat_kind.upload(r->mat_kind, (size_t)I.n * sizeof(int)));
+  RB_TRY(I.mat.upload(r->mat, (size_t)I.n * RADB200_MAT_STRIDE * sizeof(double)));
+  if (r->n_mh > 0) RB_TRY(I.mh.upload(r->mh_table, (size_t)r->n_mh * 3 * sizeof(double)));
+  else I.mh.release();
+  I.h_mat_kind.assign(r->mat_kind, r->mat_kind + I.n);
+  I.h_mat.assign(r->mat, r->mat + (size_t)I.n * RADB200_MAT_STRIDE);
+  return 0;
+}
+
 // assemble = false builds everything but leaves the matrix zero (a restored
 // state fills it)
 static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, const RadB200Geom *ext, int storage,
@@ -499,11 +538,8 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
       set_error("element %d refers to a missing source", e);
       return RADB200_E_ARG;
     }
-    if (r->mat_kind[e] < 0 || r->mat_kind[e] > 1) {
-      set_error("element %d: unsupported material kind %d", e, r->mat_kind[e]);
-      return RADB200_E_UNSUPPORTED;
-    }
   }
+  RB_TRY(check_materials(r));
   std::unique_ptr<Intrc> I(new Intrc());
   I->n = n;
   I->n3 = 3 * n;
@@ -545,18 +581,17 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
     I->stamp = st;
   }
   RB_TRY(I->elem_src.upload(r->elem_src, 2 * (size_t)n * sizeof(int)));
-  RB_TRY(I->mat_kind.upload(r->mat_kind, (size_t)n * sizeof(int)));
-  RB_TRY(I->mat.upload(r->mat, (size_t)n * RADB200_MAT_STRIDE * sizeof(double)));
-  I->h_mat_kind.assign(r->mat_kind, r->mat_kind + n);
-  I->h_mat.assign(r->mat, r->mat + (size_t)n * RADB200_MAT_STRIDE);
+  RB_TRY(upload_materials(*I, r));
   size_t nn = (size_t)I->n3 * I->ld;
-  if (storage == RADB200_STORE_F64 || storage == RADB200_STORE_MIXED) RB_TRY(I->N64.alloc(nn * sizeof(double)));
+  // mixed: every block in FP32, the near ones also as their FP64 residue
+  if (storage == RADB200_STORE_F64) RB_TRY(I->N64.alloc(nn * sizeof(double)));
   if (storage == RADB200_STORE_F32 || storage == RADB200_STORE_MIXED) RB_TRY(I->N32.alloc(nn * sizeof(float)));
   if (I->N64.p) RB_CUDA(cudaMemsetAsync(I->N64.p, 0, nn * sizeof(double)));
   if (I->N32.p) RB_CUDA(cudaMemsetAsync(I->N32.p, 0, nn * sizeof(float)));
   if (assemble)
     RB_TRY(launch_assemble(I->geom.view(fast), I->elem_src.as<int>(), I->obs.as<double>(), I->rowT.as<double>(), n, I->ld,
                            I->N32.as<float>(), I->N64.as<double>(), 0));
+  if (storage == RADB200_STORE_MIXED) RB_TRY(build_near(*I, elems, r, obs.data()));
   // external field at element centres, in element frames
   size_t vb = (size_t)I->ld * sizeof(double);
   RB_TRY(I->hext.alloc(vb));
@@ -586,16 +621,6 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   return intrc_create_impl(elems, r, ext, storage, handle, true);
 }
 
-static int check_materials(const RadB200Relax *r)
-{
-  for (int e = 0; e < r->n_elem; e++)
-    if (r->mat_kind[e] < 0 || r->mat_kind[e] > 1) {
-      set_error("element %d: unsupported material kind %d", e, r->mat_kind[e]);
-      return RADB200_E_UNSUPPORTED;
-    }
-  return 0;
-}
-
 int radb200_intrc_load(const RadB200Relax *r, const float *N, const double *h_ext, int64_t *handle)
 {
   if (!r || !N || !handle || r->n_elem <= 0 || !r->mat_kind || !r->mat) { set_error("bad arguments"); return RADB200_E_ARG; }
@@ -607,10 +632,7 @@ int radb200_intrc_load(const RadB200Relax *r, const float *N, const double *h_ex
   I->ld = (I->n3 + 31) / 32 * 32;
   I->storage = RADB200_STORE_F32;
   I->geom_ok = 0;
-  RB_TRY(I->mat_kind.upload(r->mat_kind, (size_t)n * sizeof(int)));
-  RB_TRY(I->mat.upload(r->mat, (size_t)n * RADB200_MAT_STRIDE * sizeof(double)));
-  I->h_mat_kind.assign(r->mat_kind, r->mat_kind + n);
-  I->h_mat.assign(r->mat, r->mat + (size_t)n * RADB200_MAT_STRIDE);
+  RB_TRY(upload_materials(*I, r));
   const size_t nn = (size_t)I->n3 * I->ld;
   RB_TRY(I->N32.alloc(nn * sizeof(float)));
   RB_CUDA(cudaMemset(I->N32.p, 0, nn * sizeof(float)));
@@ -644,10 +666,7 @@ int radb200_intrc_set_materials(int64_t handle, const RadB200Relax *r)
   if (!I) return RADB200_E_HANDLE;
   if (!r || !r->mat_kind || !r->mat || r->n_elem != I->n) { set_error("bad arguments"); return RADB200_E_ARG; }
   RB_TRY(check_materials(r));
-  RB_TRY(I->mat_kind.upload(r->mat_kind, (size_t)I->n * sizeof(int)));
-  RB_TRY(I->mat.upload(r->mat, (size_t)I->n * RADB200_MAT_STRIDE * sizeof(double)));
-  I->h_mat_kind.assign(r->mat_kind, r->mat_kind + I->n);
-  I->h_mat.assign(r->mat, r->mat + (size_t)I->n * RADB200_MAT_STRIDE);
+  RB_TRY(upload_materials(*I, r));
   // factors and the converged state belong to the old materials
   I->drop_lu_graphs();
   I->lu_mode = -1;
@@ -667,7 +686,7 @@ struct StateHeader {
   int64_t solve_id, lu_solve_id;
   int32_t nsec, pad;
 };
-enum { SEC_N64 = 1, SEC_N32, SEC_HEXT, SEC_M, SEC_LASTM, SEC_LU64, SEC_LU32, SEC_LUINV };
+enum { SEC_N64 = 1, SEC_N32, SEC_HEXT, SEC_M, SEC_LASTM, SEC_LU64, SEC_LU32, SEC_LUINV, SEC_NEARD };
 struct Sec {
   int64_t tag;
   DBuf *buf;
@@ -680,6 +699,7 @@ std::vector<Sec> state_sections(Intrc &I)
   std::vector<Sec> v;
   if (I.N64.p) v.push_back({SEC_N64, &I.N64, nn * 8});
   if (I.N32.p) v.push_back({SEC_N32, &I.N32, nn * 4});
+  if (I.near_nnz > 0) v.push_back({SEC_NEARD, &I.near_D, I.near_nnz * 72});
   v.push_back({SEC_HEXT, &I.hext, vb});
   v.push_back({SEC_M, &I.M, vb});
   if (I.last_kind >= 0 && I.lastM.p) v.push_back({SEC_LASTM, &I.lastM, vb});
@@ -754,6 +774,7 @@ int radb200_intrc_restore(const RadB200Geom *elems, const RadB200Relax *r, const
     switch (tag) {
       case SEC_N64: dst = &I->N64; want = nn * 8; break;
       case SEC_N32: dst = &I->N32; want = nn * 4; break;
+      case SEC_NEARD: dst = &I->near_D; want = I->near_nnz * 72; break;
       case SEC_HEXT: dst = &I->hext; want = (int64_t)I->ld * 8; break;
       case SEC_M: dst = &I->M; want = (int64_t)I->ld * 8; break;
       case SEC_LASTM: dst = &I->lastM; want = (int64_t)I->ld * 8; break;
@@ -815,6 +836,21 @@ int radb200_intrc_matrix(int64_t handle, int dtype, void *out)
     RB_CUDA(cudaMemcpy2D(out, I->n3 * es, I->N64.p, I->ld * es, I->n3 * es, I->n3, cudaMemcpyDeviceToHost));
   } else if (dtype == 0 && I->N32.p) {
     RB_CUDA(cudaMemcpy2D(out, I->n3 * es, I->N32.p, I->ld * es, I->n3 * es, I->n3, cudaMemcpyDeviceToHost));
+  } else if (dtype == 1 && I->near_nnz > 0) {
+    // mixed storage: FP32 blocks plus the FP64 residue of the near ones
+    const size_t n3 = (size_t)I->n3;
+    std::vector<float> tmp(n3 * n3);
+    RB_CUDA(cudaMemcpy2D(tmp.data(), n3 * 4, I->N32.p, I->ld * 4, n3 * 4, n3, cudaMemcpyDeviceToHost));
+    double *o = (double *)out;
+    for (size_t k = 0; k < n3 * n3; k++) o[k] = tmp[k];
+    std::vector<double> D((size_t)I->near_nnz * 9);
+    RB_CUDA(cudaMemcpy(D.data(), I->near_D.p, D.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < I->n; i++)
+      for (int k = I->h_near_ptr[i]; k < I->h_near_ptr[i + 1]; k++) {
+        const int j = I->h_near_col[k];
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++) o[(3 * (size_t)i + a) * n3 + 3 * j + b] += D[9 * (size_t)k + 3 * a + b];
+      }
   } else {
     // convert on the host from whatever is stored
     size_t nn = (size_t)I->n3 * I->n3;

@@ -124,6 +124,19 @@ struct DevGeom {
   GeomView view(int fast = 0) const;
 };
 
+// ---- near blocks of mixed storage ------------------------------------------
+// With RADB200_STORE_MIXED every block is stored in FP32 and the pairs within
+// the near range additionally keep their FP64 residue D = N(FP64) - N32, in
+// CSR by observer element (ptr, col, D [nnz][9]) and indexed by source element
+// for the transposed product (tptr, tidx: entry numbers grouped by column).
+struct NearView {
+  const int *ptr = nullptr;
+  const int *col = nullptr;
+  const double *D = nullptr;
+  const int *tptr = nullptr;
+  const int *tidx = nullptr;
+};
+
 // ---- interaction state -------------------------------------------------------
 struct Intrc {
   int n = 0;        // elements
@@ -135,6 +148,19 @@ struct Intrc {
   DevGeom geom;     // relaxable elements (object frames, images)
   DBuf elem_src, obs, rowT;           // [2n] int, [3n] obs points, [9n] s*Minv of main image
   DBuf N32, N64;                      // [n3 x ld]
+  DBuf near_ptr, near_col, near_D, near_tptr, near_tidx;  // mixed storage: FP64 residue of near pairs
+  int64_t near_nnz = 0;
+  double near_factor = 0.0;           // near range: centre distance <= factor * (r_i + r_j)
+  std::vector<int> h_near_ptr, h_near_col;
+  NearView near() const
+  {
+    NearView v;
+    if (near_nnz > 0) {
+      v.ptr = near_ptr.as<int>(); v.col = near_col.as<int>(); v.D = near_D.as<double>();
+      v.tptr = near_tptr.as<int>(); v.tidx = near_tidx.as<int>();
+    }
+    return v;
+  }
   DBuf hext;                          // [ld]
   DBuf mat_kind, mat, mh;             // materials
   std::vector<int> h_mat_kind;
@@ -221,6 +247,14 @@ int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what,
 int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int n,
                     int ld, float *N32, double *N64, cudaStream_t st);
 int launch_rowtrans_vec(const double *rowT, const double *in, double *out, int n, cudaStream_t st);
+// near lists of mixed storage from the element geometry (host, near.cu);
+// obs: [3n] element centres (main images)
+int build_near(Intrc &I, const RadB200Geom *elems, const RadB200Relax *r, const double *obs);
+// FP64 residue of the near pairs: D[k] = block(row[k], col[k]) - N32 (assemble.cu)
+int launch_assemble_near(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int ld,
+                         const float *N32, const int *row, const int *col, int64_t nnz, double *D, cudaStream_t st);
+// out[j] += sum over near entries (i, j) of D_ij^T x_i (near.cu)
+int launch_near_t(const Intrc &I, const double *x, double *out, cudaStream_t st);
 // electron trajectories, one CTA each (field.cu); prec NULL: one RK4 step per
 // tabulation interval, else step-doubling control with these [4] accuracies
 int launch_trajectories(const GeomView &g, double energy_gev, const double *d_init, int n_traj, double y0, double y1,

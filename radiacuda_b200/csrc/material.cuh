@@ -4,7 +4,11 @@
 //       radTLinearAnisotropMaterial radmater.h:164-303, radTLinearIsotropMaterial :328-362
 //   saturating isotropic formula:       |M| = sum ms_i tanh(ksi_i |H| / ms_i), M || H
 //       radTNonlinearIsotropMaterial radmater.h:417-600, radmater.cpp:72-306
-// Record layout: RADB200_MAT_STRIDE doubles, see include/radb200.h.
+//   saturating isotropic table:         |M|(|H|) by cubic Hermite pieces between
+//       the points (H_k, M_k) with the table's derivatives dM/dH_k at the nodes,
+//       M || H (the same class with gArrayHM, radmater.cpp:618-710)
+// Record layout: RADB200_MAT_STRIDE doubles, see include/radb200.h; the
+// tables of all elements are rows (H, M, dM/dH) of one array mh.
 #pragma once
 #include "formulas.cuh"
 
@@ -41,25 +45,63 @@ __device__ __forceinline__ double tanh_ksi0(const double *m)
   return k;
 }
 
-// M(H) for element material (kind, m)
-__device__ __forceinline__ V3<double> mat_M(int kind, const double *m, V3<double> H)
+// Tabulated law at |H| = h: m[0] first row of the element's table in mh,
+// m[1] its rows.  Below the first point the first M (derivative: the first
+// node's); above the last point M continues along the last node's slope for
+// M(H) (AbsMvsAbsH_Interpol, radmater.cpp:619-646) while the pair used for
+// dM/dH stops there with zero slope (AbsMvsAbsH_FuncAndDer_Interpol,
+// :678-710); in between the cubic with the end values and slopes of the piece
+// (CubPln, radmater.h:631-639).
+__device__ __forceinline__ void table_law(const double *__restrict__ mh, const double *m, double h, bool for_der,
+                                          double &f, double &df)
+{
+  const int L = (int)m[1];
+  const double *T = mh + 3 * (size_t)m[0];
+  int k = 0;
+  while (k < L && T[3 * k] <= h) k++;
+  k--;  // last node at or below h
+  if (k < 0) { f = T[1]; df = T[2]; return; }
+  if (k >= L - 1) {
+    const double *t = T + 3 * (L - 1);
+    if (for_der) { f = t[1]; df = 0.0; }
+    else { f = t[1] + (h - t[0]) * t[2]; df = t[2]; }
+    return;
+  }
+  const double *t = T + 3 * k;
+  const double step = t[3] - t[0], is = 1.0 / step, sl = (t[4] - t[1]) * is;
+  const double a0 = t[1], a1 = t[2], a2 = (3.0 * sl - 2.0 * t[2] - t[5]) * is, a3 = (-2.0 * sl + t[2] + t[5]) * is * is;
+  const double x = h - t[0];
+  f = a0 + x * (a1 + x * (a2 + x * a3));
+  df = a1 + x * (2.0 * a2 + x * 3.0 * a3);
+}
+
+// |M| and |M| / |H| of a saturating law at |H| = h > 0
+__device__ __forceinline__ double sat_abs_m(int kind, const double *m, const double *__restrict__ mh, double h)
+{
+  double f, df;
+  if (kind == RADB200_MAT_TABLE) table_law(mh, m, h, false, f, df);
+  else tanh_law(m, h, f, df);
+  return f;
+}
+
+// M(H) for element material (kind, m); mh: the table rows (table laws only)
+__device__ __forceinline__ V3<double> mat_M(int kind, const double *m, V3<double> H, const double *__restrict__ mh)
 {
   if (kind == RADB200_MAT_LINEAR)
     return mk3<double>(m[0] * H.x + m[1] * H.y + m[2] * H.z + m[9], m[3] * H.x + m[4] * H.y + m[5] * H.z + m[10],
                        m[6] * H.x + m[7] * H.y + m[8] * H.z + m[11]);
   double h = sqrt(H.x * H.x + H.y * H.y + H.z * H.z);
   double ksi;
-  if (h <= 1e-10) ksi = tanh_ksi0(m);
-  else {
-    double f, df;
-    tanh_law(m, h, f, df);
-    ksi = f / h;
-  }
+  if (kind == RADB200_MAT_TABLE) {
+    if (h == 0.0) return mk3<double>(m[9], m[10], m[11]);
+    ksi = sat_abs_m(kind, m, mh, h) / h;
+  } else if (h <= 1e-10) ksi = tanh_ksi0(m);
+  else ksi = sat_abs_m(kind, m, mh, h) / h;
   return mk3<double>(ksi * H.x + m[9], ksi * H.y + m[10], ksi * H.z + m[11]);
 }
 
-// dM/dH at H (radmater.cpp:206-277; linear: chi tensor)
-__device__ __forceinline__ void mat_D(int kind, const double *m, V3<double> H, double *D)
+// dM/dH at H (radmater.cpp:206-306; linear: chi tensor)
+__device__ __forceinline__ void mat_D(int kind, const double *m, V3<double> H, double *D, const double *__restrict__ mh)
 {
   if (kind == RADB200_MAT_LINEAR) {
     for (int k = 0; k < 9; k++) D[k] = m[k];
@@ -67,7 +109,10 @@ __device__ __forceinline__ void mat_D(int kind, const double *m, V3<double> H, d
   }
   double h0 = sqrt(H.x * H.x + H.y * H.y + H.z * H.z);
   double f, df;
-  tanh_law(m, h0, f, df);
+  if (kind == RADB200_MAT_TABLE) {
+    if (h0 < 1e-10) { f = 0.0; df = mh[3 * (size_t)m[0] + 2]; }
+    else table_law(mh, m, h0, true, f, df);
+  } else tanh_law(m, h0, f, df);
   if (h0 < 1e-10) {
     for (int k = 0; k < 9; k++) D[k] = (k % 4 == 0) ? df : 0.0;
     return;
@@ -84,9 +129,9 @@ __device__ __forceinline__ void mat_D(int kind, const double *m, V3<double> H, d
 
 // FindNewH: solve H = Hq + Q_ii M(H) for the element's own field.
 // Linear: H = (I - Q chi)^-1 (Hq + Q Mr)  (radmater.h:223-231).
-// Nonlinear: damped secant on |H| with at most 15 passes (radmater.cpp:72-164).
+// Saturating: damped secant on |H| with at most 15 passes (radmater.cpp:72-164).
 __device__ __forceinline__ V3<double> find_new_h(int kind, const double *m, const double *Q, V3<double> Hq,
-                                                 V3<double> H0, double prec_e2)
+                                                 V3<double> H0, double prec_e2, const double *__restrict__ mh)
 {
   double A[9], Ai[9];
   if (kind == RADB200_MAT_LINEAR) {
@@ -104,9 +149,9 @@ __device__ __forceinline__ V3<double> find_new_h(int kind, const double *m, cons
   double ah = sqrt(H0.x * H0.x + H0.y * H0.y + H0.z * H0.z);
   V3<double> H = H0;
   for (int it = 0; it < 15; it++) {
-    double f = 0.0, df, ksi;
-    if (ah <= 1e-10) { ksi = tanh_ksi0(m); f = 0.0; }
-    else { tanh_law(m, ah, f, df); ksi = f / ah; }
+    double f = 0.0, ksi;
+    if (ah <= 1e-10) { ksi = (kind == RADB200_MAT_TABLE) ? mh[3 * (size_t)m[0] + 2] : tanh_ksi0(m); f = 0.0; }
+    else { f = sat_abs_m(kind, m, mh, ah); ksi = f / ah; }
     for (int k = 0; k < 9; k++) A[k] = ((k % 4) == 0 ? 1.0 : 0.0) - ksi * Q[k];
     inv3x3(A, Ai);
     H = mk3<double>(Ai[0] * Hq.x + Ai[1] * Hq.y + Ai[2] * Hq.z, Ai[3] * Hq.x + Ai[4] * Hq.y + Ai[5] * Hq.z,

@@ -91,15 +91,42 @@ __device__ __forceinline__ void rows3_dot(const MT *__restrict__ N, int ld, int 
 
 constexpr int RLX_WARPS = 8;
 
+// Adds the FP64 near residue of element e's rows (mixed storage) to h,
+// warp-wide: lanes take the near entries in turn, then a butterfly reduce.
+__device__ __forceinline__ void near_rows3(const NearView &nv, int e, const double *__restrict__ x, double &h0,
+                                           double &h1, double &h2)
+{
+  const int lane = threadIdx.x & 31;
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int k = nv.ptr[e] + lane; k < nv.ptr[e + 1]; k += 32) {
+    const int j = nv.col[k];
+    const double *d = nv.D + 9 * (size_t)k;
+    const double x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
+    a0 += d[0] * x0 + d[1] * x1 + d[2] * x2;
+    a1 += d[3] * x0 + d[4] * x1 + d[5] * x2;
+    a2 += d[6] * x0 + d[7] * x1 + d[8] * x2;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+  }
+  h0 += a0;
+  h1 += a1;
+  h2 += a2;
+}
+
 // One Jacobi proposal: H = N M + H_ext; per element H' = FindNewH(H - Q_ii M),
 // M' = M(H'); writes Mp, Hn, F = M' - M and per-CTA partial sums of |F|^2.
 template <typename MT>
 __global__ void __launch_bounds__(32 * RLX_WARPS) jacobi_kernel(const MT *__restrict__ N, int ld, int n,
                                                                const double *__restrict__ M, const double *__restrict__ hext,
                                                                const int *__restrict__ kind, const double *__restrict__ mat,
+                                                               const double *__restrict__ mh,
                                                                double prec_e2, double *__restrict__ Hn,
                                                                double *__restrict__ Mp, double *__restrict__ F,
-                                                               double *__restrict__ part)
+                                                               double *__restrict__ part, NearView nv)
 {
   __shared__ double ssq[RLX_WARPS];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -108,6 +135,7 @@ __global__ void __launch_bounds__(32 * RLX_WARPS) jacobi_kernel(const MT *__rest
   if (e < n) {
     double h0, h1, h2;
     rows3_dot<MT, 2>(N, ld, e, M, h0, h1, h2);
+    if (nv.ptr) near_rows3(nv, e, M, h0, h1, h2);
     if (lane == 0) {
       double Q[9];
       const MT *d = N + (size_t)(3 * e) * ld + 3 * e;
@@ -120,8 +148,8 @@ __global__ void __launch_bounds__(32 * RLX_WARPS) jacobi_kernel(const MT *__rest
       int k = kind[e];
       const double *mr = mat + (size_t)e * RADB200_MAT_STRIDE;
       V3<double> H0 = mk3<double>(Hn[3 * e], Hn[3 * e + 1], Hn[3 * e + 2]);
-      V3<double> H = find_new_h(k, mr, Q, Hq, H0, prec_e2);
-      V3<double> Mn = mat_M(k, mr, H);
+      V3<double> H = find_new_h(k, mr, Q, Hq, H0, prec_e2, mh);
+      V3<double> Mn = mat_M(k, mr, H, mh);
       Hn[3 * e] = H.x; Hn[3 * e + 1] = H.y; Hn[3 * e + 2] = H.z;
       Mp[3 * e] = Mn.x; Mp[3 * e + 1] = Mn.y; Mp[3 * e + 2] = Mn.z;
       double f0 = Mn.x - m0, f1 = Mn.y - m1, f2 = Mn.z - m2;
@@ -138,17 +166,19 @@ __global__ void __launch_bounds__(32 * RLX_WARPS) jacobi_kernel(const MT *__rest
   }
 }
 
-// y = N x + b (plain matvec, warp per element, used by NK / refinement / adjoint)
+// y = N x + b (plain matvec, warp per element, used by NK / refinement / adjoint);
+// with nv.ptr set, N is FP32 and the near blocks get their FP64 residue
 template <typename MT>
 __global__ void __launch_bounds__(32 * RLX_WARPS) matvec_kernel(const MT *__restrict__ N, int ld, int n,
                                                                const double *__restrict__ x, const double *__restrict__ b,
-                                                               double alpha, double *__restrict__ y)
+                                                               double alpha, double *__restrict__ y, NearView nv)
 {
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int e = blockIdx.x * RLX_WARPS + warp;
   if (e >= n) return;
   double h0, h1, h2;
   rows3_dot<MT, 2>(N, ld, e, x, h0, h1, h2);
+  if (nv.ptr) near_rows3(nv, e, x, h0, h1, h2);
   if (lane == 0) {
     double b0 = b ? b[3 * e] : 0.0, b1 = b ? b[3 * e + 1] : 0.0, b2 = b ? b[3 * e + 2] : 0.0;
     y[3 * e] = alpha * h0 + b0;
@@ -269,9 +299,9 @@ static int jacobi_step(Intrc &I, Ctx &c, const MT *N, double prec_e2, double *mi
   RB_TRY(c.part.alloc((size_t)nb * sizeof(double)));
   RB_TRY(c.scal.alloc(64 * sizeof(double)));
   jacobi_kernel<MT><<<nb, 32 * RLX_WARPS, 0, c.st>>>(N, I.ld, I.n, I.M.as<double>(), I.hext.as<double>(),
-                                                      I.mat_kind.as<int>(), I.mat.as<double>(), prec_e2,
+                                                      I.mat_kind.as<int>(), I.mat.as<double>(), I.mh.as<double>(), prec_e2,
                                                       I.H.as<double>(), I.Mp.as<double>(), I.F.as<double>(),
-                                                      c.part.as<double>());
+                                                      c.part.as<double>(), I.near());
   RB_TRY(check_launch("jacobi_kernel"));
   sum_kernel<<<1, 256, 0, c.st>>>(c.part.as<double>(), nb, c.scal.as<double>());
   RB_TRY(check_launch("sum_kernel"));
@@ -285,16 +315,16 @@ static int jacobi_step(Intrc &I, Ctx &c, const MT *N, double prec_e2, double *mi
 int run_matvec(Intrc &I, const double *x, const double *b, double alpha, double *y, cudaStream_t st)
 {
   int nb = grid_elems(I.n);
-  if (I.N64.p) matvec_kernel<double><<<nb, 32 * RLX_WARPS, 0, st>>>(I.N64.as<double>(), I.ld, I.n, x, b, alpha, y);
-  else matvec_kernel<float><<<nb, 32 * RLX_WARPS, 0, st>>>(I.N32.as<float>(), I.ld, I.n, x, b, alpha, y);
+  if (I.N64.p) matvec_kernel<double><<<nb, 32 * RLX_WARPS, 0, st>>>(I.N64.as<double>(), I.ld, I.n, x, b, alpha, y, NearView());
+  else matvec_kernel<float><<<nb, 32 * RLX_WARPS, 0, st>>>(I.N32.as<float>(), I.ld, I.n, x, b, alpha, y, I.near());
   return check_launch("matvec_kernel");
 }
 
 int run_matvec_f32(Intrc &I, const double *x, const double *b, double alpha, double *y, cudaStream_t st)
 {
   int nb = grid_elems(I.n);
-  if (I.N32.p) matvec_kernel<float><<<nb, 32 * RLX_WARPS, 0, st>>>(I.N32.as<float>(), I.ld, I.n, x, b, alpha, y);
-  else matvec_kernel<double><<<nb, 32 * RLX_WARPS, 0, st>>>(I.N64.as<double>(), I.ld, I.n, x, b, alpha, y);
+  if (I.N32.p) matvec_kernel<float><<<nb, 32 * RLX_WARPS, 0, st>>>(I.N32.as<float>(), I.ld, I.n, x, b, alpha, y, NearView());
+  else matvec_kernel<double><<<nb, 32 * RLX_WARPS, 0, st>>>(I.N64.as<double>(), I.ld, I.n, x, b, alpha, y, NearView());
   return check_launch("matvec_kernel");
 }
 
@@ -477,7 +507,8 @@ int relax_jacobi(Intrc &I, double prec, int max_iter, double omega0, double *sta
 
 template <typename MT>
 __global__ void newton_B_kernel(const MT *__restrict__ N, int ld, int n, const double *__restrict__ H,
-                                const int *__restrict__ kind, const double *__restrict__ mat, double *__restrict__ B)
+                                const int *__restrict__ kind, const double *__restrict__ mat,
+                                const double *__restrict__ mh, double *__restrict__ B)
 {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
@@ -485,7 +516,7 @@ __global__ void newton_B_kernel(const MT *__restrict__ N, int ld, int n, const d
   const MT *d = N + (size_t)(3 * e) * ld + 3 * e;
   for (int a = 0; a < 3; a++)
     for (int b = 0; b < 3; b++) Q[3 * a + b] = (double)d[(size_t)a * ld + b];
-  mat_D(kind[e], mat + (size_t)e * RADB200_MAT_STRIDE, mk3<double>(H[3 * e], H[3 * e + 1], H[3 * e + 2]), D);
+  mat_D(kind[e], mat + (size_t)e * RADB200_MAT_STRIDE, mk3<double>(H[3 * e], H[3 * e + 1], H[3 * e + 2]), D, mh);
   for (int a = 0; a < 3; a++)
     for (int b = 0; b < 3; b++)
       A[3 * a + b] = (a == b ? 1.0 : 0.0) - (Q[3 * a] * D[b] + Q[3 * a + 1] * D[3 + b] + Q[3 * a + 2] * D[6 + b]);
@@ -548,8 +579,8 @@ int relax_newton(Intrc &I, double prec, int max_iter, double *status)
   while (misfit > prec && matvecs < max_iter && newton < 100) {
     newton++;
     int nb = (n + 127) / 128;
-    if (I.N64.p) newton_B_kernel<double><<<nb, 128>>>(I.N64.as<double>(), ld, n, I.H.as<double>(), I.mat_kind.as<int>(), I.mat.as<double>(), B);
-    else newton_B_kernel<float><<<nb, 128>>>(I.N32.as<float>(), ld, n, I.H.as<double>(), I.mat_kind.as<int>(), I.mat.as<double>(), B);
+    if (I.N64.p) newton_B_kernel<double><<<nb, 128>>>(I.N64.as<double>(), ld, n, I.H.as<double>(), I.mat_kind.as<int>(), I.mat.as<double>(), I.mh.as<double>(), B);
+    else newton_B_kernel<float><<<nb, 128>>>(I.N32.as<float>(), ld, n, I.H.as<double>(), I.mat_kind.as<int>(), I.mat.as<double>(), I.mh.as<double>(), B);
     RB_TRY(check_launch("newton_B_kernel"));
     RB_CUDA(cudaMemcpy(R0, I.F.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice));
     RB_CUDA(cudaMemcpy(M0, M, n3 * sizeof(double), cudaMemcpyDeviceToDevice));

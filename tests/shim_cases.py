@@ -183,6 +183,43 @@ def case_direct_solve(rad):
     return out
 
 
+# A soft-iron curve |M|(mu0 |H|) in T, tabulated (the shape of a low-carbon
+# steel: steep start, knee near 1.4 T, saturation near 2.1 T)
+IRON_TABLE = [[0.0, 0.0], [1e-4, 0.28], [3e-4, 0.72], [6e-4, 1.05], [1e-3, 1.25], [2e-3, 1.45],
+              [4e-3, 1.58], [8e-3, 1.70], [2e-2, 1.83], [5e-2, 1.93], [0.1, 2.0], [0.3, 2.07],
+              [1.0, 2.12], [3.0, 2.15]]
+
+
+def _table_yoke(rad):
+    rad.UtiDelAll()
+    rad.FldLenRndSw("off")
+    pieces = []
+    for c, d, k in (([15.0, 0.0, 30.0], [30.0, 40.0, 20.0], [3, 2, 2]), ([45.0, 0.0, 47.5], [90.0, 40.0, 15.0], [4, 2, 1]),
+                    ([80.0, 0.0, 20.37], [20.0, 40.0, 40.0], [2, 2, 3])):
+        b = rad.ObjRecMag(c, d, [0, 0, 0])
+        rad.ObjDivMag(b, k)
+        pieces.append(b)
+    yoke = rad.ObjCnt(pieces)
+    rad.MatApl(yoke, rad.MatSatIsoTab(IRON_TABLE))
+    rad.TrfZerPerp(yoke, [0, 0, 0], [1, 0, 0])
+    rad.TrfZerPara(yoke, [0, 0, 0], [0, 0, 1])
+    coil = rad.ObjRaceTrk([0, 0, 30], [2, 14], [40, 50], 16, 6, 25.0, "man", "z")
+    h = rad.ObjCnt([yoke, coil])
+    P = MD.iron_dipole_points(5, 30.0)
+    return h, P.tolist()
+
+
+def case_table_m9(rad):
+    """Tabulated M(H) (MatSatIsoTab) relaxed by method 9 on the device."""
+    h, P = _table_yoke(rad)
+    return _solve_pair(rad, h, P, 9, 1e-10, 5000)
+
+
+def case_table_m11(rad):
+    h, P = _table_yoke(rad)
+    return _solve_pair(rad, h, P, 11, 1e-10, 5000)
+
+
 def case_break_policy(rad):
     """UtiGpuFallback('break'): an assembly the GPU cannot take raises
     Radia::Error602 instead of falling back (used where no device exists)."""

@@ -23,7 +23,8 @@ pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = ["magnet_array", "mixed_sym_m9", "mixed_sym_m11", "iron_dipole_m11", "symmetry_mix",
-         "single_precision_field", "srcobj", "cpu_assembly_gpu_relax", "material_change", "direct_solve"]
+         "single_precision_field", "srcobj", "cpu_assembly_gpu_relax", "material_change", "direct_solve",
+         "table_m9", "table_m11"]
 
 
 @pytest.fixture(scope="module")
@@ -61,7 +62,7 @@ def test_magnet_array_anisotropic_relaxes_on_the_gpu(shim):
     _check_pair(shim["magnet_array"], 5e-6)
 
 
-@pytest.mark.parametrize("case", ["mixed_sym_m9", "mixed_sym_m11", "iron_dipole_m11"])
+@pytest.mark.parametrize("case", ["mixed_sym_m9", "mixed_sym_m11", "iron_dipole_m11", "table_m9", "table_m11"])
 def test_saturating_models_methods_9_and_11(shim, case):
     _check_pair(shim[case], 5e-5)
 

@@ -69,9 +69,9 @@ def test_field_noalloc_matches_allocating_entry_point(cuda, rad):
     arrs = model.pack_sources(rad._objs, h, tuple(rad._rand))
     g, keep = _device_geom(arrs, torch, cuda)
     P = rng.uniform(-90, 90, size=(3000, 3))
+    # points inside the magnets too, so the M path (what == 2) sees both sides
+    P[:200] = _inside_points(arrs, 200, rng)
     d_pts = torch.from_numpy(P).to(cuda)
-    # sample points inside the magnets too, so the M path (what == 2) sees both sides
-    P[:200] = [c for c in _inside_points(arrs, 200, rng)]
     for what in (0, 1, 2):
         ref = _native.field(arrs, P, what, 0)
         for call in range(2):
