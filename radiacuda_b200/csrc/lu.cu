@@ -391,7 +391,19 @@ static double g_upd_bytes = 0.0, g_upd_flops = 0.0;
 // forward substitution over its 128-row sub-blocks, and the trailing matrix
 // receives ONE update with K = LU_OUTER: the C traffic of the dominant GEMM
 // drops by LU_OUTER / 128 against 128-wide steps.
-constexpr int LU_OUTER = 512;
+constexpr int LU_OUTER_DEFAULT = 512;
+// the outer panel width: LU_OUTER_DEFAULT, or RADB200_LU_OUTER (a multiple of
+// 128 from 256 to 2048) for tuning
+static int lu_outer()
+{
+  static int w = 0;
+  if (!w) {
+    const char *e = getenv("RADB200_LU_OUTER");
+    int v = e ? atoi(e) : LU_OUTER_DEFAULT;
+    w = (v >= 256 && v <= 2048 && v % LU_NB == 0) ? v : LU_OUTER_DEFAULT;
+  }
+  return w;
+}
 
 // One-panel look-ahead: the trailing update of outer step k is split into the
 // columns of panel k+1 (on the main stream, first) and the rest (on a side
@@ -477,6 +489,7 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
     }
     return 0;
   };
+  const int LU_OUTER = lu_outer();
   for (int K0 = 0; K0 < n3; K0 += LU_OUTER) {
     const int NBe = std::min(LU_OUTER, n3 - K0);
     const int pend = K0 + NBe;  // end of the panel's columns

@@ -10,7 +10,8 @@ seeded models of tests/models.py:
   c1  432 anisotropic blocks, Solve(prec 1e-10, method 4), B at the 10,000
       grid points 5 mm above the array;
   c2  the 4,000-block saturating dipole (2 mirror planes, racetrack),
-      Solve(prec 1e-9, method 4), B at a seeded 10,000-point subsample of the
+      Solve(prec 1e-7, method 4: the reference's FP32 matrix puts the floor
+      of its misfit near there), B at a seeded 10,000-point subsample of the
       100^3 gap grid;
   c3  a 3,000-tetrahedron mesh of the 20k model's construction at chi = 1000:
       the FP64 interaction matrix built column by column from the reference's
@@ -21,7 +22,7 @@ seeded models of tests/models.py:
       oracle at chi = 1000);
   c4  the 640-block planar undulator, Solve(prec 1e-10), B at 4,000 axis points;
   c5  the 6,080-element hybrid undulator (saturating poles, a mirror plane),
-      Solve(prec 1e-9), B at a seeded 10,000-point subsample of its 1e5 points.
+      Solve(prec 1e-7), B at a seeded 10,000-point subsample of its 1e5 points.
 
 Field evaluations and the matrix columns of c3 are split over worker
 processes forked after the model is built and solved.
@@ -83,7 +84,7 @@ def c1(out):
 def c2(out):
     m = MD.iron_dipole(R, n_target=4000)
     idx, P = subsample(MD.iron_dipole_points(100), 10000, 22)
-    out["c2_status"] = solve(m, 1e-9, 20000)
+    out["c2_status"] = solve(m, 1e-7, 6000)
     out["c2_idx"] = idx
     out["c2_b"] = field_parallel(m, "b", P)
 
@@ -149,7 +150,7 @@ def c4(out):
 def c5(out):
     m = MD.hybrid_undulator(R)[0]
     idx, P = subsample(MD.hybrid_points(), 10000, 55)
-    out["c5_status"] = solve(m, 1e-9, 20000)
+    out["c5_status"] = solve(m, 1e-7, 6000)
     out["c5_idx"] = idx
     out["c5_b"] = field_parallel(m, "b", P)
 

@@ -53,6 +53,7 @@ def test_c2_iron_dipole_4000_four_images_racetrack(cuda, rad, gold):
     P = MD.iron_dipole_points(100)[gold["c2_idx"]]
     B = _relaxed_field(rad, h, P, 1e-9, 20000)
     e = errs(B, gold["c2_b"])
+    assert gold["c2_status"][0] < 2e-7
     assert e[0] < 5e-5 and e[1] < 5e-5, e
 
 
@@ -68,6 +69,7 @@ def test_c5_hybrid_undulator_6080(cuda, rad, gold):
     P = MD.hybrid_points()[gold["c5_idx"]]
     B = _relaxed_field(rad, h, P, 1e-9, 20000)
     e = errs(B, gold["c5_b"])
+    assert gold["c5_status"][0] < 2e-7
     assert e[0] < 5e-5 and e[1] < 5e-5, e
 
 
