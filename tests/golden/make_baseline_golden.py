@@ -108,7 +108,7 @@ def _columns(js):
 
 def c3(out, n_tets=3000, ncell=8, chi=1000.0, n_pts=2000):
     whole, body = MD.tet_mesh(R, ncell=ncell, n_tets=n_tets, chi=chi)
-    V = MD.tet_mesh_vertices(ncell, n_tets)
+    V = np.asarray(MD.tet_mesh_vertices(ncell, n_tets))
     elems = R.ObjCntStuf(body)
     assert len(elems) == n_tets
     cen = V.mean(axis=1)
@@ -159,11 +159,11 @@ def main(names):
     out = dict(np.load(OUT)) if os.path.exists(OUT) else {}
     for nm in names:
         t = time.time()
-        print(nm)
+        print(nm, flush=True)
         globals()[nm](out)
-        print(f"  {nm} done in {time.time() - t:.1f} s")
-    np.savez_compressed(OUT, **out)
-    print("wrote", OUT)
+        print(f"  {nm} done in {time.time() - t:.1f} s", flush=True)
+        np.savez_compressed(OUT, **out)
+        print("wrote", OUT, flush=True)
 
 
 if __name__ == "__main__":
