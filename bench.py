@@ -253,7 +253,7 @@ def run_ours(args, rank, world):
     if not e2e:
         e2e = [float("nan")]
 
-    # roofline of the LU trailing update (TF32 tcgen05 GEMM, K = 512): its
+    # roofline of the LU trailing update (TF32 tcgen05 GEMM, K = 768): its
     # flops (2 m^2 K per launch) over the event-timed launch durations,
     # against the dense TF32 rate (half the measured bf16 rate); the HBM side
     # (C read + written, panels once) beside it
@@ -266,7 +266,7 @@ def run_ours(args, rank, world):
     upd_tflops = upd_f.value / max(upd_s.value, 1e-30) / 1e12
     upd_gbs = upd_b.value / max(upd_s.value, 1e-30) / 1e9
     upd_bytes_per_launch = upd_b.value / max(upd_n.value, 1)
-    roof_upd = {"kernel": "tc_update_kernel (LU trailing update A22 -= L21 U12, K = 512)", "bound": "tensor",
+    roof_upd = {"kernel": "tc_update_tma_kernel (LU trailing update A22 -= L21 U12, K = 768)", "bound": "tensor",
                 "achieved": round(upd_tflops, 1), "peak": round(tf32_peak, 1), "unit": "TFLOP/s",
                 "frac": round(upd_tflops / tf32_peak, 4),
                 "peak_source": ("measured sustained bf16 dense / 2 (TF32 runs at half the bf16 rate)" if bf16 else

@@ -362,6 +362,11 @@ int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs)
     RB_TRY(tetidx.upload(h.tetidx.data(), h.tetidx.size() * sizeof(int)));
     RB_TRY(tetrec.upload(h.tetrec.data(), h.tetrec.size() * sizeof(double)));
     all_tets = std::all_of(h.tetidx.begin(), h.tetidx.end(), [](int t) { return t >= 0; }) ? 1 : 0;
+    m_tiles = m_groups = 0;
+    // field geometry of an all-tetrahedron model: the mesh form (unique edges and faces)
+    if (all_tets && !tensor_coeffs) RB_TRY(build_mesh(G, h.tetidx, h.tetrec, *this));
+  } else {
+    m_tiles = m_groups = 0;
   }
   RB_TRY(trf.upload(G->trf, (size_t)G->n_trf * RADB200_TRF_STRIDE * sizeof(double)));
   RB_TRY(rec.upload(G->rec, (size_t)G->n_rec * RADB200_REC_STRIDE * sizeof(double)));
@@ -411,6 +416,15 @@ GeomView DevGeom::view(int fast) const
   v.tetidx = tetidx.as<int>();
   v.tetrec = tetrec.as<double>();
   v.all_tets = all_tets;
+  v.mesh.n_tiles = m_tiles;
+  v.mesh.tile = m_tile.as<int4>();
+  v.mesh.mv = m_v.as<double>();
+  v.mesh.me = m_e.as<double>();
+  v.mesh.mf = m_f.as<double>();
+  v.mesh.n_groups = m_groups;
+  v.mesh.group = m_group.as<int4>();
+  v.mesh.gbox = m_gbox.as<double>();
+  v.mesh.gtet = m_gtet.as<int>();
   return v;
 }
 

@@ -195,7 +195,9 @@ __device__ __forceinline__ void tet_unit(const double *su, V3<double> P, int wha
   acc[2] += F[6] * f.x + F[7] * f.y + F[8] * f.z;
 }
 
-template <typename T, int PPT>
+// PPT points per thread; TPI tetrahedra per iteration of the unit loop (two
+// independent evaluation chains interleave when TPI == 2)
+template <typename T, int PPT, int TPI = 1>
 __global__ void __launch_bounds__(128) field_tet_kernel(GeomView g, const double *__restrict__ pts, int64_t npts, int what,
                                                         double *__restrict__ out, int ub, int ue, int chunk, int accumulate)
 {
@@ -220,9 +222,20 @@ __global__ void __launch_bounds__(128) field_tet_kernel(GeomView g, const double
       su[e] = v;
     }
     __syncthreads();
-    for (int k = 0; k < cnt; k++) {
-      tet_unit<T>(su + k * TET_U, P0, what, a0);
-      if (PPT == 2) tet_unit<T>(su + k * TET_U, P1, what, a1);
+    if (TPI == 2) {
+      int k = 0;
+      for (; k + 1 < cnt; k += 2) {
+        double b0[3] = {0, 0, 0};
+        tet_unit<T>(su + k * TET_U, P0, what, a0);
+        tet_unit<T>(su + (k + 1) * TET_U, P0, what, b0);
+        a0[0] += b0[0]; a0[1] += b0[1]; a0[2] += b0[2];
+      }
+      if (k < cnt) tet_unit<T>(su + k * TET_U, P0, what, a0);
+    } else {
+      for (int k = 0; k < cnt; k++) {
+        tet_unit<T>(su + k * TET_U, P0, what, a0);
+        if (PPT == 2) tet_unit<T>(su + k * TET_U, P1, what, a1);
+      }
     }
   }
   if (i0 < npts) {
@@ -237,7 +250,7 @@ __global__ void __launch_bounds__(128) field_tet_kernel(GeomView g, const double
   }
 }
 
-template <typename T, int PPT>
+template <typename T, int PPT, int TPI = 1>
 static int launch_tet_ppt(const GeomView &g, const double *d_pts, int64_t npts, int what, double *d_out, int ub, int ue,
                           int accumulate, DBuf &scratch, cudaStream_t st)
 {
@@ -252,11 +265,11 @@ static int launch_tet_ppt(const GeomView &g, const double *d_pts, int64_t npts, 
   nchunk = (nu + chunk - 1) / chunk;
   dim3 grid((unsigned)nblk, (unsigned)nchunk);
   if (nchunk == 1) {
-    field_tet_kernel<T, PPT><<<grid, 128, 0, st>>>(g, d_pts, npts, what, d_out, ub, ue, chunk, accumulate);
+    field_tet_kernel<T, PPT, TPI><<<grid, 128, 0, st>>>(g, d_pts, npts, what, d_out, ub, ue, chunk, accumulate);
     return check_launch("field_tet_kernel");
   }
   RB_TRY(scratch.alloc((size_t)nchunk * npts * 3 * sizeof(double)));
-  field_tet_kernel<T, PPT><<<grid, 128, 0, st>>>(g, d_pts, npts, what, scratch.as<double>(), ub, ue, chunk, 0);
+  field_tet_kernel<T, PPT, TPI><<<grid, 128, 0, st>>>(g, d_pts, npts, what, scratch.as<double>(), ub, ue, chunk, 0);
   RB_TRY(check_launch("field_tet_kernel"));
   int64_t n3 = npts * 3;
   chunk_reduce_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(scratch.as<double>(), nchunk, n3, d_out, accumulate);
@@ -272,9 +285,11 @@ static int launch_tet(const GeomView &g, const double *d_pts, int64_t npts, int 
   static int ppt = 0;
   if (!ppt) {
     const char *e = getenv("RADB200_TET_PPT");
-    ppt = (e && atoi(e) == 2) ? 2 : 1;
+    ppt = (e && atoi(e) == 2) ? 2 : (e && atoi(e) == 3) ? 3 : 1;
   }
   if (ppt == 2) return launch_tet_ppt<T, 2>(g, d_pts, npts, what, d_out, ub, ue, accumulate, scratch, st);
+  // RADB200_TET_PPT=3: one point, two tetrahedra interleaved per iteration
+  if (ppt == 3) return launch_tet_ppt<T, 1, 2>(g, d_pts, npts, what, d_out, ub, ue, accumulate, scratch, st);
   return launch_tet_ppt<T, 1>(g, d_pts, npts, what, d_out, ub, ue, accumulate, scratch, st);
 }
 
@@ -306,6 +321,18 @@ static int launch_kind(const GeomView &g, const double *d_pts, int64_t npts, int
   return check_launch("chunk_reduce_kernel");
 }
 
+// RADB200_MESH_FORM=0 evaluates all-tetrahedron models one tetrahedron at a
+// time instead of by their unique edges and faces (A/B comparisons)
+static bool mesh_form_enabled()
+{
+  static int on = -1;
+  if (on < 0) {
+    const char *e = getenv("RADB200_MESH_FORM");
+    on = (e && atoi(e) == 0) ? 0 : 1;
+  }
+  return on == 1;
+}
+
 int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what, int precision, double *d_out,
                  DBuf &scratch, cudaStream_t st)
 {
@@ -323,6 +350,12 @@ int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what,
     int rc;
     if (kind == 0)
       rc = launch_kind<double, UK_REC>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);
+    // the mesh form in FP64 only: with FP32 terms its largest per-point B
+    // error on the 20,000-tetrahedron model was 2.1e-6 against 7.6e-7 for the
+    // tetrahedra one by one, at a 1.25x speed-up (1.42x in FP64)
+    else if (kind == 1 && g.fast && g.all_tets && g.mesh.n_tiles > 0 && what != 2 && precision != 1 &&
+             mesh_form_enabled())
+      rc = launch_mesh_field(g, d_pts, npts, what, precision, d_out, acc, scratch, st);
     else if (kind == 1 && g.fast && g.all_tets)
       rc = (precision == 1) ? launch_tet<float>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st)
                             : launch_tet<double>(g, d_pts, npts, what, d_out, ub, ue, acc, scratch, st);

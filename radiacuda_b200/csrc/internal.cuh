@@ -86,6 +86,32 @@ struct DBuf {
   template <typename T> T *as() const { return (T *)p; }
 };
 
+// ---- tetrahedral meshes by their unique vertices, edges and faces -----------
+// The vertex/edge form sums, per tetrahedron, a logarithm per edge and a
+// solid angle per face.  Tetrahedra of a mesh share vertices, edges and
+// faces, and the sum is linear in the per-edge and per-face coefficients, so
+// the field of all tetrahedra under one image transform is evaluated once per
+// UNIQUE edge (coefficients G summed over the tetrahedra sharing it) and per
+// unique face (A = sum of s a_f, s = +-1 the face's orientation in each
+// tetrahedron against the face's own).  Tiles group spatially close
+// tetrahedra: up to MESH_VT vertices whose distances to the point are
+// computed once per tile, and the edges and faces the tile owns (each unique
+// edge or face belongs to exactly one tile).
+constexpr int MESH_VT = 32, MESH_EMAX = 128, MESH_FMAX = 160;
+constexpr int MESH_E = 6;   // edge record: a, b (tile-local vertices), l, G (3)
+constexpr int MESH_F = 13;  // face record: a, b, c, l_ab, l_ac, l_bc, m (3, unnormalized normal), v_a . m, A (3)
+struct MeshView {
+  int n_tiles = 0;
+  const int4 *tile = nullptr;   // [2 per tile] {first vertex slot, vertices, first edge, edges}, {first face, faces, transform, 0}
+  const double *mv = nullptr;   // tile-local vertices, 3 doubles per slot (object frame of the transform)
+  const double *me = nullptr;   // [edges * MESH_E]
+  const double *mf = nullptr;   // [faces * MESH_F]
+  int n_groups = 0;
+  const int4 *group = nullptr;  // {first entry of gtet, tetrahedra, transform, 0}
+  const double *gbox = nullptr; // [groups * 6] bounding box (lo, hi) in the transform's object frame
+  const int *gtet = nullptr;    // polyhedron index of every tetrahedron of each group
+};
+
 // ---- geometry on the device --------------------------------------------------
 // Kernel-side view (passed by value).  Mirrors RadB200Geom plus a unit table:
 // one unit per (source, image), kinds 0 cuboid, 1 polyhedron, 2 arc, 3 background.
@@ -109,6 +135,7 @@ struct GeomView {
   const double *tetrec;
   int all_tets;       // every polyhedron has a tetrahedron record
   int fast;           // 1: evaluate polyhedra in the vertex/edge form
+  MeshView mesh;      // all-tetrahedron models: unique edges and faces (n_tiles 0: none)
 };
 
 struct DevGeom {
@@ -116,6 +143,8 @@ struct DevGeom {
   // polyhedron topology (vertex/edge form), see TopoView in formulas.cuh
   DBuf tinfo, tinfo2, tv, te, tel, teg, teG, tt, ttm, tfn, tfa;
   DBuf tetidx, tetrec;  // fixed-topology tetrahedron records (tet_fast)
+  DBuf m_tile, m_v, m_e, m_f, m_group, m_gbox, m_gtet;  // mesh form (MeshView)
+  int m_tiles = 0, m_groups = 0;
   int n_units = 0, n_rec = 0, n_poly = 0;
   int ustart[5] = {0, 0, 0, 0, 0};
   int all_tets = 0;
@@ -170,6 +199,7 @@ struct Intrc {
   // LU factors (row-major [n3 x ld]) and solve state
   DBuf LU32, LU64, lu_scratch;
   DBuf LUinv;                         // [2][3N x 128] inverses of the diagonal blocks (L, then U)
+  DBuf tri_sync;                      // counters and flags of the one-launch triangular sweeps
   int lu_tc = 0;                      // the factorization ran on the tensor cores
   int lu_mode = -1;                   // factors valid for this mode (-1 none)
   int lu_of_d = 0;                    // 1: the factors are of I - D N at the converged state of solve lu_solve_id
@@ -247,6 +277,13 @@ int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what,
 int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int n,
                     int ld, float *N32, double *N64, cudaStream_t st);
 int launch_rowtrans_vec(const double *rowT, const double *in, double *out, int n, cudaStream_t st);
+// mesh form of an all-tetrahedron geometry from its tetrahedron records
+// (mesh.cu); tetidx[p] = record of polyhedron p
+int build_mesh(const RadB200Geom *G, const std::vector<int> &tetidx, const std::vector<double> &tetrec, DevGeom &dg);
+// field of the tetrahedra in the mesh form, all units of kind polyhedron
+// (what 0 B, 1 H; mesh.cu)
+int launch_mesh_field(const GeomView &g, const double *d_pts, int64_t npts, int what, int precision, double *d_out,
+                      int accumulate, DBuf &scratch, cudaStream_t st);
 // near lists of mixed storage from the element geometry (host, near.cu);
 // obs: [3n] element centres (main images)
 int build_near(Intrc &I, const RadB200Geom *elems, const RadB200Relax *r, const double *obs);

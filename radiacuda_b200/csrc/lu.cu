@@ -391,7 +391,7 @@ static double g_upd_bytes = 0.0, g_upd_flops = 0.0;
 // forward substitution over its 128-row sub-blocks, and the trailing matrix
 // receives ONE update with K = LU_OUTER: the C traffic of the dominant GEMM
 // drops by LU_OUTER / 128 against 128-wide steps.
-constexpr int LU_OUTER_DEFAULT = 512;
+constexpr int LU_OUTER_DEFAULT = 768;  // swept 512, 768, 1024 on the 60,000^2 factorization
 // the outer panel width: LU_OUTER_DEFAULT, or RADB200_LU_OUTER (a multiple of
 // 128 from 256 to 2048) for tuning
 static int lu_outer()
@@ -556,9 +556,222 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
   return 0;
 }
 
-template <typename T>
-static int lu_solve(const T *A, const T *Linv, const T *Uinv, int n3, int ld, double *x, cudaStream_t st)
+// ---- triangular sweeps in one launch per factor ---------------------------------
+// Forward with the unit-lower factor: x_k = Linv_k (b_k - sum_{j<k} L_kj x_j);
+// backward with U: x_k = Uinv_k (b_k - sum_{j>k} U_kj x_j), blocks of 128.
+// One persistent launch per sweep: each CTA takes the next block in sweep
+// order from an atomic counter, subtracts the products with the blocks already
+// solved as their flags appear (streaming its row panel of the factor while
+// the chain of blocks advances), applies the diagonal block's inverse, and
+// publishes x_k and its flag (release; readers acquire, then read x_j through
+// L2).  A CTA waits only on blocks taken before its own by CTAs that are
+// running, so every wait ends; each is also bounded by TRI_SPIN polls, after
+// which the launch records an error in *err and every CTA returns.
+// sync layout: [counter, flags of the blocks]; zeroed before each sweep.
+constexpr long long TRI_SPIN = 1ll << 24;
+
+__device__ __forceinline__ int ld_acquire_s32(const int *p)
 {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_s32(int *p, int v)
+{
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// One lane's slice of a 128-wide row of the factor (or of a diagonal-block
+// inverse), loaded ahead of use, and its dot product with xs.
+template <typename T> struct RowSlice;
+template <> struct RowSlice<float> {
+  float4 v;
+  __device__ __forceinline__ void load(const float *row, int lane) { v = __ldg(reinterpret_cast<const float4 *>(row) + lane); }
+  __device__ __forceinline__ void zero() { v = make_float4(0.f, 0.f, 0.f, 0.f); }
+  __device__ __forceinline__ double dot(const double *xs, int lane) const
+  {
+    const double *xp = xs + 4 * lane;
+    return (double)v.x * xp[0] + (double)v.y * xp[1] + (double)v.z * xp[2] + (double)v.w * xp[3];
+  }
+};
+template <> struct RowSlice<double> {
+  double2 a, b;
+  __device__ __forceinline__ void load(const double *row, int lane)
+  {
+    a = __ldg(reinterpret_cast<const double2 *>(row) + lane);
+    b = __ldg(reinterpret_cast<const double2 *>(row) + 32 + lane);
+  }
+  __device__ __forceinline__ void zero() { a = b = make_double2(0.0, 0.0); }
+  __device__ __forceinline__ double dot(const double *xs, int lane) const
+  {
+    return a.x * xs[2 * lane] + a.y * xs[2 * lane + 1] + b.x * xs[64 + 2 * lane] + b.y * xs[64 + 2 * lane + 1];
+  }
+};
+
+// rows per warp per batch: 8 warps x TRI_ROWS<T> x TRI_BATCH<T> = 128 rows
+template <typename T> constexpr int tri_rows() { return sizeof(T) == 4 ? 16 : 8; }
+
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(256, 2) tri_sweep_kernel(const T *__restrict__ A, int ld, const T *__restrict__ Inv, int n3,
+                                                        double *x, int *sync, int *err)
+{
+  constexpr int NR = tri_rows<T>(), NB = LU_NB / (8 * NR);  // rows per batch, batches
+  __shared__ double xs[LU_NB], acc_s[LU_NB];
+  __shared__ int s_t, s_bad;
+  const int nblk = (n3 + LU_NB - 1) / LU_NB;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int *flags = sync + 1;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) { s_t = atomicAdd(sync, 1); s_bad = 0; }
+    __syncthreads();
+    const int t = s_t;
+    if (t >= nblk) return;
+    const int k = UPPER ? nblk - 1 - t : t;
+    const int k0 = k * LU_NB, nb = min(LU_NB, n3 - k0);
+    // this warp's rows: (warp * NB + batch) * NR + i, accumulated in shared
+    // memory by the warp's lane 0 (every row belongs to one warp)
+    if (threadIdx.x < LU_NB) acc_s[threadIdx.x] = threadIdx.x < nb ? x[k0 + threadIdx.x] : 0.0;
+    for (int s = 0; s < t; s++) {
+      const int j = UPPER ? nblk - 1 - s : s;
+      const int j0 = j * LU_NB, nbj = min(LU_NB, n3 - j0);
+      const bool full = (nbj == LU_NB);
+      // the tile's first batch is loaded before the wait: it does not depend on x_j
+      RowSlice<T> v[NR];
+      if (full) {
+#pragma unroll
+        for (int i = 0; i < NR; i++) {
+          const int r = warp * NB * NR + i;
+          if (r < nb) v[i].load(A + (size_t)(k0 + r) * ld + j0, lane);
+          else v[i].zero();
+        }
+      }
+      if (threadIdx.x == 0) {
+        long long it = 0;
+        while (ld_acquire_s32(flags + j) == 0) {
+          if (++it > TRI_SPIN || ld_acquire_s32(err) != 0) { s_bad = 1; atomicExch(err, 1); break; }
+        }
+      }
+      __syncthreads();  // the flag seen; every warp done with the previous xs
+      if (s_bad) return;
+      if (threadIdx.x < LU_NB) xs[threadIdx.x] = threadIdx.x < nbj ? __ldcg(x + j0 + threadIdx.x) : 0.0;
+      __syncthreads();
+      if (full) {
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+          if (b > 0) {
+#pragma unroll
+            for (int i = 0; i < NR; i++) {
+              const int r = (warp * NB + b) * NR + i;
+              if (r < nb) v[i].load(A + (size_t)(k0 + r) * ld + j0, lane);
+              else v[i].zero();
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < NR; i++) {
+            const double w = warp_sum(v[i].dot(xs, lane));
+            if (lane == 0) acc_s[(warp * NB + b) * NR + i] -= w;
+          }
+        }
+      } else {
+        // the last, partial block: masked columns
+#pragma unroll
+        for (int b = 0; b < NB; b++)
+#pragma unroll
+          for (int i = 0; i < NR; i++) {
+            const int r = (warp * NB + b) * NR + i;
+            double w = 0.0;
+            if (r < nb) {
+              const T *a = A + (size_t)(k0 + r) * ld + j0;
+              for (int c = lane; c < nbj; c += 32) w += (double)a[c] * xs[c];
+            }
+            w = warp_sum(w);
+            if (lane == 0) acc_s[r] -= w;
+          }
+      }
+    }
+    // x_k = Inv_k acc (rows of Inv beyond nb hold zero columns)
+    __syncthreads();
+    if (threadIdx.x < LU_NB) xs[threadIdx.x] = threadIdx.x < nb ? acc_s[threadIdx.x] : 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+      RowSlice<T> v[NR];
+#pragma unroll
+      for (int i = 0; i < NR; i++) {
+        const int r = (warp * NB + b) * NR + i;
+        if (r < nb) v[i].load(Inv + (size_t)(k0 + r) * LU_NB, lane);
+        else v[i].zero();
+      }
+#pragma unroll
+      for (int i = 0; i < NR; i++) {
+        const int r = (warp * NB + b) * NR + i;
+        const double w = warp_sum(v[i].dot(xs, lane));
+        if (lane == 0 && r < nb) x[k0 + r] = w;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release_s32(flags + k, 1);
+    }
+  }
+}
+
+// RADB200_TRI_SWEEP=0: the per-block launches below instead (A/B comparisons)
+static bool tri_sweep_enabled()
+{
+  static int on = -1;
+  if (on < 0) {
+    const char *e = getenv("RADB200_TRI_SWEEP");
+    on = (e && atoi(e) == 0) ? 0 : 1;
+  }
+  return on == 1;
+}
+
+static DBuf g_tri_err;  // allocated with the first factors, before any capture
+
+// the sweeps' counters and flags of an interaction (allocated with its factors,
+// so that a captured solve never sees the buffer move)
+static int tri_sync_alloc(Intrc &I)
+{
+  const size_t per = (size_t)(I.n3 + LU_NB - 1) / LU_NB + 1;
+  RB_TRY(I.tri_sync.alloc(2 * per * sizeof(int)));
+  if (!g_tri_err.p) {
+    RB_TRY(g_tri_err.alloc(sizeof(int)));
+    RB_CUDA(cudaMemset(g_tri_err.p, 0, sizeof(int)));
+  }
+  return 0;
+}
+
+template <typename T>
+static int lu_solve_sweeps(const T *A, const T *Linv, const T *Uinv, int n3, int ld, double *x, int *sync,
+                           cudaStream_t st)
+{
+  const int nblk = (n3 + LU_NB - 1) / LU_NB;
+  const size_t per = (size_t)nblk + 1;
+  RB_CUDA(cudaMemsetAsync(sync, 0, 2 * per * sizeof(int), st));
+  const int grid = std::min(nblk, 148 * 4);
+  tri_sweep_kernel<T, false><<<grid, 256, 0, st>>>(A, ld, Linv, n3, x, sync, g_tri_err.as<int>());
+  RB_TRY(check_launch("tri_sweep_kernel"));
+  tri_sweep_kernel<T, true><<<grid, 256, 0, st>>>(A, ld, Uinv, n3, x, sync + per, g_tri_err.as<int>());
+  return check_launch("tri_sweep_kernel");
+}
+
+// error flag of the sweeps: 0, or 1 when a wait ran out (then cleared)
+int tri_sweep_error(int *flag)
+{
+  *flag = 0;
+  if (!g_tri_err.p) return 0;
+  RB_CUDA(cudaMemcpy(flag, g_tri_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (*flag) RB_CUDA(cudaMemset(g_tri_err.p, 0, sizeof(int)));
+  return 0;
+}
+
+template <typename T>
+static int lu_solve(const T *A, const T *Linv, const T *Uinv, int n3, int ld, double *x, int *sync, cudaStream_t st)
+{
+  if (sync && tri_sweep_enabled()) return lu_solve_sweeps<T>(A, Linv, Uinv, n3, ld, x, sync, st);
   for (int k0 = 0; k0 < n3; k0 += LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
     block_matvec_kernel<T><<<1, 256, 0, st>>>(Linv, k0, nb, x);
@@ -588,12 +801,12 @@ static int lu_solve_direct(Intrc &I, int transposed, double *x, cudaStream_t st)
   if (I.lu_mode == RADB200_LU_F64) {
     const double *L = I.LUinv.as<double>(), *U = L + (size_t)n3 * LU_NB;
     return transposed ? lu_solve_t<double>(I.LU64.as<double>(), L, U, n3, ld, x, st)
-                      : lu_solve<double>(I.LU64.as<double>(), L, U, n3, ld, x, st);
+                      : lu_solve<double>(I.LU64.as<double>(), L, U, n3, ld, x, I.tri_sync.as<int>(), st);
   }
   if (I.lu_mode == RADB200_LU_TF32) {
     const float *L = I.LUinv.as<float>(), *U = L + (size_t)n3 * LU_NB;
     return transposed ? lu_solve_t<float>(I.LU32.as<float>(), L, U, n3, ld, x, st)
-                      : lu_solve<float>(I.LU32.as<float>(), L, U, n3, ld, x, st);
+                      : lu_solve<float>(I.LU32.as<float>(), L, U, n3, ld, x, I.tri_sync.as<int>(), st);
   }
   set_error("no LU factors on this interaction");
   return RADB200_E_ARG;
@@ -703,6 +916,7 @@ int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_sec
   RB_TRY(tc_error_flag(&tcflag));
   if (tcflag) { I.lu_mode = -1; set_error("LU: a tensor-core update timed out waiting for its MMAs"); return RADB200_E_TIMEOUT; }
   if (herr) { I.lu_mode = -1; set_error("LU: vanishing pivot (matrix not factorable without pivoting)"); return RADB200_E_NUMERIC; }
+  RB_TRY(tri_sync_alloc(I));
   I.lu_mode = mode;
   I.lu_of_d = of_d;
   I.lu_solve_id = I.solve_id;
@@ -730,6 +944,9 @@ int direct_solve(Intrc &I, int mode, double rtol, int max_iter, double *status)
   int its = 0;
   RB_TRY(gmres(op, n3, ld, b, I.M.as<double>(), rtol, max_iter, 30, &relres, &its, 0));
   RB_CUDA(cudaDeviceSynchronize());
+  int tri_err = 0;
+  RB_TRY(tri_sweep_error(&tri_err));
+  if (tri_err) { set_error("direct solve: a triangular sweep timed out waiting for a block"); return RADB200_E_TIMEOUT; }
   status[0] = relres;
   status[1] = its;
   status[2] = tf;

@@ -2,7 +2,7 @@
 five benchmark configurations, at their stated sizes.
 
     make -f oracle/Makefile.ref -j8                # builds oracle/_ref
-    python tests/golden/make_baseline_golden.py [c1 c2 c3 c4 c5]
+    python tests/golden/make_baseline_golden.py [c1 c2 c3 c3o c3q c4 c5]
 
 Runs the reference Radia CPU module (oracle/_ref, FldLenRndSw('off')) on the
 seeded models of tests/models.py:
@@ -20,6 +20,14 @@ seeded models of tests/models.py:
       2,000 points outside the body -- the FP64 oracle of the direct-solve
       path (the reference stores its own matrix in FP32, which is not a 1e-6
       oracle at chi = 1000);
+  c3o the same 3,000-tetrahedron system built and solved by the CPU oracle
+      (oracle/oracle.py: the interaction matrix of the restated element
+      fields, LAPACK, B by the oracle field) -- the FP64 oracle proper;
+  c3q the reference's self-interaction block of each of those tetrahedra,
+      kept for the elements where it departs from the oracle's by more than
+      1e-9 (one element, whose nearly axis-parallel edge sends the reference
+      into a tolerance branch; tests/test_oracle_quadrature.py settles which
+      of the two is right with an independent surface-charge quadrature);
   c4  the 640-block planar undulator, Solve(prec 1e-10), B at 4,000 axis points;
   c5  the 6,080-element hybrid undulator (saturating poles, a mirror plane),
       Solve(prec 1e-7), B at a seeded 10,000-point subsample of its 1e5 points.
@@ -40,6 +48,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
 sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, ROOT)
 
 import models as MD  # noqa: E402
 import radia as R  # noqa: E402
@@ -140,6 +149,51 @@ def c3(out, n_tets=3000, ncell=8, chi=1000.0, n_pts=2000):
     out["c3_residual"] = np.array([res])
 
 
+def _oracle_c3_pack(n_tets=3000, ncell=8, chi=1000.0):
+    from oracle import oracle as O
+    from radiacuda_b200 import model, rad
+    whole, body = MD.tet_mesh(rad, ncell=ncell, n_tets=n_tets, chi=chi)
+    return O, model, rad, whole, model.pack_interaction(rad._objs, whole, 0, tuple(rad._rand))
+
+
+def c3o(out, n_pts=2000, ncell=8):
+    O, model, rad, whole, pack = _oracle_c3_pack(ncell=ncell)
+    N = O.assemble(pack)
+    M = O.linear_direct(pack, N, O.extfield(pack))
+    for lf, m in zip(pack.leaves, M.reshape(-1, 3)):
+        lf.obj.m = m.copy()
+    P = MD.tet_mesh_points(n_pts, ncell=ncell)
+    out["c3o_M"] = M
+    out["c3o_b"] = O.field(model.pack_sources(rad._objs, whole, tuple(rad._rand)), P, 0)
+
+
+def c3q(out, ncell=8, n_tets=3000):
+    O, _, _, _, pack = _oracle_c3_pack(ncell=ncell, n_tets=n_tets)
+    N = O.assemble(pack)
+    _, body = MD.tet_mesh(R, ncell=ncell, n_tets=n_tets, chi=1000.0)
+    V = np.asarray(MD.tet_mesh_vertices(ncell, n_tets))
+    elems = R.ObjCntStuf(body)
+    cen = V.mean(axis=1)
+    for e in elems:
+        R.ObjSetM(e, [0.0, 0.0, 0.0])
+    idx, blocks = [], []
+    for j, e in enumerate(elems):
+        blk = np.zeros((3, 3))
+        for k in range(3):
+            m = [0.0, 0.0, 0.0]
+            m[k] = 1.0
+            R.ObjSetM(e, m)
+            blk[:, k] = R.Fld(e, "h", cen[j].tolist())
+        R.ObjSetM(e, [0.0, 0.0, 0.0])
+        if np.abs(blk - N[3 * j:3 * j + 3, 3 * j:3 * j + 3]).max() > 1e-9:
+            idx.append(j)
+            blocks.append(blk)
+    out["c3q_idx"] = np.array(idx, dtype=np.int64)
+    out["c3q_ref"] = np.array(blocks).reshape(-1, 3, 3)
+    out["c3q_V"] = V[idx].reshape(-1, 4, 3)
+    print(f"  reference self blocks off the oracle's by > 1e-9: elements {idx}")
+
+
 def c4(out):
     m, _ = MD.undulator(R)
     P = MD.undulator_points()
@@ -167,4 +221,4 @@ def main(names):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["c1", "c2", "c3", "c4", "c5"])
+    main(sys.argv[1:] or ["c1", "c2", "c3", "c3o", "c3q", "c4", "c5"])

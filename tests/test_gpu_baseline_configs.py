@@ -6,9 +6,15 @@ Tolerances, per point (|dB_i| / |B_i|, points where |B_i| is below 1e-3 of
 the largest measured against that floor) and as the max-norm ratio: 5e-6 for
 linear and 5e-5 for saturating materials after relaxation (the reference's
 tests/test_recmag_asm.py:134-157 bars); 1e-6 for the 3,000-tetrahedron
-chi = 1000 direct solve against the FP64 oracle built from the reference's
-own element fields -- the precision target, for the plain FP64 path and for
-the mixed path (TF32 tensor-core LU + FP64 GMRES-IR, FP32 field terms).
+chi = 1000 direct solve against the FP64 oracle (c3o: the CPU oracle's
+interaction matrix, LAPACK, the oracle's field) -- the precision target, for
+the plain FP64 path and for the mixed path (TF32 tensor-core LU + FP64
+GMRES-IR, FP32 field terms). Against the system built from the reference's
+own element fields (c3) the bar is 5e-6: one of its 3,000 self blocks is off
+by 1e-4 (a tolerance branch of the reference's polygon integrals on a nearly
+axis-parallel edge; tests/test_oracle_quadrature.py shows the oracle right
+there against an independent quadrature), and at chi = 1000 that element
+alone moves B outside by 3.0e-6, the gap between the two goldens.
 """
 import os
 
@@ -86,5 +92,10 @@ def test_c3_chi1000_direct_solve_3000_tets_vs_fp64_oracle(cuda, rad, gold, path)
         st = rad.RlxAuto(im, 1e-13, 200, 13)
         B = np.array(rad.Fld(whole, "b", P.tolist(), precision="single"))
     assert st[0] < 1e-12, st
-    e = errs(B, gold["c3_b"])
+    e = errs(B, gold["c3o_b"])
     assert e[0] < 1e-6 and e[1] < 1e-6, (path, e)
+    g = errs(gold["c3o_b"], gold["c3_b"])
+    r = errs(B, gold["c3_b"])
+    assert r[0] < 5e-6 and r[1] < 5e-6, (path, r)
+    # the distance to the reference-built golden is the distance between the goldens
+    assert abs(r[1] - g[1]) < 0.1 * g[1], (path, r, g)
