@@ -26,6 +26,7 @@ No counterpart in the reference: Radia has no derivatives.
 from __future__ import annotations
 
 import time
+import warnings
 from typing import Dict, Optional, Sequence
 
 import numpy as np
@@ -38,7 +39,7 @@ _WHAT = {"b": 0, "h": 1}
 
 class FieldProblem:
     def __init__(self, obj: int, pts, what: str = "b", srcobj: int = 0, storage: int = 1,
-                 solver: str = "auto", prec: float = 1e-13, max_iter: int = 200, adj_rtol: float = 1e-12):
+                 solver: str = "auto", prec: float = 1e-13, max_iter: int = 2000, adj_rtol: float = 1e-12):
         if what not in _WHAT:
             raise ValueError("what must be 'b' or 'h'")
         self.pack = model.pack_interaction(_rad._objs, int(obj), int(srcobj), tuple(_rad._rand))
@@ -120,6 +121,10 @@ class FieldProblem:
                                np.zeros(3 * self.n))
         self._intrc, self._M = I, M
         self.last_status["forward"] = st
+        if not st[0] <= self.prec:
+            # the reference's wording for a relaxation that stopped short
+            warnings.warn("The specified accuracy was not reached. This may indicate diverging or incomplete "
+                          f"relaxation (misfit {st[0]:.3e}).", RuntimeWarning)
         t2 = time.perf_counter()
         g = {k: v.copy() for k, v in self.pack.elems.items()}
         for e, (kind, idx) in enumerate(self.pack.elem_src):

@@ -4,10 +4,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <thread>
 
 #include "internal.cuh"
 
@@ -35,20 +37,23 @@ int check_launch(const char *what)
   return 0;
 }
 
-// ---- reuse of large device blocks -----------------------------------------
-// Released blocks of BIG_BLOCK bytes and more wait here (after the device is
-// idle, so no kernel still uses them) until an allocation of at most 25% less
-// on the same device takes them, up to a cap of RADB200_BUFCACHE_GB (default:
-// 40% of the first device's memory; 0 turns reuse off).  A failed cudaMalloc
-// returns every cached block of that device to the driver and tries again;
+// ---- reuse of device blocks ---------------------------------------------------
+// Released blocks wait here (after the device is idle, so no kernel still
+// uses them) for the next request of their class on the same device: blocks
+// above SMALL_MAX by size (a request takes a cached block at most 25% larger),
+// up to RADB200_BUFCACHE_GB (default: 40% of the first device's memory; 0
+// turns reuse off); smaller blocks by power-of-two class, up to
+// RADB200_SMALLCACHE_GB (default 2).  A failed cudaMalloc returns every cached
+// block of that device to the driver and tries again;
 // radb200_release_cached_memory returns all of them.  Blocks are keyed by
 // device ordinal and the pool is guarded by a mutex, so host threads and
 // device switches do not mix blocks up.  The pool is never destroyed (blocks
 // outlive static DBufs).
 namespace {
 struct BigPool {
-  std::map<int, std::multimap<size_t, void *>> blocks;  // device -> size -> block
-  size_t total = 0, cap = 0;
+  std::map<int, std::multimap<size_t, void *>> blocks;      // device -> size -> block (large)
+  std::map<int, std::map<size_t, std::vector<void *>>> small;  // device -> class -> blocks
+  size_t total = 0, cap = 0, small_total = 0, small_cap = 0;
   bool init = false;
   std::mutex mu;
 };
@@ -68,6 +73,8 @@ void big_init(BigPool &bp)
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) bp.cap = tot / 10 * 4;
     else cudaGetLastError();
   }
+  const char *es = getenv("RADB200_SMALLCACHE_GB");
+  bp.small_cap = (size_t)((es ? atof(es) : 2.0) * 1073741824.0);
 }
 int current_device()
 {
@@ -86,52 +93,85 @@ void big_flush(BigPool &bp, int dev)
     if (it->first != cur) cudaSetDevice(cur);
     it = bp.blocks.erase(it);
   }
+  for (auto it = bp.small.begin(); it != bp.small.end();) {
+    if (dev >= 0 && it->first != dev) { ++it; continue; }
+    if (it->first != cur) cudaSetDevice(it->first);
+    for (auto &kv : it->second)
+      for (void *q : kv.second) { cudaFree(q); bp.small_total -= kv.first; }
+    if (it->first != cur) cudaSetDevice(cur);
+    it = bp.small.erase(it);
+  }
   cudaGetLastError();
+}
+size_t small_class(size_t b)
+{
+  size_t s = 256;
+  while (s < b) s <<= 1;
+  return s;
 }
 }  // namespace
 
-void big_release_all()
+void pool_release_all()
 {
   BigPool &bp = big_pool();
   std::lock_guard<std::mutex> lk(bp.mu);
   big_flush(bp, -1);
 }
 
-void *big_alloc(size_t b, size_t *got)
+void *pool_alloc(size_t b, size_t *got)
 {
   BigPool &bp = big_pool();
   std::lock_guard<std::mutex> lk(bp.mu);
   big_init(bp);
   const int dev = current_device();
-  auto &mine = bp.blocks[dev];
-  auto it = mine.lower_bound(b);
-  if (it != mine.end() && it->first <= b + b / 4) {
-    void *p = it->second;
-    *got = it->first;
-    bp.total -= it->first;
-    mine.erase(it);
-    return p;
+  size_t want = b;
+  if (b <= SMALL_MAX) {
+    want = small_class(b);
+    auto &cls = bp.small[dev][want];
+    if (!cls.empty()) {
+      void *p = cls.back();
+      cls.pop_back();
+      bp.small_total -= want;
+      *got = want;
+      return p;
+    }
+  } else {
+    auto &mine = bp.blocks[dev];
+    auto it = mine.lower_bound(b);
+    if (it != mine.end() && it->first <= b + b / 4) {
+      void *p = it->second;
+      *got = it->first;
+      bp.total -= it->first;
+      mine.erase(it);
+      return p;
+    }
   }
   void *p = nullptr;
-  if (cudaMalloc(&p, b) != cudaSuccess) {
+  if (cudaMalloc(&p, want) != cudaSuccess) {
     cudaGetLastError();
     big_flush(bp, dev);
-    if (cudaMalloc(&p, b) != cudaSuccess) {
+    if (cudaMalloc(&p, want) != cudaSuccess) {
       cudaGetLastError();
-      set_error("device allocation of %zu bytes failed", b);
+      set_error("device allocation of %zu bytes failed", want);
       return nullptr;
     }
   }
-  *got = b;
+  *got = want;
   return p;
 }
 
-void big_free(void *p, size_t b)
+void pool_free(void *p, size_t b)
 {
   BigPool &bp = big_pool();
   std::lock_guard<std::mutex> lk(bp.mu);
   big_init(bp);
-  if (bp.total + b <= bp.cap && cudaDeviceSynchronize() == cudaSuccess) {
+  if (b <= SMALL_MAX) {
+    if (bp.small_total + b <= bp.small_cap && cudaDeviceSynchronize() == cudaSuccess) {
+      bp.small[current_device()][b].push_back(p);
+      bp.small_total += b;
+      return;
+    }
+  } else if (bp.total + b <= bp.cap && cudaDeviceSynchronize() == cudaSuccess) {
     bp.blocks[current_device()].emplace(b, p);
     bp.total += b;
     return;
@@ -231,14 +271,17 @@ static void build_tet_record(const std::vector<double> &V, const std::vector<std
   out.insert(out.end(), rec, rec + (tensor ? TET_REC_TENSOR : TET_REC_FIELD));
 }
 
-static void build_topo(const RadB200Geom *G, bool tensor, HostTopo &h)
+// Polyhedra [pa, pb) into h, their entries of tinfo / tinfo2 / tetidx at
+// p - pa and every offset relative to h's own arrays.
+static void build_topo_range(const RadB200Geom *G, bool tensor, int pa, int pb, HostTopo &h)
 {
-  h.tinfo.resize(G->n_poly);
-  h.tinfo2.resize(G->n_poly);
-  h.tetidx.assign(G->n_poly, -1);
-  for (int p = 0; p < G->n_poly; p++) {
-    int f0 = G->poly_info[4 * p], nf = G->poly_info[4 * p + 1];
-    const double *M = G->poly + (size_t)p * RADB200_POLY_STRIDE + 3;
+  h.tinfo.resize(pb - pa);
+  h.tinfo2.resize(pb - pa);
+  h.tetidx.assign(pb - pa, -1);
+  for (int pg = pa; pg < pb; pg++) {
+    const int p = pg - pa;
+    int f0 = G->poly_info[4 * pg], nf = G->poly_info[4 * pg + 1];
+    const double *M = G->poly + (size_t)pg * RADB200_POLY_STRIDE + 3;
     int v0 = (int)(h.tv.size() / 3), e0 = (int)h.tel.size(), t0 = (int)h.tt.size(), ff0 = (int)(h.tfn.size() / 3);
     std::vector<double> V;  // local vertices
     std::vector<std::vector<int>> loops(nf);
@@ -341,13 +384,53 @@ static void build_topo(const RadB200Geom *G, bool tensor, HostTopo &h)
   }
 }
 
-int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs)
+// All polyhedra, in ranges on up to 16 host threads, joined in order.
+static void build_topo(const RadB200Geom *G, bool tensor, HostTopo &h)
+{
+  const int np = G->n_poly;
+  const int nth = std::max(1, std::min({16, (int)std::thread::hardware_concurrency(), np / 512}));
+  if (nth <= 1) {
+    build_topo_range(G, tensor, 0, np, h);
+    return;
+  }
+  std::vector<HostTopo> part(nth);
+  {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+      th.emplace_back(build_topo_range, G, tensor, (int)((long long)np * t / nth), (int)((long long)np * (t + 1) / nth),
+                      std::ref(part[t]));
+    for (auto &t : th) t.join();
+  }
+  const int rs = tensor ? TET_REC_TENSOR : TET_REC_FIELD;
+  h = HostTopo();
+  for (auto &q : part) {
+    const int nv = (int)(h.tv.size() / 3), ne = (int)h.tel.size(), nt = (int)h.tt.size(), nf = (int)(h.tfn.size() / 3);
+    const int ntet = (int)(h.tetrec.size() / rs);
+    for (auto &a : q.tinfo) h.tinfo.push_back(make_int4(a.x + nv, a.y, a.z + ne, a.w));
+    for (auto &a : q.tinfo2) h.tinfo2.push_back(make_int4(a.x + nt, a.y, a.z + nf, a.w));
+    for (int t : q.tetidx) h.tetidx.push_back(t >= 0 ? t + ntet : -1);
+    h.tt.insert(h.tt.end(), q.tt.begin(), q.tt.end());
+    h.te.insert(h.te.end(), q.te.begin(), q.te.end());
+    h.tv.insert(h.tv.end(), q.tv.begin(), q.tv.end());
+    h.tel.insert(h.tel.end(), q.tel.begin(), q.tel.end());
+    h.teg.insert(h.teg.end(), q.teg.begin(), q.teg.end());
+    h.teG.insert(h.teG.end(), q.teG.begin(), q.teG.end());
+    h.ttm.insert(h.ttm.end(), q.ttm.begin(), q.ttm.end());
+    h.tfn.insert(h.tfn.end(), q.tfn.begin(), q.tfn.end());
+    h.tfa.insert(h.tfa.end(), q.tfa.begin(), q.tfa.end());
+    h.tetrec.insert(h.tetrec.end(), q.tetrec.begin(), q.tetrec.end());
+  }
+}
+
+int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs, bool mesh)
 {
   RB_TRY(validate_geom(G));
   all_tets = 0;
   if (G->n_poly > 0) {
     HostTopo h;
+    PhaseClock pc;
     build_topo(G, tensor_coeffs, h);
+    pc.mark("geometry: topology (host)");
     RB_TRY(tinfo.upload(h.tinfo.data(), h.tinfo.size() * sizeof(int4)));
     RB_TRY(tinfo2.upload(h.tinfo2.data(), h.tinfo2.size() * sizeof(int4)));
     RB_TRY(tv.upload(h.tv.data(), h.tv.size() * sizeof(double)));
@@ -364,7 +447,9 @@ int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs)
     all_tets = std::all_of(h.tetidx.begin(), h.tetidx.end(), [](int t) { return t >= 0; }) ? 1 : 0;
     m_tiles = m_groups = 0;
     // field geometry of an all-tetrahedron model: the mesh form (unique edges and faces)
-    if (all_tets && !tensor_coeffs) RB_TRY(build_mesh(G, h.tetidx, h.tetrec, *this));
+    pc.mark("geometry: topology upload");
+    if (all_tets && !tensor_coeffs && mesh) RB_TRY(build_mesh(G, h.tetidx, h.tetrec, *this));
+    pc.mark("geometry: mesh form");
   } else {
     m_tiles = m_groups = 0;
   }
@@ -457,6 +542,37 @@ int field_vjp(Intrc &I, const double *M, const double *pts, int64_t npts, int wh
 
 using namespace rb;
 
+namespace rb {
+double g_tm[3] = {0.0, 0.0, 0.0};
+bool timing_on()
+{
+  static int on = -1;
+  if (on < 0) {
+    const char *e = getenv("RADB200_TIMING");
+    on = (e && atoi(e) != 0) ? 1 : 0;
+  }
+  return on == 1;
+}
+double now_s()
+{
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+PhaseClock::PhaseClock() : on(timing_on()), t(on ? now_s() : 0.0)
+{
+  for (int k = 0; k < 3; k++) tm0[k] = g_tm[k];
+}
+void PhaseClock::mark(const char *what)
+{
+  if (!on) return;
+  cudaDeviceSynchronize();
+  const double u = now_s();
+  fprintf(stderr, "RADB200_TIMING %-28s %9.3f ms (malloc %.3f, free %.3f, h2d %.3f)\n", what, 1e3 * (u - t),
+          1e3 * (g_tm[0] - tm0[0]), 1e3 * (g_tm[1] - tm0[1]), 1e3 * (g_tm[2] - tm0[2]));
+  t = u;
+  for (int k = 0; k < 3; k++) tm0[k] = g_tm[k];
+}
+}  // namespace rb
+
 extern "C" {
 
 const char *radb200_last_error(void) { return g_err; }
@@ -468,12 +584,17 @@ int radb200_device_sync(void)
   return 0;
 }
 
+
 int radb200_field_dev(const RadB200Geom *g, const double *d_pts, int64_t npts, int what, int precision, double *d_out)
 {
   if (npts < 0 || what < 0 || what > 2 || precision < 0 || precision > 2) { set_error("bad field arguments"); return RADB200_E_ARG; }
-  RB_TRY(g_fld_geom.upload(g));
+  PhaseClock pc;
+  // the mesh form serves FP64 B / H only
+  RB_TRY(g_fld_geom.upload(g, false, precision != 1 && what != 2));
+  pc.mark("field: geometry upload");
   RB_TRY(launch_field(g_fld_geom.view(precision != 0), d_pts, npts, what, precision == 1 ? 1 : 0, d_out, g_fld_scratch, 0));
   RB_CUDA(cudaStreamSynchronize(0));
+  pc.mark("field: kernels");
   return 0;
 }
 
@@ -559,8 +680,10 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
   I->n3 = 3 * n;
   I->ld = (I->n3 + 31) / 32 * 32;
   I->storage = storage;
+  PhaseClock pc;
   RB_TRY(I->geom.upload(elems, fast != 0));
   I->fast = fast;
+  pc.mark("create: geometry upload");
   // observation points and row transforms from each element's main image
   std::vector<double> obs(3 * (size_t)n), rowT(9 * (size_t)n);
   I->h_obsJ.assign(9 * (size_t)n, 0.0);
@@ -596,6 +719,7 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
   }
   RB_TRY(I->elem_src.upload(r->elem_src, 2 * (size_t)n * sizeof(int)));
   RB_TRY(upload_materials(*I, r));
+  pc.mark("create: observers, materials");
   size_t nn = (size_t)I->n3 * I->ld;
   // mixed: every block in FP32, the near ones also as their FP64 residue
   if (storage == RADB200_STORE_F64) RB_TRY(I->N64.alloc(nn * sizeof(double)));
@@ -605,7 +729,9 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
   if (assemble)
     RB_TRY(launch_assemble(I->geom.view(fast), I->elem_src.as<int>(), I->obs.as<double>(), I->rowT.as<double>(), n, I->ld,
                            I->N32.as<float>(), I->N64.as<double>(), 0));
+  pc.mark("create: assembly");
   if (storage == RADB200_STORE_MIXED) RB_TRY(build_near(*I, elems, r, obs.data()));
+  pc.mark("create: near pairs");
   // external field at element centres, in element frames
   size_t vb = (size_t)I->ld * sizeof(double);
   RB_TRY(I->hext.alloc(vb));
@@ -623,6 +749,7 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
   RB_CUDA(cudaMemset(I->M.p, 0, vb)); RB_CUDA(cudaMemset(I->H.p, 0, vb));
   RB_CUDA(cudaMemset(I->Mp.p, 0, vb)); RB_CUDA(cudaMemset(I->F.p, 0, vb));
   RB_CUDA(cudaDeviceSynchronize());
+  pc.mark("create: external field");
   int64_t h = g_next_handle++;
   g_intrc[h] = std::move(I);
   *handle = h;
@@ -819,7 +946,7 @@ int radb200_intrc_restore(const RadB200Geom *elems, const RadB200Relax *r, const
 
 int radb200_release_cached_memory(void)
 {
-  rb::big_release_all();
+  rb::pool_release_all();
   return 0;
 }
 
@@ -858,10 +985,13 @@ int radb200_intrc_matrix(int64_t handle, int dtype, void *out)
     double *o = (double *)out;
     for (size_t k = 0; k < n3 * n3; k++) o[k] = tmp[k];
     std::vector<double> D((size_t)I->near_nnz * 9);
+    std::vector<int> ptr(I->n + 1), col(I->near_nnz);
     RB_CUDA(cudaMemcpy(D.data(), I->near_D.p, D.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    RB_CUDA(cudaMemcpy(ptr.data(), I->near_ptr.p, ptr.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    RB_CUDA(cudaMemcpy(col.data(), I->near_col.p, col.size() * sizeof(int), cudaMemcpyDeviceToHost));
     for (int i = 0; i < I->n; i++)
-      for (int k = I->h_near_ptr[i]; k < I->h_near_ptr[i + 1]; k++) {
-        const int j = I->h_near_col[k];
+      for (int k = ptr[i]; k < ptr[i + 1]; k++) {
+        const int j = col[k];
         for (int a = 0; a < 3; a++)
           for (int b = 0; b < 3; b++) o[(3 * (size_t)i + a) * n3 + 3 * j + b] += D[9 * (size_t)k + 3 * a + b];
       }

@@ -25,6 +25,20 @@ int check_launch(const char *what);   // cudaGetLastError after a launch
       return RADB200_E_CUDA;                                                        \
     }                                                                               \
   } while (0)
+// RADB200_TIMING=1 prints the phases of interaction creation and field
+// calls on stderr; each mark synchronizes the device first, so a phase
+// includes its kernels.  Off: a mark costs one branch.
+struct PhaseClock {
+  bool on;
+  double t;
+  double tm0[3];
+  PhaseClock();
+  void mark(const char *what);
+};
+bool timing_on();
+double now_s();
+extern double g_tm[3];  // seconds in cudaMalloc, cudaFree, cudaMemcpy of DBufs (timing on)
+
 #define RB_TRY(x)            \
   do {                       \
     int r_ = (x);            \
@@ -32,13 +46,19 @@ int check_launch(const char *what);   // cudaGetLastError after a launch
   } while (0)
 
 // ---- device buffers ----------------------------------------------------------
-// Blocks of BIG_BLOCK bytes and more are kept for reuse when released (up to
-// a cap, see big_free in capi.cu): an interaction's 10-60 GB of matrix and
-// factors would otherwise be unmapped and mapped again by every create/free.
+// Every DBuf block comes from a per-device pool (pool_alloc / pool_free in
+// capi.cu).  Blocks above SMALL_MAX have their exact size and are reused by
+// any request up to 25% smaller (an interaction's 10-60 GB of matrix and
+// factors would otherwise be unmapped and mapped again by every
+// create/free); smaller ones are rounded up to a power of two and reused by
+// class.  cudaMalloc and cudaFree on a busy device can each take tens of
+// milliseconds (cudaFree also synchronizes), which for the dozens of small
+// buffers of an interaction adds up to a large share of its assembly.
 constexpr size_t BIG_BLOCK = (size_t)256 << 20;
-void *big_alloc(size_t b, size_t *got);  // nullptr on failure (error set)
-void big_free(void *p, size_t b);
-void big_release_all();
+constexpr size_t SMALL_MAX = BIG_BLOCK / 2;
+void *pool_alloc(size_t b, size_t *got);  // nullptr on failure (error set)
+void pool_free(void *p, size_t b);
+void pool_release_all();
 
 struct DBuf {
   void *p = nullptr;
@@ -50,8 +70,9 @@ struct DBuf {
   void release()
   {
     if (p) {
-      if (bytes >= BIG_BLOCK) big_free(p, bytes);
-      else cudaFree(p);
+      const double t0 = timing_on() ? now_s() : 0.0;
+      pool_free(p, bytes);
+      if (t0 > 0.0) g_tm[1] += now_s() - t0;
     }
     p = nullptr;
     bytes = 0;
@@ -61,26 +82,20 @@ struct DBuf {
     if (b <= bytes && p) return 0;
     release();
     if (b == 0) return 0;
-    if (b >= BIG_BLOCK) {
-      size_t got = 0;
-      p = big_alloc(b, &got);
-      if (!p) return RADB200_E_NOMEM;
-      bytes = got;
-      return 0;
-    }
-    if (cudaMalloc(&p, b) != cudaSuccess) {
-      cudaGetLastError();
-      set_error("device allocation of %zu bytes failed", b);
-      p = nullptr;
-      return RADB200_E_NOMEM;
-    }
-    bytes = b;
+    const double t0 = timing_on() ? now_s() : 0.0;
+    size_t got = 0;
+    p = pool_alloc(b, &got);
+    if (t0 > 0.0) g_tm[0] += now_s() - t0;
+    if (!p) return RADB200_E_NOMEM;
+    bytes = got;
     return 0;
   }
   int upload(const void *h, size_t b)
   {
     RB_TRY(alloc(b));
+    const double t0 = timing_on() ? now_s() : 0.0;
     if (b) RB_CUDA(cudaMemcpy(p, h, b, cudaMemcpyHostToDevice));
+    if (t0 > 0.0) g_tm[2] += now_s() - t0;
     return 0;
   }
   template <typename T> T *as() const { return (T *)p; }
@@ -149,7 +164,7 @@ struct DevGeom {
   int ustart[5] = {0, 0, 0, 0, 0};
   int all_tets = 0;
   Guard g{0, 0, 0};
-  int upload(const RadB200Geom *G, bool tensor_coeffs = false);
+  int upload(const RadB200Geom *G, bool tensor_coeffs = false, bool mesh = true);
   GeomView view(int fast = 0) const;
 };
 
@@ -164,6 +179,7 @@ struct NearView {
   const double *D = nullptr;
   const int *tptr = nullptr;
   const int *tidx = nullptr;
+  const int *row = nullptr;  // observer element of each entry
 };
 
 // ---- interaction state -------------------------------------------------------
@@ -177,16 +193,15 @@ struct Intrc {
   DevGeom geom;     // relaxable elements (object frames, images)
   DBuf elem_src, obs, rowT;           // [2n] int, [3n] obs points, [9n] s*Minv of main image
   DBuf N32, N64;                      // [n3 x ld]
-  DBuf near_ptr, near_col, near_D, near_tptr, near_tidx;  // mixed storage: FP64 residue of near pairs
+  DBuf near_ptr, near_row, near_col, near_D, near_tptr, near_tidx;  // mixed storage: FP64 residue of near pairs
   int64_t near_nnz = 0;
   double near_factor = 0.0;           // near range: centre distance <= factor * (r_i + r_j)
-  std::vector<int> h_near_ptr, h_near_col;
   NearView near() const
   {
     NearView v;
     if (near_nnz > 0) {
       v.ptr = near_ptr.as<int>(); v.col = near_col.as<int>(); v.D = near_D.as<double>();
-      v.tptr = near_tptr.as<int>(); v.tidx = near_tidx.as<int>();
+      v.tptr = near_tptr.as<int>(); v.tidx = near_tidx.as<int>(); v.row = near_row.as<int>();
     }
     return v;
   }

@@ -57,7 +57,7 @@ static int vcopy_axpy(double *y, const double *x, double a, const double *z, dou
 int gmres(Op &op, int n3, int ld, const double *b, double *x, double rtol, int max_iter, int restart, double *relres,
           int *iters, cudaStream_t)
 {
-  restart = std::max(1, std::min(restart, 60));
+  restart = std::max(1, std::min(restart, 200));
   DBuf Vb, wb, rb_;
   RB_TRY(Vb.alloc((size_t)(restart + 1) * ld * sizeof(double)));
   RB_TRY(wb.alloc((size_t)2 * ld * sizeof(double)));

@@ -169,4 +169,48 @@ __device__ __forceinline__ V3<double> find_new_h(int kind, const double *m, cons
   return H;
 }
 
+// Newton polish of the element's implicit field, H = Hq + Q M(H), from
+// find_new_h's result: J = I - Q dM/dH, at most 20 steps, each kept only if
+// it lowers the residual.  find_new_h stops after 15 passes of a linearly
+// converging secant, so its H carries an error that a Newton iteration on the
+// relaxation as a whole cannot remove (its convergence falls back to linear);
+// polished, the fixed-point map is exact to rounding and the outer Newton
+// converges quadratically.
+__device__ __forceinline__ double implicit_residual(int kind, const double *m, const double *Q, V3<double> Hq,
+                                                    V3<double> H, const double *__restrict__ mh, double *r)
+{
+  const V3<double> M = mat_M(kind, m, H, mh);
+  r[0] = H.x - Hq.x - (Q[0] * M.x + Q[1] * M.y + Q[2] * M.z);
+  r[1] = H.y - Hq.y - (Q[3] * M.x + Q[4] * M.y + Q[5] * M.z);
+  r[2] = H.z - Hq.z - (Q[6] * M.x + Q[7] * M.y + Q[8] * M.z);
+  return sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+}
+
+__device__ __forceinline__ V3<double> polish_h(int kind, const double *m, const double *Q, V3<double> Hq, V3<double> H,
+                                               const double *__restrict__ mh)
+{
+  if (kind == RADB200_MAT_LINEAR) return H;
+  double r[3], rn = implicit_residual(kind, m, Q, Hq, H, mh, r);
+  for (int it = 0; it < 20; it++) {
+    const double hn = sqrt(H.x * H.x + H.y * H.y + H.z * H.z);
+    if (!(rn > 1e-16 * fmax(hn, 1e-30))) break;
+    double D[9], A[9], Ai[9];
+    mat_D(kind, m, H, D, mh);
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++)
+        A[3 * a + b] = (a == b ? 1.0 : 0.0) - (Q[3 * a] * D[b] + Q[3 * a + 1] * D[3 + b] + Q[3 * a + 2] * D[6 + b]);
+    inv3x3(A, Ai);
+    const V3<double> Hn = mk3<double>(H.x - (Ai[0] * r[0] + Ai[1] * r[1] + Ai[2] * r[2]),
+                                      H.y - (Ai[3] * r[0] + Ai[4] * r[1] + Ai[5] * r[2]),
+                                      H.z - (Ai[6] * r[0] + Ai[7] * r[1] + Ai[8] * r[2]));
+    double r2[3];
+    const double rn2 = implicit_residual(kind, m, Q, Hq, Hn, mh, r2);
+    if (!(rn2 < rn)) break;
+    H = Hn;
+    rn = rn2;
+    r[0] = r2[0]; r[1] = r2[1]; r[2] = r2[2];
+  }
+  return H;
+}
+
 }  // namespace rb

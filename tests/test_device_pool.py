@@ -1,4 +1,4 @@
-"""Device blocks of 256 MB and more that a freed interaction leaves are kept
+"""Large device blocks (above 128 MB) that a freed interaction leaves are kept
 for the next one, and rad.UtiDelAll returns them to the driver."""
 import pytest
 
