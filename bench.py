@@ -292,6 +292,8 @@ def run_ours(args, rank, world):
                        assembly="FP64 vertex/edge form, stored FP32 with the FP64 residue of near blocks"),
         "breakdown_s": {"assembly": round(float(np.mean(t_asm)), 4), "solve": round(float(np.mean(t_solve)), 4),
                         "field": round(fld_s, 4)},
+        "steps_s": {"total": [round(x, 4) for x in times], "assembly": [round(x, 4) for x in t_asm],
+                    "solve": [round(x, 4) for x in t_solve], "field": [round(x, 4) for x in t_fld]},
         "b_rel_err_vs_plain_fp64": err, "b_rel_err_per_point_vs_plain_fp64": err_pp,
         "b_err_note": ("max|dB| / max|B| and max_i |dB_i| / |B_i| over the 1e6 points against the plain FP64 GPU "
                        "path, which the tests pin to an FP64 oracle built from the reference's own element fields "

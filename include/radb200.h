@@ -249,11 +249,31 @@ RADB200_API int radb200_field_int_cb(const RadB200Geom *g, RadB200PointField fn,
 RADB200_API int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r,
                          const RadB200Geom *ext, int storage, int64_t *handle);
 RADB200_API int radb200_intrc_free(int64_t handle);
-/* Device blocks of 256 MB and more (matrices, factors) are kept for reuse when
- * released, up to RADB200_BUFCACHE_GB (environment; default 40% of the
- * device's memory, 0 = off), so that repeated create / free cycles do not
- * unmap and remap tens of GB each time.  No counterpart in the reference.
- * This call returns every kept block to the driver.                         */
+/* Row block of an interaction, for a relaxation split over devices: the rows
+ * of observer elements e0 .. e1-1 against every source element (3 (e1-e0) x
+ * 3N, FP32 or FP64 storage), with the external field of those rows.  The
+ * reference relaxes on one device (radgpurlx.cu); this has no counterpart
+ * there.  The handle serves radb200_relax_rows_step and radb200_intrc_free
+ * only; every other call rejects it.                                         */
+RADB200_API int radb200_intrc_create_rows(const RadB200Geom *elems, const RadB200Relax *r,
+                              const RadB200Geom *ext, int storage, int32_t e0, int32_t e1,
+                              int64_t *handle);
+/* One Jacobi proposal of a row block (the step of RADB200_RLX_JACOBI): from
+ * the full magnetization d_M [3N] (device), H = N_rows M + H_ext, each row
+ * element's implicit field H' and M' = M(H'); writes d_Mp_rows = M',
+ * d_F_rows = M' - M and, unless NULL, d_H_rows = H' of its rows
+ * [3 (e1-e0)] (device), and *sq_sum = sum |F_e|^2 over them (host).  The
+ * block keeps each row element's field as the start of its next implicit
+ * solve.                                                                     */
+RADB200_API int radb200_relax_rows_step(int64_t handle, const double *d_M, double prec,
+                            double *d_Mp_rows, double *d_F_rows, double *d_H_rows,
+                            double *sq_sum);
+/* Device blocks are kept for reuse when released: those above 128 MB
+ * (matrices, factors) up to RADB200_BUFCACHE_GB (environment; default 40% of
+ * the device's memory, 0 = off), so that repeated create / free cycles do
+ * not unmap and remap tens of GB each time; smaller ones by power-of-two
+ * class up to RADB200_SMALLCACHE_GB (default 2).  No counterpart in the
+ * reference.  This call returns every kept block to the driver.             */
 RADB200_API int radb200_release_cached_memory(void);
 /* Save / restore the device state of an interaction (the solution state that
  * UtiDmp / UtiDmpPrs would carry across processes, radintrc.cpp:1516,1946 of

@@ -37,6 +37,8 @@ def lib():
         L.radb200_field_dev.argtypes = [_vp, C.c_void_p, _i64, C.c_int, C.c_int, C.c_void_p]
         L.radb200_intrc_create.argtypes = [_vp, _vp, _vp, C.c_int, C.POINTER(C.c_int64)]
         L.radb200_intrc_free.argtypes = [_i64]
+        L.radb200_intrc_create_rows.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]
+        L.radb200_relax_rows_step.argtypes = [_i64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, _dp]
         L.radb200_intrc_save.argtypes = [_i64, C.c_void_p, _i64, C.POINTER(C.c_int64)]
         L.radb200_intrc_restore.argtypes = [_vp, _vp, _vp, C.c_int, C.c_void_p, _i64, C.POINTER(C.c_int64)]
         L.radb200_intrc_size.argtypes = [_i64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]

@@ -52,10 +52,11 @@ __device__ __forceinline__ void pair_block(const GeomView &g, const int *elem_sr
       out[3 * a + b] = rowT_i[3 * a] * B[b] + rowT_i[3 * a + 1] * B[3 + b] + rowT_i[3 * a + 2] * B[6 + b];
 }
 
+// rows: the nr observers of obs / rowT; columns: all n source elements
 template <typename OutT>
 __global__ void __launch_bounds__(256) assemble_kernel(GeomView g, const int *__restrict__ elem_src,
                                                        const double *__restrict__ obs, const double *__restrict__ rowT,
-                                                       int n, int ld, OutT *__restrict__ N)
+                                                       int nr, int n, int ld, OutT *__restrict__ N)
 {
   __shared__ OutT tile[3 * ATI][3 * ATJ + 1];
   int ti = threadIdx.x / ATJ, tj = threadIdx.x % ATJ;
@@ -64,7 +65,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(GeomView g, const int *__
   double blk[9];
 #pragma unroll
   for (int k = 0; k < 9; k++) blk[k] = 0.0;
-  if (i < n && j < n) {
+  if (i < nr && j < n) {
     V3<double> o = mk3<double>(__ldg(obs + 3 * i), __ldg(obs + 3 * i + 1), __ldg(obs + 3 * i + 2));
     double R[9];
 #pragma unroll
@@ -76,30 +77,30 @@ __global__ void __launch_bounds__(256) assemble_kernel(GeomView g, const int *__
 #pragma unroll
     for (int b = 0; b < 3; b++) tile[3 * ti + a][3 * tj + b] = (OutT)blk[3 * a + b];
   __syncthreads();
-  int n3 = 3 * n;
+  const int r3 = 3 * nr, n3 = 3 * n;
   for (int e = threadIdx.x; e < 3 * ATI * 3 * ATJ; e += blockDim.x) {
     int r = e / (3 * ATJ), c = e % (3 * ATJ);
     int gr = 3 * i0 + r, gc = 3 * j0 + c;
-    if (gr < n3 && gc < n3) N[(size_t)gr * ld + gc] = tile[r][c];
+    if (gr < r3 && gc < n3) N[(size_t)gr * ld + gc] = tile[r][c];
   }
 }
 
-int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int n, int ld,
+int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int nr, int n, int ld,
                     float *N32, double *N64, cudaStream_t st)
 {
-  dim3 grid((n + ATJ - 1) / ATJ, (n + ATI - 1) / ATI);
+  dim3 grid((n + ATJ - 1) / ATJ, (nr + ATI - 1) / ATI);
   if (grid.y > 65535) { set_error("too many elements for one assembly grid"); return RADB200_E_ARG; }
   if (N64) {
-    assemble_kernel<double><<<grid, 256, 0, st>>>(g, elem_src, obs, rowT, n, ld, N64);
+    assemble_kernel<double><<<grid, 256, 0, st>>>(g, elem_src, obs, rowT, nr, n, ld, N64);
     RB_TRY(check_launch("assemble_kernel<double>"));
   }
   if (N32) {
     if (N64) {
       // FP32 copy rounded from the FP64 matrix (one rounding, like the reference)
-      size_t tot = (size_t)3 * n * ld;
+      size_t tot = (size_t)3 * nr * ld;
       RB_TRY(launch_round_f32(N64, N32, tot, st));
     } else {
-      assemble_kernel<float><<<grid, 256, 0, st>>>(g, elem_src, obs, rowT, n, ld, N32);
+      assemble_kernel<float><<<grid, 256, 0, st>>>(g, elem_src, obs, rowT, nr, n, ld, N32);
       RB_TRY(check_launch("assemble_kernel<float>"));
     }
   }

@@ -522,7 +522,18 @@ static DBuf g_fld_pts, g_fld_out, g_fld_scratch;
 // synchronizing free per call; the library is not reentrant)
 static DevGeom g_fld_geom;
 
+// interactions over all rows; a row block only serves radb200_relax_rows_step
 Intrc *find_intrc(int64_t h)
+{
+  auto it = g_intrc.find(h);
+  if (it == g_intrc.end()) { set_error("unknown interaction handle %lld", (long long)h); return nullptr; }
+  if (it->second->nr != it->second->n) {
+    set_error("interaction %lld is a row block: only radb200_relax_rows_step and radb200_intrc_free take it", (long long)h);
+    return nullptr;
+  }
+  return it->second.get();
+}
+static Intrc *find_rows(int64_t h)
 {
   auto it = g_intrc.find(h);
   if (it == g_intrc.end()) { set_error("unknown interaction handle %lld", (long long)h); return nullptr; }
@@ -532,6 +543,7 @@ Intrc *find_intrc(int64_t h)
 int relax_jacobi(Intrc &I, double prec, int max_iter, double omega0, double *status);
 int relax_newton(Intrc &I, double prec, int max_iter, double *status);
 int relax_reset(Intrc &I);
+int relax_rows_step(Intrc &I, const double *M, double prec, double *Mp, double *F, double *sq_sum);
 int direct_solve(Intrc &I, int mode, double rtol, int max_iter, double *status);
 int adjoint_solve(Intrc &I, const double *dLdM, double rtol, int max_iter, double *lambda, double *status);
 int adjoint_grad(Intrc &I, const double *lambda, double *dMr, double *dchi, double *dc, double *dd);
@@ -659,8 +671,10 @@ static int upload_materials(Intrc &I, const RadB200Relax *r)
 
 // assemble = false builds everything but leaves the matrix zero (a restored
 // state fills it)
+// rows [e0, e1) of the observer elements (a row block, radb200_intrc_create_rows);
+// e1 < 0: all of them
 static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, const RadB200Geom *ext, int storage,
-                             int64_t *handle, bool assemble)
+                             int64_t *handle, bool assemble, int e0 = 0, int e1 = -1)
 {
   int fast = (storage & RADB200_ASM_FAST) ? 1 : 0;
   storage &= ~RADB200_ASM_FAST;
@@ -680,6 +694,12 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
   I->n3 = 3 * n;
   I->ld = (I->n3 + 31) / 32 * 32;
   I->storage = storage;
+  if (e1 < 0) e1 = n;
+  if (e0 < 0 || e1 > n || e0 >= e1) { set_error("row block [%d, %d) outside [0, %d)", e0, e1, n); return RADB200_E_ARG; }
+  I->e0 = e0;
+  I->nr = e1 - e0;
+  if (I->nr != n && storage == RADB200_STORE_MIXED) { set_error("row blocks are stored FP32 or FP64"); return RADB200_E_ARG; }
+  const int nr = I->nr;
   PhaseClock pc;
   RB_TRY(I->geom.upload(elems, fast != 0));
   I->fast = fast;
@@ -704,11 +724,12 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
       }
     }
   }
-  RB_TRY(I->obs.upload(obs.data(), obs.size() * sizeof(double)));
-  RB_TRY(I->rowT.upload(rowT.data(), rowT.size() * sizeof(double)));
+  // observers of the rows held (all of them unless a row block)
+  RB_TRY(I->obs.upload(obs.data() + 3 * (size_t)e0, 3 * (size_t)nr * sizeof(double)));
+  RB_TRY(I->rowT.upload(rowT.data() + 9 * (size_t)e0, 9 * (size_t)nr * sizeof(double)));
   {
     uint64_t st = 1469598103934665603ULL;
-    int32_t hdr[3] = {n, storage, fast};
+    int32_t hdr[5] = {n, storage, fast, e0, e1};
     st = fnv1a(st, hdr, sizeof(hdr));
     st = fnv1a(st, obs.data(), obs.size() * sizeof(double));
     st = fnv1a(st, rowT.data(), rowT.size() * sizeof(double));
@@ -720,15 +741,15 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
   RB_TRY(I->elem_src.upload(r->elem_src, 2 * (size_t)n * sizeof(int)));
   RB_TRY(upload_materials(*I, r));
   pc.mark("create: observers, materials");
-  size_t nn = (size_t)I->n3 * I->ld;
+  size_t nn = (size_t)3 * nr * I->ld;
   // mixed: every block in FP32, the near ones also as their FP64 residue
   if (storage == RADB200_STORE_F64) RB_TRY(I->N64.alloc(nn * sizeof(double)));
   if (storage == RADB200_STORE_F32 || storage == RADB200_STORE_MIXED) RB_TRY(I->N32.alloc(nn * sizeof(float)));
   if (I->N64.p) RB_CUDA(cudaMemsetAsync(I->N64.p, 0, nn * sizeof(double)));
   if (I->N32.p) RB_CUDA(cudaMemsetAsync(I->N32.p, 0, nn * sizeof(float)));
   if (assemble)
-    RB_TRY(launch_assemble(I->geom.view(fast), I->elem_src.as<int>(), I->obs.as<double>(), I->rowT.as<double>(), n, I->ld,
-                           I->N32.as<float>(), I->N64.as<double>(), 0));
+    RB_TRY(launch_assemble(I->geom.view(fast), I->elem_src.as<int>(), I->obs.as<double>(), I->rowT.as<double>(), nr, n,
+                           I->ld, I->N32.as<float>(), I->N64.as<double>(), 0));
   pc.mark("create: assembly");
   if (storage == RADB200_STORE_MIXED) RB_TRY(build_near(*I, elems, r, obs.data()));
   pc.mark("create: near pairs");
@@ -741,9 +762,9 @@ static int intrc_create_impl(const RadB200Geom *elems, const RadB200Relax *r, co
     RB_TRY(xg.upload(ext));
     I->has_ext = 1;
     DBuf tmp, scratch;
-    RB_TRY(tmp.alloc(3 * (size_t)n * sizeof(double)));
-    RB_TRY(launch_field(xg.view(fast), I->obs.as<double>(), n, 1, 0, tmp.as<double>(), scratch, 0));
-    RB_TRY(launch_rowtrans_vec(I->rowT.as<double>(), tmp.as<double>(), I->hext.as<double>(), n, 0));
+    RB_TRY(tmp.alloc(3 * (size_t)nr * sizeof(double)));
+    RB_TRY(launch_field(xg.view(fast), I->obs.as<double>(), nr, 1, 0, tmp.as<double>(), scratch, 0));
+    RB_TRY(launch_rowtrans_vec(I->rowT.as<double>(), tmp.as<double>(), I->hext.as<double>(), nr, 0));
   }
   RB_TRY(I->M.alloc(vb)); RB_TRY(I->H.alloc(vb)); RB_TRY(I->Mp.alloc(vb)); RB_TRY(I->F.alloc(vb));
   RB_CUDA(cudaMemset(I->M.p, 0, vb)); RB_CUDA(cudaMemset(I->H.p, 0, vb));
@@ -762,6 +783,24 @@ int radb200_intrc_create(const RadB200Geom *elems, const RadB200Relax *r, const 
   return intrc_create_impl(elems, r, ext, storage, handle, true);
 }
 
+int radb200_intrc_create_rows(const RadB200Geom *elems, const RadB200Relax *r, const RadB200Geom *ext, int storage,
+                              int32_t e0, int32_t e1, int64_t *handle)
+{
+  if (e1 < 0) { set_error("bad row block"); return RADB200_E_ARG; }
+  return intrc_create_impl(elems, r, ext, storage, handle, true, e0, e1);
+}
+
+int radb200_relax_rows_step(int64_t handle, const double *d_M, double prec, double *d_Mp_rows, double *d_F_rows,
+                            double *d_H_rows, double *sq_sum)
+{
+  Intrc *I = find_rows(handle);
+  if (!I) return RADB200_E_HANDLE;
+  if (!d_M || !d_Mp_rows || !d_F_rows || !sq_sum || !(prec > 0)) { set_error("bad arguments"); return RADB200_E_ARG; }
+  RB_TRY(relax_rows_step(*I, d_M, prec, d_Mp_rows, d_F_rows, sq_sum));
+  if (d_H_rows) RB_CUDA(cudaMemcpy(d_H_rows, I->H.p, 3 * (size_t)I->nr * sizeof(double), cudaMemcpyDeviceToDevice));
+  return 0;
+}
+
 int radb200_intrc_load(const RadB200Relax *r, const float *N, const double *h_ext, int64_t *handle)
 {
   if (!r || !N || !handle || r->n_elem <= 0 || !r->mat_kind || !r->mat) { set_error("bad arguments"); return RADB200_E_ARG; }
@@ -769,6 +808,7 @@ int radb200_intrc_load(const RadB200Relax *r, const float *N, const double *h_ex
   std::unique_ptr<Intrc> I(new Intrc());
   const int n = r->n_elem;
   I->n = n;
+  I->nr = n;
   I->n3 = 3 * n;
   I->ld = (I->n3 + 31) / 32 * 32;
   I->storage = RADB200_STORE_F32;

@@ -185,6 +185,8 @@ struct NearView {
 // ---- interaction state -------------------------------------------------------
 struct Intrc {
   int n = 0;        // elements
+  int e0 = 0;       // first observer row held (row blocks; 0 otherwise)
+  int nr = 0;       // observer rows held: n, or e1 - e0 for a row block
   int n3 = 0;       // 3n
   int ld = 0;       // padded leading dimension of N (multiple of 32)
   int storage = 0;
@@ -289,7 +291,7 @@ int tc_error_flag(int *flag);  // 2 when a tensor-core CTA hit its wait limit
 // ---- kernels (launch wrappers) ---------------------------------------------
 int launch_field(const GeomView &g, const double *d_pts, int64_t npts, int what, int precision,
                  double *d_out, DBuf &scratch, cudaStream_t st);
-int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int n,
+int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int nr, int n,
                     int ld, float *N32, double *N64, cudaStream_t st);
 int launch_rowtrans_vec(const double *rowT, const double *in, double *out, int n, cudaStream_t st);
 // mesh form of an all-tetrahedron geometry from its tetrahedron records

@@ -862,14 +862,24 @@ int lu_precond_transposed(Intrc &I, double *x, cudaStream_t st) { return lu_appl
 struct LinOp : Op {
   Intrc &I;
   double *tmp;
+  double t_mv = 0.0, t_pc = 0.0;  // seconds in products / sweeps (RADB200_TIMING only)
   LinOp(Intrc &i, double *t) : I(i), tmp(t) {}
   int apply(const double *v, double *out) override
   {
+    const double t0 = timing_on() ? (cudaDeviceSynchronize(), now_s()) : 0.0;
     RB_TRY(run_matvec(I, v, nullptr, 1.0, tmp, 0));
     apply_A_kernel<<<(I.n + 127) / 128, 128>>>(v, tmp, I.mat.as<double>(), I.n, out);
-    return check_launch("apply_A_kernel");
+    RB_TRY(check_launch("apply_A_kernel"));
+    if (t0 > 0.0) { cudaDeviceSynchronize(); t_mv += now_s() - t0; }
+    return 0;
   }
-  int precond(double *v) override { return lu_precond(I, v, 0); }
+  int precond(double *v) override
+  {
+    const double t0 = timing_on() ? (cudaDeviceSynchronize(), now_s()) : 0.0;
+    RB_TRY(lu_precond(I, v, 0));
+    if (t0 > 0.0) { cudaDeviceSynchronize(); t_pc += now_s() - t0; }
+    return 0;
+  }
 };
 
 int lu_build(Intrc &I, int mode, double *factor_seconds)
@@ -931,7 +941,9 @@ int direct_solve(Intrc &I, int mode, double rtol, int max_iter, double *status)
   auto t0 = std::chrono::steady_clock::now();
   const int n3 = I.n3, ld = I.ld;
   double tf = 0.0;
+  PhaseClock pc;
   RB_TRY(lu_build(I, mode, &tf));
+  pc.mark("solve: factors");
   RB_TRY(I.work.alloc((size_t)4 * ld * sizeof(double)));
   double *b = I.work.as<double>(), *tmp = b + ld;
   RB_CUDA(cudaMemset(I.work.p, 0, (size_t)4 * ld * sizeof(double)));
@@ -944,6 +956,10 @@ int direct_solve(Intrc &I, int mode, double rtol, int max_iter, double *status)
   int its = 0;
   RB_TRY(gmres(op, n3, ld, b, I.M.as<double>(), rtol, max_iter, 30, &relres, &its, 0));
   RB_CUDA(cudaDeviceSynchronize());
+  if (timing_on())
+    fprintf(stderr, "RADB200_TIMING solve: refinement, %d its: products %.3f ms, sweeps %.3f ms\n", its, 1e3 * op.t_mv,
+            1e3 * op.t_pc);
+  pc.mark("solve: refinement");
   int tri_err = 0;
   RB_TRY(tri_sweep_error(&tri_err));
   if (tri_err) { set_error("direct solve: a triangular sweep timed out waiting for a block"); return RADB200_E_TIMEOUT; }

@@ -119,6 +119,9 @@ __device__ __forceinline__ void near_rows3(const NearView &nv, int e, const doub
 
 // One Jacobi proposal: H = N M + H_ext; per element H' = FindNewH(H - Q_ii M),
 // M' = M(H'); writes Mp, Hn, F = M' - M and per-CTA partial sums of |F|^2.
+// N holds n rows, or the rows of elements e0 .. e0 + n - 1 of a row block
+// (hext, kind, mat, Hn, Mp, F then hold those rows; M is always the full
+// magnetization).
 template <typename MT>
 __global__ void __launch_bounds__(32 * RLX_WARPS) jacobi_kernel(const MT *__restrict__ N, int ld, int n,
                                                                const double *__restrict__ M, const double *__restrict__ hext,
@@ -126,7 +129,8 @@ __global__ void __launch_bounds__(32 * RLX_WARPS) jacobi_kernel(const MT *__rest
                                                                const double *__restrict__ mh,
                                                                double prec_e2, double *__restrict__ Hn,
                                                                double *__restrict__ Mp, double *__restrict__ F,
-                                                               double *__restrict__ part, NearView nv, int exact)
+                                                               double *__restrict__ part, NearView nv, int exact,
+                                                               int e0)
 {
   __shared__ double ssq[RLX_WARPS];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -137,11 +141,13 @@ __global__ void __launch_bounds__(32 * RLX_WARPS) jacobi_kernel(const MT *__rest
     rows3_dot<MT, 2>(N, ld, e, M, h0, h1, h2);
     if (nv.ptr) near_rows3(nv, e, M, h0, h1, h2);
     if (lane == 0) {
+      // row e of a block starting at element e0: its self block is column e0 + e
       double Q[9];
-      const MT *d = N + (size_t)(3 * e) * ld + 3 * e;
+      const int es = e0 + e;
+      const MT *d = N + (size_t)(3 * e) * ld + 3 * es;
       for (int a = 0; a < 3; a++)
         for (int b = 0; b < 3; b++) Q[3 * a + b] = (double)d[(size_t)a * ld + b];
-      double m0 = M[3 * e], m1 = M[3 * e + 1], m2 = M[3 * e + 2];
+      double m0 = M[3 * es], m1 = M[3 * es + 1], m2 = M[3 * es + 2];
       V3<double> Hq = mk3<double>(h0 + hext[3 * e] - (Q[0] * m0 + Q[1] * m1 + Q[2] * m2),
                                   h1 + hext[3 * e + 1] - (Q[3] * m0 + Q[4] * m1 + Q[5] * m2),
                                   h2 + hext[3 * e + 2] - (Q[6] * m0 + Q[7] * m1 + Q[8] * m2));
@@ -304,7 +310,7 @@ static int jacobi_step(Intrc &I, Ctx &c, const MT *N, double prec_e2, double *mi
   jacobi_kernel<MT><<<nb, 32 * RLX_WARPS, 0, c.st>>>(N, I.ld, I.n, I.M.as<double>(), I.hext.as<double>(),
                                                       I.mat_kind.as<int>(), I.mat.as<double>(), I.mh.as<double>(), prec_e2,
                                                       I.H.as<double>(), I.Mp.as<double>(), I.F.as<double>(),
-                                                      c.part.as<double>(), I.near(), exact);
+                                                      c.part.as<double>(), I.near(), exact, 0);
   RB_TRY(check_launch("jacobi_kernel"));
   sum_kernel<<<1, 256, 0, c.st>>>(c.part.as<double>(), nb, c.scal.as<double>());
   RB_TRY(check_launch("sum_kernel"));
@@ -404,8 +410,8 @@ int relax_jacobi(Intrc &I, double prec, int max_iter, double omega0, double *sta
   double loc_prec_e2 = prec_e2 / I.n;
   int bad = 0;
   for (it = 1; it <= max_iter; it++) {
-    if (I.N64.p) RB_TRY(jacobi_step<double>(I, c, I.N64.as<double>(), loc_prec_e2, &misfit));
-    else RB_TRY(jacobi_step<float>(I, c, I.N32.as<float>(), loc_prec_e2, &misfit));
+    if (I.N64.p) RB_TRY(jacobi_step<double>(I, c, I.N64.as<double>(), loc_prec_e2, &misfit, 1));
+    else RB_TRY(jacobi_step<float>(I, c, I.N32.as<float>(), loc_prec_e2, &misfit, 1));
     if (!std::isfinite(misfit)) { set_error("relaxation produced a non-finite misfit"); return RADB200_E_NUMERIC; }
     if (misfit <= prec) {
       // accept the converged proposal (as method 4 stores the new M)
@@ -653,6 +659,34 @@ int relax_newton(Intrc &I, double prec, int max_iter, double *status)
   double mm[2];
   RB_CUDA(cudaMemcpy(mm, c.scal.as<double>(), 2 * sizeof(double), cudaMemcpyDeviceToHost));
   status[0] = misfit; status[1] = mm[0]; status[2] = mm[1]; status[3] = matvecs;
+  return 0;
+}
+
+// One Jacobi proposal of a row block from the full magnetization M (device):
+// Mp and F of its rows, the block's sum of |F_e|^2 to the host.  The implicit
+// per-element solve stops at prec^2 / n like relax_jacobi's.
+int relax_rows_step(Intrc &I, const double *M, double prec, double *Mp, double *F, double *sq_sum)
+{
+  Ctx c(I);
+  const int nb = grid_elems(I.nr);
+  RB_TRY(c.part.alloc((size_t)nb * sizeof(double)));
+  RB_TRY(c.scal.alloc(64 * sizeof(double)));
+  const double loc = prec * prec / I.n;
+  const int *kind = I.mat_kind.as<int>() + I.e0;
+  const double *mat = I.mat.as<double>() + (size_t)I.e0 * RADB200_MAT_STRIDE;
+  if (I.N64.p)
+    jacobi_kernel<double><<<nb, 32 * RLX_WARPS, 0, c.st>>>(I.N64.as<double>(), I.ld, I.nr, M, I.hext.as<double>(), kind, mat,
+                                                           I.mh.as<double>(), loc, I.H.as<double>(), Mp, F,
+                                                           c.part.as<double>(), NearView(), 1, I.e0);
+  else
+    jacobi_kernel<float><<<nb, 32 * RLX_WARPS, 0, c.st>>>(I.N32.as<float>(), I.ld, I.nr, M, I.hext.as<double>(), kind, mat,
+                                                          I.mh.as<double>(), loc, I.H.as<double>(), Mp, F,
+                                                          c.part.as<double>(), NearView(), 1, I.e0);
+  RB_TRY(check_launch("jacobi_kernel"));
+  sum_kernel<<<1, 256, 0, c.st>>>(c.part.as<double>(), nb, c.scal.as<double>());
+  RB_TRY(check_launch("sum_kernel"));
+  RB_CUDA(cudaMemcpyAsync(sq_sum, c.scal.as<double>(), sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  RB_CUDA(cudaStreamSynchronize(c.st));
   return 0;
 }
 
