@@ -816,10 +816,23 @@ static int lu_solve_direct(Intrc &I, int transposed, double *x, cudaStream_t st)
 // and more, the ~4 n / 128 small launches of the block sweeps are captured
 // once per factorization into a CUDA graph on a fixed buffer and replayed:
 // one launch per application.
+// RADB200_LU_GRAPH=0 launches the sweeps directly, never capturing them: a
+// per-kernel profiler cannot run a launch made into a capturing stream (the
+// kernel only becomes a graph node there), so launch lists are taken with it.
+static bool lu_graph_enabled()
+{
+  static int on = -1;
+  if (on < 0) {
+    const char *e = getenv("RADB200_LU_GRAPH");
+    on = (e && atoi(e) == 0) ? 0 : 1;
+  }
+  return on == 1;
+}
+
 static int lu_apply(Intrc &I, int transposed, double *x, cudaStream_t st)
 {
   // small systems: a few applications per factorization do not repay a capture
-  if (I.n3 < 64 * LU_NB) return lu_solve_direct(I, transposed, x, st);
+  if (I.n3 < 64 * LU_NB || !lu_graph_enabled()) return lu_solve_direct(I, transposed, x, st);
   cudaGraphExec_t &ex = I.lu_graph[transposed];
   if (!ex) {
     RB_TRY(I.lu_gx.alloc((size_t)I.ld * sizeof(double)));
