@@ -173,16 +173,17 @@ __global__ void chunk_reduce_kernel(const double *__restrict__ part, int nc, int
 // shared-memory broadcasts.
 constexpr int TET_TILE = 32;
 constexpr int TET_U = TET_REC_FIELD + 21 + 3;  // record, Minv V sM (21), M (3)
+constexpr int TET_UF = 18;                     // float copies: edge lengths (6), face normals (12)
 
 template <typename T>
-__device__ __forceinline__ void tet_unit(const double *su, V3<double> P, int what, double *acc)
+__device__ __forceinline__ void tet_unit(const double *su, const float *suf, V3<double> P, int what, double *acc)
 {
   const double *Tr = su + TET_REC_FIELD, *M = Tr + 21;
   double dx = P.x - Tr[9], dy = P.y - Tr[10], dz = P.z - Tr[11];
   V3<double> q = mk3<double>(Tr[0] * dx + Tr[1] * dy + Tr[2] * dz, Tr[3] * dx + Tr[4] * dy + Tr[5] * dz,
                              Tr[6] * dx + Tr[7] * dy + Tr[8] * dz);
   double h[3];
-  int in = tet_fast<T, false, true>(su, q, h);
+  int in = tet_fast<T, false, true>(su, q, h, suf);
   V3<double> f;
   if (what == 2) f = in ? mk3<double>(M[0], M[1], M[2]) : mk3<double>(0, 0, 0);
   else {
@@ -202,6 +203,7 @@ __global__ void __launch_bounds__(128) field_tet_kernel(GeomView g, const double
                                                         double *__restrict__ out, int ub, int ue, int chunk, int accumulate)
 {
   __shared__ double su[TET_TILE * TET_U];
+  __shared__ float suf[TET_TILE * TET_UF];
   const int tid = threadIdx.x;
   const int64_t i0 = (int64_t)blockIdx.x * (128 * PPT) + tid, i1 = PPT == 2 ? i0 + 128 : npts;
   const int u0 = ub + blockIdx.y * chunk, u1 = min(ue, u0 + chunk);
@@ -221,20 +223,26 @@ __global__ void __launch_bounds__(128) field_tet_kernel(GeomView g, const double
       else v = __ldg(g.poly + (size_t)un.y * RADB200_POLY_STRIDE + 3 + (f - TET_REC_FIELD - 21));
       su[e] = v;
     }
+    if (sizeof(T) == 4)
+      for (int e = tid; e < cnt * TET_UF; e += 128) {
+        const int k = e / TET_UF, f = e - k * TET_UF;
+        const int4 un = __ldg(g.units + base + k);
+        suf[e] = (float)__ldg(g.tetrec + (size_t)__ldg(g.tetidx + un.y) * TET_REC_FIELD + 12 + f);  // rec + 12: lengths, then normals
+      }
     __syncthreads();
     if (TPI == 2) {
       int k = 0;
       for (; k + 1 < cnt; k += 2) {
         double b0[3] = {0, 0, 0};
-        tet_unit<T>(su + k * TET_U, P0, what, a0);
-        tet_unit<T>(su + (k + 1) * TET_U, P0, what, b0);
+        tet_unit<T>(su + k * TET_U, suf + k * TET_UF, P0, what, a0);
+        tet_unit<T>(su + (k + 1) * TET_U, suf + (k + 1) * TET_UF, P0, what, b0);
         a0[0] += b0[0]; a0[1] += b0[1]; a0[2] += b0[2];
       }
-      if (k < cnt) tet_unit<T>(su + k * TET_U, P0, what, a0);
+      if (k < cnt) tet_unit<T>(su + k * TET_U, suf + k * TET_UF, P0, what, a0);
     } else {
       for (int k = 0; k < cnt; k++) {
-        tet_unit<T>(su + k * TET_U, P0, what, a0);
-        if (PPT == 2) tet_unit<T>(su + k * TET_U, P1, what, a1);
+        tet_unit<T>(su + k * TET_U, suf + k * TET_UF, P0, what, a0);
+        if (PPT == 2) tet_unit<T>(su + k * TET_U, suf + k * TET_UF, P1, what, a1);
       }
     }
   }

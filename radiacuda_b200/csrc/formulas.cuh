@@ -511,10 +511,15 @@ __device__ __forceinline__ double rd_rec(const double *p)
   return __ldg(p);
 }
 
-// SMEM: the record lives in shared memory (plain loads instead of __ldg)
+// SMEM: the record lives in shared memory (plain loads instead of __ldg).
+// recf (T = float, optional): the edge lengths (6) and face normals (12) of
+// the record already rounded to float, so that a pair reads them without a
+// conversion each (the same values as T(record entry)).
 template <typename T, bool TENSOR, bool SMEM = false>
-__device__ __forceinline__ int tet_fast(const double *__restrict__ rec, V3<double> q, double *out)
+__device__ __forceinline__ int tet_fast(const double *__restrict__ rec, V3<double> q, double *out,
+                                        const float *__restrict__ recf = nullptr)
 {
+  const bool fl = sizeof(T) == 4 && recf != nullptr;
   const double C = 1.0 / (4.0 * 3.141592653589793238);
   T rx[4], ry[4], rz[4], R[4];
 #pragma unroll
@@ -536,7 +541,7 @@ __device__ __forceinline__ int tet_fast(const double *__restrict__ rec, V3<doubl
 #pragma unroll
   for (int e = 0; e < 6; e++) {
     const int a = tet_edge_a(e), b = tet_edge_b(e);
-    T l = T(rd_rec<SMEM>(rec + 12 + e));
+    T l = fl ? T(recf[e]) : T(rd_rec<SMEM>(rec + 12 + e));
     T D;
     if (d[e] >= T(0)) D = R[a] * R[b] + d[e];
     else {
@@ -556,7 +561,10 @@ __device__ __forceinline__ int tet_fast(const double *__restrict__ rec, V3<doubl
 #pragma unroll
   for (int f = 0; f < 4; f++) {
     const int a = tet_face_a(f), b = tet_face_b(f), c = tet_face_c(f);
-    T num = rx[a] * T(rd_rec<SMEM>(rec + 18 + 3 * f)) + ry[a] * T(rd_rec<SMEM>(rec + 19 + 3 * f)) + rz[a] * T(rd_rec<SMEM>(rec + 20 + 3 * f));
+    const T m0 = fl ? T(recf[6 + 3 * f]) : T(rd_rec<SMEM>(rec + 18 + 3 * f));
+    const T m1 = fl ? T(recf[7 + 3 * f]) : T(rd_rec<SMEM>(rec + 19 + 3 * f));
+    const T m2 = fl ? T(recf[8 + 3 * f]) : T(rd_rec<SMEM>(rec + 20 + 3 * f));
+    T num = rx[a] * m0 + ry[a] * m1 + rz[a] * m2;
     T den = R[a] * R[b] * R[c] + d[tet_pair(a, b)] * R[c] + d[tet_pair(a, c)] * R[b] + d[tet_pair(b, c)] * R[a];
     double om = 2.0 * (double)atan2T(-num, den);
     omega_tot += om;
