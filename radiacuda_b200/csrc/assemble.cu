@@ -85,9 +85,111 @@ __global__ void __launch_bounds__(256) assemble_kernel(GeomView g, const int *__
   }
 }
 
+// Sources that are all tetrahedra in the vertex/edge form with one image
+// each (a mesh without symmetries): the CTA's 32 source records (tensor
+// record and image transform) are staged in shared memory once, instead of
+// every pair walking elem_src -> poly_info -> tetidx -> record in global
+// memory; the arithmetic and its order are pair_block's, so the blocks are
+// the same to the bit.
+constexpr int AT_U = TET_REC_TENSOR + 21;  // record, image transform (Minv, V, s M)
+union AssembleTetSmem {
+  double su[ATJ * AT_U];
+  float t32[3 * ATI][3 * ATJ + 1];
+  double t64[3 * ATI][3 * ATJ + 1];
+};
+
+template <typename OutT>
+__global__ void __launch_bounds__(256) assemble_tet_kernel(GeomView g, const int *__restrict__ elem_src,
+                                                           const double *__restrict__ obs, const double *__restrict__ rowT,
+                                                           int nr, int n, int ld, OutT *__restrict__ N)
+{
+  __shared__ AssembleTetSmem sm;
+  __shared__ int s_rec[ATJ], s_trf[ATJ];
+  const int tid = threadIdx.x;
+  const int ti = tid / ATJ, tj = tid % ATJ;
+  const int i0 = blockIdx.y * ATI, j0 = blockIdx.x * ATJ;
+  if (tid < ATJ) {
+    const int j = j0 + tid;
+    int rec = 0, trf = 0;
+    if (j < n) {
+      const int idx = __ldg(elem_src + 2 * j + 1);
+      rec = __ldg(g.tetidx + idx);
+      trf = __ldg(g.poly_info + 4 * idx + 2);
+    }
+    s_rec[tid] = rec;
+    s_trf[tid] = trf;
+  }
+  __syncthreads();
+  for (int e = tid; e < ATJ * AT_U; e += blockDim.x) {
+    const int k = e / AT_U, f = e - k * AT_U;
+    double v = 0.0;
+    if (j0 + k < n)
+      v = f < TET_REC_TENSOR ? __ldg(g.tetrec + (size_t)s_rec[k] * TET_REC_TENSOR + f)
+                             : __ldg(g.trf + (size_t)s_trf[k] * RADB200_TRF_STRIDE + (f - TET_REC_TENSOR));
+    sm.su[e] = v;
+  }
+  __syncthreads();
+  const int i = i0 + ti, j = j0 + tj;
+  double blk[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) blk[k] = 0.0;
+  if (i < nr && j < n) {
+    const double *rec = sm.su + tj * AT_U, *Tr = rec + TET_REC_TENSOR;
+    const double ox = __ldg(obs + 3 * i), oy = __ldg(obs + 3 * i + 1), oz = __ldg(obs + 3 * i + 2);
+    const double dx = ox - Tr[9], dy = oy - Tr[10], dz = oz - Tr[11];
+    const V3<double> q = mk3<double>(Tr[0] * dx + Tr[1] * dy + Tr[2] * dz, Tr[3] * dx + Tr[4] * dy + Tr[5] * dz,
+                                     Tr[6] * dx + Tr[7] * dy + Tr[8] * dz);
+    double Q[9], B[9];
+    tet_fast<double, true, true>(rec, q, Q);
+    const double *F = Tr + 12;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double f0 = F[3 * a], f1 = F[3 * a + 1], f2 = F[3 * a + 2];
+#pragma unroll
+      for (int b = 0; b < 3; b++) B[3 * a + b] = 0.0 + (f0 * Q[b] + f1 * Q[3 + b] + f2 * Q[6 + b]);
+    }
+    const double *R = rowT + 9 * (size_t)i;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double r0 = __ldg(R + 3 * a), r1 = __ldg(R + 3 * a + 1), r2 = __ldg(R + 3 * a + 2);
+#pragma unroll
+      for (int b = 0; b < 3; b++) blk[3 * a + b] = r0 * B[b] + r1 * B[3 + b] + r2 * B[6 + b];
+    }
+  }
+  __syncthreads();  // every pair done with the staged records: the tile reuses them
+  OutT(*tile)[3 * ATJ + 1] = reinterpret_cast<OutT(*)[3 * ATJ + 1]>(sizeof(OutT) == 4 ? (void *)sm.t32 : (void *)sm.t64);
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) tile[3 * ti + a][3 * tj + b] = (OutT)blk[3 * a + b];
+  __syncthreads();
+  const int r3 = 3 * nr, n3 = 3 * n;
+  for (int e = tid; e < 3 * ATI * 3 * ATJ; e += blockDim.x) {
+    const int r = e / (3 * ATJ), c = e % (3 * ATJ);
+    const int gr = 3 * i0 + r, gc = 3 * j0 + c;
+    if (gr < r3 && gc < n3) N[(size_t)gr * ld + gc] = tile[r][c];
+  }
+}
+
 int launch_assemble(const GeomView &g, const int *elem_src, const double *obs, const double *rowT, int nr, int n, int ld,
                     float *N32, double *N64, cudaStream_t st)
 {
+  if (g.fast && g.all_tets && g.tet_single) {
+    dim3 grid((n + ATJ - 1) / ATJ, (nr + ATI - 1) / ATI);
+    if (grid.y > 65535) { set_error("too many elements for one assembly grid"); return RADB200_E_ARG; }
+    if (N64) {
+      assemble_tet_kernel<double><<<grid, 256, 0, st>>>(g, elem_src, obs, rowT, nr, n, ld, N64);
+      RB_TRY(check_launch("assemble_tet_kernel<double>"));
+    }
+    if (N32) {
+      if (N64) RB_TRY(launch_round_f32(N64, N32, (size_t)3 * nr * ld, st));
+      else {
+        assemble_tet_kernel<float><<<grid, 256, 0, st>>>(g, elem_src, obs, rowT, nr, n, ld, N32);
+        RB_TRY(check_launch("assemble_tet_kernel<float>"));
+      }
+    }
+    return 0;
+  }
   dim3 grid((n + ATJ - 1) / ATJ, (nr + ATI - 1) / ATI);
   if (grid.y > 65535) { set_error("too many elements for one assembly grid"); return RADB200_E_ARG; }
   if (N64) {

@@ -426,6 +426,7 @@ int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs, bool mesh)
 {
   RB_TRY(validate_geom(G));
   all_tets = 0;
+  tet_single = 0;
   if (G->n_poly > 0) {
     HostTopo h;
     PhaseClock pc;
@@ -445,6 +446,8 @@ int DevGeom::upload(const RadB200Geom *G, bool tensor_coeffs, bool mesh)
     RB_TRY(tetidx.upload(h.tetidx.data(), h.tetidx.size() * sizeof(int)));
     RB_TRY(tetrec.upload(h.tetrec.data(), h.tetrec.size() * sizeof(double)));
     all_tets = std::all_of(h.tetidx.begin(), h.tetidx.end(), [](int t) { return t >= 0; }) ? 1 : 0;
+    tet_single = all_tets && G->n_rec == 0 && G->n_arc == 0 && G->n_bkg == 0;
+    for (int i = 0; i < G->n_poly && tet_single; i++) tet_single = G->poly_info[4 * i + 3] == 1;
     m_tiles = m_groups = 0;
     // field geometry of an all-tetrahedron model: the mesh form (unique edges and faces)
     pc.mark("geometry: topology upload");
@@ -501,6 +504,7 @@ GeomView DevGeom::view(int fast) const
   v.tetidx = tetidx.as<int>();
   v.tetrec = tetrec.as<double>();
   v.all_tets = all_tets;
+  v.tet_single = tet_single;
   v.mesh.n_tiles = m_tiles;
   v.mesh.tile = m_tile.as<int4>();
   v.mesh.mv = m_v.as<double>();

@@ -149,6 +149,7 @@ struct GeomView {
   const int *tetidx;  // per polyhedron: tetrahedron record or -1
   const double *tetrec;
   int all_tets;       // every polyhedron has a tetrahedron record
+  int tet_single;     // ... and the sources are only those tetrahedra, one image each
   int fast;           // 1: evaluate polyhedra in the vertex/edge form
   MeshView mesh;      // all-tetrahedron models: unique edges and faces (n_tiles 0: none)
 };
@@ -162,7 +163,7 @@ struct DevGeom {
   int m_tiles = 0, m_groups = 0;
   int n_units = 0, n_rec = 0, n_poly = 0;
   int ustart[5] = {0, 0, 0, 0, 0};
-  int all_tets = 0;
+  int all_tets = 0, tet_single = 0;
   Guard g{0, 0, 0};
   int upload(const RadB200Geom *G, bool tensor_coeffs = false, bool mesh = true);
   GeomView view(int fast = 0) const;
