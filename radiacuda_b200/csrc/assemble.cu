@@ -99,7 +99,7 @@ union AssembleTetSmem {
 };
 
 template <typename OutT>
-__global__ void __launch_bounds__(256) assemble_tet_kernel(GeomView g, const int *__restrict__ elem_src,
+__global__ void __launch_bounds__(256, 3) assemble_tet_kernel(GeomView g, const int *__restrict__ elem_src,
                                                            const double *__restrict__ obs, const double *__restrict__ rowT,
                                                            int nr, int n, int ld, OutT *__restrict__ N)
 {

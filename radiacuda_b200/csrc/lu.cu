@@ -586,6 +586,7 @@ __device__ __forceinline__ void st_release_s32(int *p, int v)
 template <typename T> struct RowSlice;
 template <> struct RowSlice<float> {
   float4 v;
+  __device__ __forceinline__ void set(float4 q) { v = q; }
   __device__ __forceinline__ void load(const float *row, int lane) { v = __ldg(reinterpret_cast<const float4 *>(row) + lane); }
   __device__ __forceinline__ void zero() { v = make_float4(0.f, 0.f, 0.f, 0.f); }
   __device__ __forceinline__ double dot(const double *xs, int lane) const
@@ -596,6 +597,7 @@ template <> struct RowSlice<float> {
 };
 template <> struct RowSlice<double> {
   double2 a, b;
+  __device__ __forceinline__ void set(float4) {}  // unused: inverses are staged for float factors only
   __device__ __forceinline__ void load(const double *row, int lane)
   {
     a = __ldg(reinterpret_cast<const double2 *>(row) + lane);
@@ -616,6 +618,8 @@ __global__ void __launch_bounds__(256, 2) tri_sweep_kernel(const T *__restrict__
                                                         double *x, int *sync, int *err)
 {
   constexpr int NR = tri_rows<T>(), NB = LU_NB / (8 * NR);  // rows per batch, batches
+  constexpr bool STAGE_INV = sizeof(T) == 4;  // Inv_k in shared memory (dynamic, LU_NB^2 floats)
+  extern __shared__ float4 sinv4[];
   __shared__ double xs[LU_NB], acc_s[LU_NB];
   __shared__ int s_t, s_bad;
   const int nblk = (n3 + LU_NB - 1) / LU_NB;
@@ -632,6 +636,15 @@ __global__ void __launch_bounds__(256, 2) tri_sweep_kernel(const T *__restrict__
     // this warp's rows: (warp * NB + batch) * NR + i, accumulated in shared
     // memory by the warp's lane 0 (every row belongs to one warp)
     if (threadIdx.x < LU_NB) acc_s[threadIdx.x] = threadIdx.x < nb ? x[k0 + threadIdx.x] : 0.0;
+    // the diagonal block's inverse, needed last, on the chain's critical path:
+    // staged now (visible after the barriers below), while the chain is
+    // still far from this block
+    if (STAGE_INV)
+      for (int e = threadIdx.x; e < LU_NB * LU_NB / 4; e += blockDim.x) {
+        const int r = e / (LU_NB / 4);
+        sinv4[e] = r < nb ? __ldg(reinterpret_cast<const float4 *>(Inv + (size_t)(k0 + r) * LU_NB) + (e % (LU_NB / 4)))
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
     for (int s = 0; s < t; s++) {
       const int j = UPPER ? nblk - 1 - s : s;
       const int j0 = j * LU_NB, nbj = min(LU_NB, n3 - j0);
@@ -700,7 +713,10 @@ __global__ void __launch_bounds__(256, 2) tri_sweep_kernel(const T *__restrict__
 #pragma unroll
       for (int i = 0; i < NR; i++) {
         const int r = (warp * NB + b) * NR + i;
-        if (r < nb) v[i].load(Inv + (size_t)(k0 + r) * LU_NB, lane);
+        if (STAGE_INV) {
+          const float4 q = sinv4[r * (LU_NB / 4) + lane];
+          v[i].set(q);
+        } else if (r < nb) v[i].load(Inv + (size_t)(k0 + r) * LU_NB, lane);
         else v[i].zero();
       }
 #pragma unroll
@@ -737,6 +753,13 @@ static int tri_sync_alloc(Intrc &I)
 {
   const size_t per = (size_t)(I.n3 + LU_NB - 1) / LU_NB + 1;
   RB_TRY(I.tri_sync.alloc(2 * per * sizeof(int)));
+  static bool attr = false;
+  if (!attr) {
+    const int dyn = LU_NB * LU_NB * (int)sizeof(float);
+    RB_CUDA(cudaFuncSetAttribute(tri_sweep_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    RB_CUDA(cudaFuncSetAttribute(tri_sweep_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    attr = true;
+  }
   if (!g_tri_err.p) {
     RB_TRY(g_tri_err.alloc(sizeof(int)));
     RB_CUDA(cudaMemset(g_tri_err.p, 0, sizeof(int)));
@@ -752,9 +775,12 @@ static int lu_solve_sweeps(const T *A, const T *Linv, const T *Uinv, int n3, int
   const size_t per = (size_t)nblk + 1;
   RB_CUDA(cudaMemsetAsync(sync, 0, 2 * per * sizeof(int), st));
   const int grid = std::min(nblk, 148 * 4);
-  tri_sweep_kernel<T, false><<<grid, 256, 0, st>>>(A, ld, Linv, n3, x, sync, g_tri_err.as<int>());
+  // FP32 factors: the inverses staged in dynamic shared memory (the limit is
+  // raised in tri_sync_alloc, before any capture)
+  const size_t dyn = sizeof(T) == 4 ? (size_t)LU_NB * LU_NB * sizeof(float) : 0;
+  tri_sweep_kernel<T, false><<<grid, 256, dyn, st>>>(A, ld, Linv, n3, x, sync, g_tri_err.as<int>());
   RB_TRY(check_launch("tri_sweep_kernel"));
-  tri_sweep_kernel<T, true><<<grid, 256, 0, st>>>(A, ld, Uinv, n3, x, sync + per, g_tri_err.as<int>());
+  tri_sweep_kernel<T, true><<<grid, 256, dyn, st>>>(A, ld, Uinv, n3, x, sync + per, g_tri_err.as<int>());
   return check_launch("tri_sweep_kernel");
 }
 

@@ -1,7 +1,7 @@
 """Small, self-contained launches of the hot kernels for profiling.
 
     python tests/profile_cases.py field    [--tets N] [--points P] [--precision double|single|fast]
-    python tests/profile_cases.py assemble [--tets N]
+    python tests/profile_cases.py assemble [--tets N]           (vertex/edge form, FP32 storage)
     python tests/profile_cases.py lu       [--tets N] [--mode 0|1]
     python tests/profile_cases.py relax    [--blocks N]
     python tests/profile_cases.py adjoint  [--pairs N] [--points P]
@@ -52,7 +52,7 @@ def main(argv=None):
             B = rad.Fld(m, "b", P, precision=a.precision)
             print("field", P.shape[0], "points", time.perf_counter() - t0, "s", float(np.abs(B).max()))
         elif a.case == "assemble":
-            im = rad.RlxPre(m, storage="f32")
+            im = rad.RlxPre(m, storage="f32", fast=True)
             print("assembly", time.perf_counter() - t0, "s")
         else:
             im = rad.RlxPre(m, storage="f64")
