@@ -326,7 +326,8 @@ constexpr int TM_NST = 4;
 constexpr int TM_STAGE_A = TC_BM * TM_KC * 4;   // 16 KB
 constexpr int TM_STAGE_B = TC_BN * TM_KC * 4;   // 32 KB
 constexpr int TM_STAGE = TM_STAGE_A + TM_STAGE_B;
-constexpr int TM_SMEM = TM_NST * TM_STAGE + 1024;
+constexpr int TM_SMEM_W = 8 * 32 * 32 * 4;  // one 32 x 32 transpose buffer per epilogue warp (XOR-swizzled columns)
+constexpr int TM_SMEM = TM_NST * TM_STAGE + 1024 + TM_SMEM_W;
 
 __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
 {
@@ -368,6 +369,7 @@ __device__ __forceinline__ int tm_wait(uint32_t bar, uint32_t parity)
 }
 
 constexpr int TM_THREADS = 288;  // warps 0-7: epilogue; warp 8: TMA loads and MMAs
+
 
 // Warp-specialised: warp 8 (one lane) streams the chunks of all of the CTA's
 // tiles through the operand stages into two TMEM accumulators (columns
@@ -480,49 +482,70 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
     __syncwarp();
   } else {
     // ---------------- epilogue: warps 0-7 ----------------
+    // Warp (q, hc) owns rows q*32.. of the tile (its TMEM lane quarter) and
+    // the column half hc*128.., in four 32-column slices.  C is read and
+    // written row-contiguous: lane l takes 4 columns, (l % 8) * 4.., of row
+    // (l / 8) of every group of 4 rows, so a warp instruction covers four
+    // full 128-byte lines.  The accumulator rows arrive lane = row
+    // (tcgen05.ld 32x32b) and are turned around through a 32 x 32 shared
+    // buffer per warp in 16-byte groups: group g of row r sits at group
+    // position g ^ (r % 8), so the row-wise group writes and the column-wise
+    // group reads of each 8-lane phase hit all 32 banks once.  The tile's C values are loaded before its
+    // accumulator is waited on.
     const int q = warp & 3, hc = warp >> 2;
-    const int r = q * 32 + lane;
+    float *W = reinterpret_cast<float *>(sbase + TM_NST * TM_STAGE) + warp * 32 * 32;
+    const int lr = lane >> 3, lc = (lane & 7) * 4;
     for (int i = 0; i < my_tiles; i++) {
       const int tile = blockIdx.x + i * gridDim.x;
       int row0, col0;
       tile_rc(tile, tiles_m, tiles_n, row0, col0);
       const int buf = i & 1;
-      const int gr = row0 + r, gcb = col0 + hc * 128;
-      float4 cv[32];
+      const int rbase = row0 + q * 32, cbase = col0 + hc * 128;
+      // C slice sl (8 float4 per thread) for rows rbase + 4 rr + lr, columns cbase + 32 sl + lc ..:
+      // slices 0 and 1 are loaded before the accumulator wait, slice sl + 2
+      // while slice sl is written back
+      auto load_slice = [&](float4 *cs, int sl) {
 #pragma unroll
-      for (int j = 0; j < 32; j++) {
-        int gc = gcb + 4 * j;
-        cv[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (!overwrite && gr < m) {
-          const float *src = C + (size_t)gr * ldc + gc;
-          if (gc + 3 < n) cv[j] = *reinterpret_cast<const float4 *>(src);
-          else if (gc < n) {
-            cv[j].x = src[0];
-            if (gc + 1 < n) cv[j].y = src[1];
-            if (gc + 2 < n) cv[j].z = src[2];
+        for (int rr = 0; rr < 8; rr++) {
+          const int gr = rbase + 4 * rr + lr, gc = cbase + 32 * sl + lc;
+          cs[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (!overwrite && gr < m) {
+            const float *src = C + (size_t)gr * ldc + gc;
+            if (gc + 3 < n) cs[rr] = *reinterpret_cast<const float4 *>(src);
+            else if (gc < n) {
+              cs[rr].x = src[0];
+              if (gc + 1 < n) cs[rr].y = src[1];
+              if (gc + 2 < n) cs[rr].z = src[2];
+            }
           }
         }
-      }
-      if (!tm_wait(smem_u32(&accf[buf]), (uint32_t)((i / 2) & 1))) { timed_out = 1; break; }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      };
+      auto store_slice = [&](const float4 *cs, int sl) {
 #pragma unroll
-      for (int cb = 0; cb < 128; cb += 16) {
-        uint32_t v[16];
-        uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * TC_BN + hc * 128 + cb);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-              "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (gr < m) {
+        for (int h = 0; h < 2; h++) {
+          uint32_t v[16];
+          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * TC_BN + hc * 128 + sl * 32 + h * 16);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+                "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+              : "r"(taddr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-          for (int j4 = 0; j4 < 4; j4++) {
-            const int j = cb / 4 + j4;
-            const int gc = gcb + 4 * j;
-            float4 t = make_float4(__uint_as_float(v[4 * j4]), __uint_as_float(v[4 * j4 + 1]),
-                                   __uint_as_float(v[4 * j4 + 2]), __uint_as_float(v[4 * j4 + 3]));
-            float4 o = overwrite ? t : make_float4(cv[j].x - t.x, cv[j].y - t.y, cv[j].z - t.z, cv[j].w - t.w);
+          for (int c4 = 0; c4 < 4; c4++)
+            *reinterpret_cast<float4 *>(W + lane * 32 + (((h * 4 + c4) ^ (lane & 7)) << 2)) =
+                make_float4(__uint_as_float(v[4 * c4]), __uint_as_float(v[4 * c4 + 1]), __uint_as_float(v[4 * c4 + 2]),
+                            __uint_as_float(v[4 * c4 + 3]));
+        }
+        __syncwarp();
+#pragma unroll
+        for (int rr = 0; rr < 8; rr++) {
+          const int rl = 4 * rr + lr;
+          const float4 t = *reinterpret_cast<const float4 *>(W + rl * 32 + (((lane & 7) ^ (rl & 7)) << 2));
+          const int gr = rbase + rl, gc = cbase + 32 * sl + lc;
+          if (gr < m) {
+            const float4 c4 = cs[rr];
+            const float4 o = overwrite ? t : make_float4(c4.x - t.x, c4.y - t.y, c4.z - t.z, c4.w - t.w);
             float *dst = C + (size_t)gr * ldc + gc;
             if (gc + 3 < n) *reinterpret_cast<float4 *>(dst) = o;
             else if (gc < n) {
@@ -532,7 +555,19 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
             }
           }
         }
-      }
+        __syncwarp();  // the next slice overwrites W
+      };
+      float4 c0[8], c1[8], c2[8], c3[8];
+      load_slice(c0, 0);
+      load_slice(c1, 1);
+      if (!tm_wait(smem_u32(&accf[buf]), (uint32_t)((i / 2) & 1))) { timed_out = 1; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      store_slice(c0, 0);
+      load_slice(c2, 2);
+      store_slice(c1, 1);
+      load_slice(c3, 3);
+      store_slice(c2, 2);
+      store_slice(c3, 3);
       // this thread's reads of the buffer are done: release it to the producer
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acce[buf])) : "memory");
