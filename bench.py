@@ -253,25 +253,36 @@ def run_ours(args, rank, world):
     if not e2e:
         e2e = [float("nan")]
 
-    # roofline of the LU trailing update (TF32 tcgen05 GEMM, K = 768): its
-    # flops (2 m^2 K per launch) over the event-timed launch durations,
-    # against the dense TF32 rate (half the measured bf16 rate); the HBM side
-    # (C read + written, panels once) beside it
+    # roofline of the LU trailing update (tcgen05 GEMM, K = 768): its flops
+    # (2 m^2 K per launch) over the event-timed launch durations, against the
+    # dense rate of its operand type (FP16: the measured bf16 rate; TF32: half
+    # of it); the HBM side (C read + written, panels once) beside it
     peaks = _peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     # the trailing update runs inside a seconds-long step: the sustained rate
     # (a GEMM loop under the power cap) is its denominator
     bf16 = peaks.get("bf16_tflops_sustained")
-    tf32_peak = float(bf16) / 2.0 if bf16 else 1400.0 / 2.0
+    # which GEMM the LU ran: 3 = TMA-fed with scaled FP16 operands (the dense
+    # FP16 rate equals the bf16 one), 2 = TMA-fed with TF32 operands (half of it)
+    L.radb200_tc_selftest.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    tc_state, tc_err = C.c_int(0), C.c_double(0.0)
+    L.radb200_tc_selftest(C.byref(tc_state), C.byref(tc_err))
+    f16_ops = tc_state.value == 3
+    div = 1.0 if f16_ops else 2.0
+    tf32_peak = float(bf16) / div if bf16 else 1400.0 / div
     upd_tflops = upd_f.value / max(upd_s.value, 1e-30) / 1e12
     upd_gbs = upd_b.value / max(upd_s.value, 1e-30) / 1e9
     upd_bytes_per_launch = upd_b.value / max(upd_n.value, 1)
-    roof_upd = {"kernel": "tc_update_tma_kernel (LU trailing update A22 -= L21 U12, K = 768)", "bound": "tensor",
+    roof_upd = {"kernel": ("tc_update_tma_kernel<FP16 operands> (LU trailing update A22 -= L21 U12, K = 768; "
+                           "operands scaled by powers of two, FP32 accumulation)" if f16_ops else
+                           "tc_update_tma_kernel<TF32 operands> (LU trailing update A22 -= L21 U12, K = 768)"),
+                "bound": "tensor",
                 "achieved": round(upd_tflops, 1), "peak": round(tf32_peak, 1), "unit": "TFLOP/s",
                 "frac": round(upd_tflops / tf32_peak, 4),
-                "peak_source": ("measured sustained bf16 dense / 2 (TF32 runs at half the bf16 rate)" if bf16 else
-                                "fallback sustained bf16 / 2"),
-                "frac_of_burst": round(upd_tflops / (float(peaks.get("bf16_tflops", 1590.0)) / 2.0), 4),
+                "peak_source": (("measured sustained bf16 dense (the FP16 rate)" if f16_ops else
+                                 "measured sustained bf16 dense / 2 (TF32 runs at half the bf16 rate)") if bf16 else
+                                "fallback sustained bf16" + ("" if f16_ops else " / 2")),
+                "frac_of_burst": round(upd_tflops / (float(peaks.get("bf16_tflops", 1590.0)) / div), 4),
                 "hbm_achieved_gbs": round(upd_gbs, 1), "hbm_peak_gbs": hbm, "hbm_frac": round(upd_gbs / hbm, 4),
                 "traffic": round(TC_TRAFFIC_OVER_ALGORITHMIC * upd_bytes_per_launch),
                 "traffic_note": "ncu dram bytes / algorithmic bytes (0.92) of the same kernel on a 9,000^2 LU, "
@@ -286,9 +297,10 @@ def run_ours(args, rank, world):
     res = {
         "metric": METRIC, "value": round(t_step, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * t_step, 2), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64+tf32+f32", "data": "synthetic (seeded)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f16+f32" if f16_ops else "f64+tf32+f32", "data": "synthetic (seeded)",
         "config": dict(WORKLOAD, parallelism=f"replicas{world}", l2="flushed (256 MB write) before every step",
-                       solver="TF32 LU + FP64 GMRES-IR", field="vertex/edge tetrahedron form, FP32 terms, FP64 vertex offsets and accumulation",
+                       solver=("LU with FP32 factors, tensor-core updates on scaled FP16 operands (FP32 accumulation), FP64 GMRES-IR"
+                               if f16_ops else "TF32 LU + FP64 GMRES-IR"), field="vertex/edge tetrahedron form, FP32 terms, FP64 vertex offsets and accumulation",
                        assembly="FP64 vertex/edge form, stored FP32 with the FP64 residue of near blocks"),
         "breakdown_s": {"assembly": round(float(np.mean(t_asm)), 4), "solve": round(float(np.mean(t_solve)), 4),
                         "field": round(fld_s, 4)},

@@ -32,6 +32,7 @@
 // several tiles and chunks per CTA) and keeps the tensor-core path only if it
 // agrees to TF32 accuracy.
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <math.h>
 #include <stdlib.h>
 
@@ -377,11 +378,18 @@ constexpr int TM_THREADS = 288;  // warps 0-7: epilogue; warp 8: TMA loads and M
 // that buffer's "full" barrier; warps 0-7 drain a finished buffer (C loaded
 // beforehand, C - AB stored) and arrive on its "empty" barrier, so the MMAs
 // of tile i+1 run while tile i is written back.  Every wait is bounded.
+// F16: the operands are FP16 copies scaled by powers of two (*scale holds
+// 1 / (sA sB), applied to the accumulator in the epilogue): kind::f16 MMAs of
+// K = 16 (32 bytes of a 128-byte row, as the TF32 K = 8 step), 64 elements
+// per stage row instead of 32, so a stage feeds twice the flops.
+template <bool F16>
 __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                                       const __grid_constant__ CUtensorMap tmB,
                                                                       float *__restrict__ C, int ldc, int m, int n, int k,
-                                                                      int *__restrict__ err, int overwrite)
+                                                                      int *__restrict__ err, int overwrite,
+                                                                      const float *__restrict__ scale)
 {
+  constexpr int KC = F16 ? 2 * TM_KC : TM_KC;  // K elements per stage
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *sbase = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ uint64_t full[TM_NST], empty[TM_NST], accf[2], acce[2];
@@ -391,7 +399,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tiles_n = (n + TC_BN - 1) / TC_BN, tiles_m = (m + TC_BM - 1) / TC_BM;
   const int ntiles = tiles_n * tiles_m;
-  const int nch = (k + TM_KC - 1) / TM_KC;
+  const int nch = (k + KC - 1) / KC;
   if (tid == 0) abort_cta = *(volatile int *)err;
   __syncthreads();
   if (abort_cta != 0 || (int)blockIdx.x >= ntiles || nch < 1) return;
@@ -432,11 +440,12 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
         mbar_expect_tx(fb, (uint32_t)TM_STAGE);
         int rr, ccol;
         tile_rc(tt, tiles_m, tiles_n, rr, ccol);
-        tma_load_2d(so, &tmA, cc * TM_KC, rr, fb);
-        tma_load_2d(so + TM_STAGE_A, &tmB, cc * TM_KC, ccol, fb);
+        tma_load_2d(so, &tmA, cc * KC, rr, fb);
+        tma_load_2d(so + TM_STAGE_A, &tmB, cc * KC, ccol, fb);
       };
       for (; issued < TM_NST - 1 && issued < G; issued++) issue(issued);
-      const uint32_t idesc = umma_idesc(0);
+      // F16: A and B formats 0 (f16); TF32: 2 (tf32)
+      const uint32_t idesc = F16 ? (umma_idesc(0) & ~((7u << 7) | (7u << 10))) : umma_idesc(0);
       for (int i = 0; i < my_tiles && !timed_out; i++) {
         const int buf = i & 1;
         // the epilogue of tile i - 2 has released this accumulator buffer
@@ -453,10 +462,16 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
             uint64_t da = umma_desc_sw128(ua + 32u * s);
             uint64_t db = umma_desc_sw128(ub + 32u * s);
             uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dacc),
-                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+            if (F16)
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dacc),
+                  "l"(da), "l"(db), "r"(idesc), "r"(acc));
+            else
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dacc),
+                  "l"(da), "l"(db), "r"(idesc), "r"(acc));
           }
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                            smem_u32(&empty[st]))
@@ -495,6 +510,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
     const int q = warp & 3, hc = warp >> 2;
     float *W = reinterpret_cast<float *>(sbase + TM_NST * TM_STAGE) + warp * 32 * 32;
     const int lr = lane >> 3, lc = (lane & 7) * 4;
+    const float osc = F16 ? __ldg(scale) : 1.0f;
     for (int i = 0; i < my_tiles; i++) {
       const int tile = blockIdx.x + i * gridDim.x;
       int row0, col0;
@@ -541,7 +557,8 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
 #pragma unroll
         for (int rr = 0; rr < 8; rr++) {
           const int rl = 4 * rr + lr;
-          const float4 t = *reinterpret_cast<const float4 *>(W + rl * 32 + (((lane & 7) ^ (rl & 7)) << 2));
+          float4 t = *reinterpret_cast<const float4 *>(W + rl * 32 + (((lane & 7) ^ (rl & 7)) << 2));
+          if (F16) { t.x *= osc; t.y *= osc; t.z *= osc; t.w *= osc; }
           const int gr = rbase + rl, gc = cbase + 32 * sl + lc;
           if (gr < m) {
             const float4 c4 = cs[rr];
@@ -592,7 +609,7 @@ __global__ void tc_ref_kernel(float *C, int ld, int m, int n, int k, const float
 }
 
 static int g_tc_state = -1;   // -1 untested, 0 disabled, 1 enabled
-static int g_tc_tma = 0;      // 1: the TMA-fed kernel passed the self-test and is used
+static int g_tc_tma = 0;      // 1: the TMA-fed kernel (TF32 operands) passed the self-test; 2: also with FP16 operands
 static double g_tc_err = -1.0;
 static DBuf g_tc_err_flag;
 
@@ -623,9 +640,83 @@ __global__ void tc_transpose_kernel(const float *__restrict__ B, int ldb, int k,
   }
 }
 
+// ---- FP16 operands: power-of-two scaling against the FP16 range -------------
+// max |A| (m x k) and max |B| (k x n) into mx[0], mx[1] (float bits; non-
+// negative floats order as unsigned integers)
+__global__ void tc_absmax_kernel(const float *__restrict__ A, int lda, int m, int k, const float *__restrict__ B, int ldb,
+                                 int n, unsigned *__restrict__ mx)
+{
+  __shared__ float red[2][8];
+  float a = 0.f, b = 0.f;
+  const int64_t na = (int64_t)m * k, nbt = (int64_t)k * n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < na; e += (int64_t)gridDim.x * blockDim.x)
+    a = fmaxf(a, fabsf(A[(e / k) * lda + e % k]));
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nbt; e += (int64_t)gridDim.x * blockDim.x)
+    b = fmaxf(b, fabsf(B[(e / n) * ldb + e % n]));
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+    b = fmaxf(b, __shfl_xor_sync(0xffffffffu, b, o));
+  }
+  if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = a; red[1][threadIdx.x >> 5] = b; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)blockDim.x / 32; w++) { a = fmaxf(a, red[0][w]); b = fmaxf(b, red[1][w]); }
+    atomicMax(mx, __float_as_uint(a));
+    atomicMax(mx + 1, __float_as_uint(b));
+  }
+}
+
+// the power of two that brings max |x| to at most 2^14 (1 for an all-zero operand)
+__device__ __forceinline__ float f16_scale(unsigned maxbits)
+{
+  const float mxv = __uint_as_float(maxbits);
+  if (!(mxv > 0.f) || !isfinite(mxv)) return 1.f;
+  int e;
+  frexpf(mxv, &e);  // mxv < 2^e
+  return ldexpf(1.f, 14 - e);
+}
+
+// Ah[r][c] = FP16(sA A[r][c]) for c < k, 0 for k <= c < kp
+__global__ void tc_f16_rows_kernel(const float *__restrict__ A, int lda, int m, int k, const unsigned *__restrict__ mx,
+                                   __half *__restrict__ Ah, int kp)
+{
+  const float sa = f16_scale(mx[0]);
+  const int64_t tot = (int64_t)m * kp;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / kp), c = (int)(e % kp);
+    Ah[e] = __float2half_rn(c < k ? sa * A[(size_t)r * lda + c] : 0.f);
+  }
+}
+
+// Bth[c][r] = FP16(sB B[r][c]) (n x kp, K contiguous)
+__global__ void tc_f16_transpose_kernel(const float *__restrict__ B, int ldb, int k, int n, const unsigned *__restrict__ mx,
+                                        __half *__restrict__ Bth, int kp)
+{
+  __shared__ float t[32][33];
+  const float sb = f16_scale(mx[1]);
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int r = r0 + i, c = c0 + threadIdx.x;
+    t[i][threadIdx.x] = (r < k && c < n) ? B[(size_t)r * ldb + c] : 0.f;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int c = c0 + i, r = r0 + threadIdx.x;
+    if (c < n && r < kp) Bth[(size_t)c * kp + r] = __float2half_rn(sb * t[threadIdx.x][i]);
+  }
+}
+
+// the epilogue's factor 1 / (sA sB)
+__global__ void tc_f16_outscale_kernel(const unsigned *__restrict__ mx, float *__restrict__ osc)
+{
+  osc[0] = 1.f / (f16_scale(mx[0]) * f16_scale(mx[1]));
+}
+
 // B^T scratch, [n x ldbt] floats, ldbt = k rounded up to 4; one per slot so
 // that updates on two streams (the LU's look-ahead) never share it
 static DBuf g_tc_bt_slots[2];
+// FP16 path, per slot: A and B^T copies, the two maxima and the output factor
+static DBuf g_tc_ah_slots[2], g_tc_bh_slots[2], g_tc_mx_slots[2];
 
 // max_ctas > 0 caps the persistent grid (the self-test uses it to make every
 // CTA loop over several tiles)
@@ -652,15 +743,17 @@ static TensorMapEncodeFn tensor_map_encoder()
 
 // 2-D FP32 map of a row-major rows x cols matrix (pitch ld floats), boxes of
 // 32 columns x box_rows rows, 128-byte swizzle, zero fill outside
-static int encode_map(CUtensorMap *map, const float *base, int rows, int cols, int ld, int box_rows)
+static int encode_map(CUtensorMap *map, const void *base, int rows, int cols, int ld, int box_rows, bool f16 = false)
 {
   TensorMapEncodeFn enc = tensor_map_encoder();
   if (!enc) return RADB200_E_UNSUPPORTED;
+  // 128-byte rows of the box: 32 FP32 or 64 FP16 elements
   cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
-  cuuint32_t box[2] = {(cuuint32_t)TM_KC, (cuuint32_t)box_rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * (f16 ? 2u : 4u)};
+  cuuint32_t box[2] = {(cuuint32_t)(f16 ? 2 * TM_KC : TM_KC), (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
-  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, estr,
+  CUresult r = enc(map, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims,
+                   strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
@@ -684,6 +777,36 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
     RB_CUDA(cudaGetDevice(&dev));
     RB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   }
+  int grid = (int)std::min<long long>(tiles, max_ctas > 0 ? max_ctas : nsm);
+  if (use_tma == 2) {
+    // FP16 operands scaled into range (A is left as it is)
+    const int kp = (k + 7) / 8 * 8;
+    DBuf &ah = g_tc_ah_slots[slot & 1], &bh = g_tc_bh_slots[slot & 1], &mx = g_tc_mx_slots[slot & 1];
+    RB_TRY(ah.alloc((size_t)m * kp * sizeof(__half)));
+    RB_TRY(bh.alloc((size_t)n * kp * sizeof(__half)));
+    RB_TRY(mx.alloc(4 * sizeof(unsigned)));
+    RB_CUDA(cudaMemsetAsync(mx.p, 0, 2 * sizeof(unsigned), st));
+    const int64_t tot = (int64_t)m * k + (int64_t)k * n;
+    const int nb = (int)std::min<int64_t>((tot + 255) / 256, 148 * 8);
+    tc_absmax_kernel<<<std::max(nb, 1), 256, 0, st>>>(A, lda, m, k, B, ldb, n, mx.as<unsigned>());
+    RB_TRY(check_launch("tc_absmax_kernel"));
+    const int nra = (int)std::min<int64_t>(((int64_t)m * kp + 255) / 256, 148 * 16);
+    tc_f16_rows_kernel<<<std::max(nra, 1), 256, 0, st>>>(A, lda, m, k, mx.as<unsigned>(), ah.as<__half>(), kp);
+    RB_TRY(check_launch("tc_f16_rows_kernel"));
+    tc_f16_transpose_kernel<<<dim3((n + 31) / 32, (kp + 31) / 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, mx.as<unsigned>(),
+                                                                                     bh.as<__half>(), kp);
+    RB_TRY(check_launch("tc_f16_transpose_kernel"));
+    float *osc = reinterpret_cast<float *>(mx.as<unsigned>() + 2);
+    tc_f16_outscale_kernel<<<1, 1, 0, st>>>(mx.as<unsigned>(), osc);
+    RB_TRY(check_launch("tc_f16_outscale_kernel"));
+    CUtensorMap ma, mb;
+    RB_TRY(encode_map(&ma, ah.p, m, k, kp, TC_BM, true));
+    RB_TRY(encode_map(&mb, bh.p, n, k, kp, TC_BN, true));
+    RB_CUDA(cudaFuncSetAttribute(tc_update_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TM_SMEM));
+    tc_update_tma_kernel<true><<<grid, TM_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(),
+                                                                  overwrite, osc);
+    return check_launch("tc_update_tma_kernel<f16>");
+  }
   RB_TRY(g_tc_bt.alloc((size_t)n * ldbt * sizeof(float)));
   {
     int64_t tot = (int64_t)m * k;
@@ -693,13 +816,13 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
   }
   tc_transpose_kernel<<<dim3((n + 31) / 32, (k + 31) / 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, g_tc_bt.as<float>(), ldbt);
   RB_TRY(check_launch("tc_transpose_kernel"));
-  int grid = (int)std::min<long long>(tiles, max_ctas > 0 ? max_ctas : nsm);
   if (use_tma) {
     CUtensorMap ma, mb;
     RB_TRY(encode_map(&ma, A, m, k, lda, TC_BM));
     RB_TRY(encode_map(&mb, g_tc_bt.as<float>(), n, k, ldbt, TC_BN));
-    RB_CUDA(cudaFuncSetAttribute(tc_update_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TM_SMEM));
-    tc_update_tma_kernel<<<grid, TM_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(), overwrite);
+    RB_CUDA(cudaFuncSetAttribute(tc_update_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TM_SMEM));
+    tc_update_tma_kernel<false><<<grid, TM_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(),
+                                                                   overwrite, nullptr);
     return check_launch("tc_update_tma_kernel");
   }
   RB_CUDA(cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
@@ -759,30 +882,35 @@ static int tc_selftest_case(int m, int n, int k, int overwrite, int use_tma, dou
 // Keeps the tensor-core path only if every case matches the CUDA-core
 // reference to TF32 accuracy: K of 4 chunks of 32 (120) and of 10 (300),
 // ragged m and n, and the overwrite form the LU panels use.  The cp.async-fed
-// kernel is tested first; the TMA-fed kernel is then tested on the same cases
-// and used only if it passes them all.
+// kernel is tested first, then the TMA-fed kernel with TF32 operands, then
+// with scaled FP16 operands (the same 11-bit significand as TF32 inside the
+// scaled range); each is used only if it and the ones before it pass every
+// case.  RADB200_TC_F16=0 stops at the TF32 TMA kernel (A/B comparisons).
 static int tc_selftest()
 {
   RB_TRY(g_tc_err_flag.alloc(sizeof(int)));
   g_tc_state = 0;
   g_tc_tma = 0;
   g_tc_err = 0.0;
+  const char *ef = getenv("RADB200_TC_F16");
+  const int last = (ef && atoi(ef) == 0) ? 1 : 2;
   const int cases[3][4] = {{300, 400, 120, 0}, {300, 300, 300, 0}, {260, 290, 64, 1}};
-  for (int use_tma = 0; use_tma <= 1; use_tma++) {
+  for (int use_tma = 0; use_tma <= last; use_tma++) {
     double worst = 0.0;
     for (auto &cs : cases) {
       double err = 1.0;
       int timeout = 0;
       RB_TRY(tc_selftest_case(cs[0], cs[1], cs[2], cs[3], use_tma, &err, &timeout));
       if (timeout) {  // an MMA or copy never completed: leave this kernel off
-        set_error("tensor-core self-test: a completion wait timed out (%s kernel)", use_tma ? "TMA" : "cp.async");
-        RB_CUDA(cudaMemset(g_tc_err_flag.p, 0, sizeof(int)));  // the other kernel may still run
+        set_error("tensor-core self-test: a completion wait timed out (%s kernel)",
+                  use_tma == 2 ? "TMA FP16" : use_tma ? "TMA" : "cp.async");
+        RB_CUDA(cudaMemset(g_tc_err_flag.p, 0, sizeof(int)));  // the kernels before it may still run
         return 0;
       }
       worst = std::max(worst, err);
     }
     if (!(worst < 1e-4)) return 0;
-    if (use_tma) g_tc_tma = 1;
+    if (use_tma) g_tc_tma = use_tma;
     else { g_tc_state = 1; g_tc_err = worst; }
   }
   return 0;
@@ -817,7 +945,7 @@ int tc_error_flag(int *flag)
 extern "C" RADB200_API int radb200_tc_selftest(int *state, double *err)
 {
   if (rb::g_tc_state < 0) RB_TRY(rb::tc_selftest());
-  *state = rb::g_tc_state + rb::g_tc_tma;  // 0 off, 1 cp.async-fed kernel, 2 TMA-fed kernel
+  *state = rb::g_tc_state + rb::g_tc_tma;  // 0 off, 1 cp.async-fed kernel, 2 TMA-fed kernel, 3 with FP16 operands
   *err = rb::g_tc_err;
   return 0;
 }
