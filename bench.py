@@ -73,6 +73,15 @@ class Clocks:
             self.f = open(self.out, "w")
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
+            # the sampler's start-up (driver initialisation) stalls the GPU for
+            # a moment: time nothing until its first sample is written
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and self.p.poll() is None:
+                self.f.flush()
+                if os.path.getsize(self.out) > 0:
+                    break
+                time.sleep(0.05)
+            time.sleep(0.5)
         except Exception:
             self.p = None
         return self
@@ -294,6 +303,7 @@ def run_ours(args, rank, world):
     n_tets = src["poly"].shape[0]
     fld_s = float(np.mean(t_fld))
     achieved = P.shape[0] * n_tets * FIELD_OPS_PER_TET / fld_s / 1e12
+    clk = clocks.summary(int(os.environ.get("LOCAL_RANK", 0)))
     res = {
         "metric": METRIC, "value": round(t_step, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * t_step, 2), "higher_is_better": False,
@@ -320,13 +330,8 @@ def run_ours(args, rank, world):
                 "d2h_bytes_per_step": int(P.nbytes + n3 * 8)},
         "gpu_launches": int(launches),
         "roofline": roof_upd,
-        "roofline_field": {"kernel": "field_tet_kernel<float> (FP32 terms)", "bound": "fp32 pipe",
-                           "achieved": round(achieved, 3), "peak": round(fp32_peak.value, 3), "unit": "TFLOP/s",
-                           "frac": round(achieved / fp32_peak.value, 4),
-                           "peak_source": "measured FP32 FMA loop (radb200_measure_fma_peak) on this GPU",
-                           "algorithmic": f"{FIELD_OPS_PER_TET} ops per (point, tetrahedron)",
-                           "traffic": None},
-        "clocks": clocks.summary(int(os.environ.get("LOCAL_RANK", 0))),
+        "roofline_field": field_roofline(P.shape[0] * n_tets / fld_s, achieved, fp32_peak.value, clk),
+        "clocks": clk,
     }
     return res
 
@@ -638,6 +643,34 @@ TC_TRAFFIC_OVER_ALGORITHMIC = 0.92
 # 6 edge dot products (6 x 5), 6 edge logarithms with their accumulation
 # (6 x 40), 4 solid angles with theirs (4 x 51), final scaling (3).
 FIELD_OPS_PER_TET = 4 * 16 + 6 * 5 + 6 * 40 + 4 * 51 + 3
+
+# Instructions the FP32 field kernel issues per (point, tetrahedron) pair,
+# from ncu's smsp__inst_executed.sum x 32 / pairs on the 20,000-point,
+# 20,000-tetrahedron case (profiles/field_tet_kernel_f32_20k_tets.md), and
+# their split over the pipes.  The kernel is issue-bound: its roofline is the
+# SMs' issue rate, 4 warp-instructions (128 thread-instructions) per clock
+# per SM, divided by these instructions per pair.
+FIELD_INST_PER_PAIR = 793
+FIELD_INST_MIX = {"fma": 329, "alu": 157, "fp64": 81, "lsu": 60, "xu": 50}
+B200_SMS = 148
+
+
+def field_roofline(pairs_per_s, op_tflops, fp32_peak, clk):
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    peak = B200_SMS * mhz * 1e6 * 128 / 1e12  # thread-instructions issued per second, 1e12
+    ach = pairs_per_s * FIELD_INST_PER_PAIR / 1e12
+    return {"kernel": "field_tet_kernel<float> (FP32 terms)", "bound": "issue",
+            "achieved": round(ach, 3), "peak": round(peak, 3), "unit": "T instructions/s", "frac": round(ach / peak, 4),
+            "peak_source": f"{B200_SMS} SMs x 128 thread-instructions per clock at the median SM clock sampled "
+                           f"during the timed steps ({mhz:.0f} MHz)",
+            "algorithmic": f"{FIELD_INST_PER_PAIR} instructions per (point, tetrahedron), ncu-counted "
+                           f"(per pipe: {FIELD_INST_MIX})",
+            "pairs_per_s": round(pairs_per_s, 1),
+            "op_model": {"achieved_tflops": round(op_tflops, 3), "fp32_fma_peak_tflops": round(fp32_peak, 3),
+                         "frac": round(op_tflops / fp32_peak, 4),
+                         "note": f"{FIELD_OPS_PER_TET} FP64-equivalent ops per pair with elementary functions "
+                                 "weighted at standard-implementation costs"},
+            "traffic": None}
 
 
 # ---------------------------------------------------------------------------
