@@ -293,12 +293,14 @@ def run_ours(args, rank, world):
                                 "fallback sustained bf16" + ("" if f16_ops else " / 2")),
                 "frac_of_burst": round(upd_tflops / (float(peaks.get("bf16_tflops", 1590.0)) / div), 4),
                 "hbm_achieved_gbs": round(upd_gbs, 1), "hbm_peak_gbs": hbm, "hbm_frac": round(upd_gbs / hbm, 4),
-                "traffic": round(TC_TRAFFIC_OVER_ALGORITHMIC * upd_bytes_per_launch),
+                "traffic": round(TC_TRAFFIC_OVER_ALGORITHMIC["f16" if f16_ops else "tf32"] * upd_bytes_per_launch),
                 "traffic_note": "ncu dram bytes / algorithmic bytes (0.92) of the same kernel on a 9,000^2 LU, "
                                 "times the algorithmic bytes per launch",
                 "launches_per_step": int(upd_n.value // max(args.steps, 1)),
                 "seconds_per_step": round(upd_s.value / max(args.steps, 1), 4),
-                "algorithmic": "2 m^2 K flops; 8 m^2 + 8 m K bytes per launch (FP32 C read + written, panels read once)"}
+                "algorithmic": ("2 m^2 K flops; 8 m^2 + 4 m K bytes per launch (FP32 C read + written, FP16 panels "
+                                "read once)" if f16_ops else
+                                "2 m^2 K flops; 8 m^2 + 8 m K bytes per launch (FP32 C read + written, panels read once)")}
     # the field kernel (FP64 pipe, transcendental-bound) against the measured FP64 FMA peak
     n_tets = src["poly"].shape[0]
     fld_s = float(np.mean(t_fld))
@@ -632,8 +634,9 @@ def trajectory_timing(reps=3):
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum over the algorithmic bytes of the
-# trailing-update kernel (561 MB / 611 MB), from an ncu capture of a 9,000^2 LU
-TC_TRAFFIC_OVER_ALGORITHMIC = 0.92
+# trailing-update kernel, from ncu captures of a 9,000^2 LU: 561 MB / 611 MB with
+# TF32 operands, 475 MB / 515.7 MB with FP16 operands
+TC_TRAFFIC_OVER_ALGORITHMIC = {"tf32": 0.92, "f16": 0.92}
 
 
 # FP64 operations of one (point, tetrahedron) term of the vertex/edge form

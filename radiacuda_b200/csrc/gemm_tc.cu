@@ -928,7 +928,7 @@ int tc_gemm_f32(float *C, int ldc, int m, int n, int k, float *A, int lda, const
   if (g_tc_state <= 0) return 0;
   RB_TRY(g_tc_err_flag.alloc(sizeof(int)));
   RB_TRY(launch_tc(C, ldc, m, n, k, A, lda, B, ldb, st, overwrite, max_ctas, -1, slot));
-  *used = 1;
+  *used = g_tc_tma == 2 ? 2 : 1;  // 2: the operands went to the tensor cores as FP16
   return 0;
 }
 

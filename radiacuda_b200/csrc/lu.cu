@@ -483,8 +483,10 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
     if (g_update_timing) {
       RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used + 1], q));
       g_upd_ev.used++;
-      // algorithmic bytes: C read + written, the L and U panels read once
-      g_upd_bytes += (double)sizeof(T) * (2.0 * m * n + (double)m * k + (double)k * n);
+      // algorithmic bytes: C read + written, the L and U panels read once (as
+      // FP16 copies when the tensor cores took FP16 operands)
+      const double opb = used == 2 ? 2.0 : (double)sizeof(T);
+      g_upd_bytes += (double)sizeof(T) * 2.0 * m * n + opb * ((double)m * k + (double)k * n);
       g_upd_flops += 2.0 * m * n * k;
     }
     return 0;
