@@ -8,27 +8,32 @@
 // positive semi-definite, so A is (close to) positive definite and needs no
 // row exchanges; a vanishing pivot is reported as RADB200_E_NUMERIC.
 //
-// Two levels: outer panels of 512 columns, 128-wide steps inside.  Step k
+// Two levels: outer panels of 768 columns, 128-wide steps inside.  Step k
 // (width nb = 128) inside a panel:
 //   1. one CTA factors the diagonal block in shared memory (FP64) and writes
-//      the inverses of its unit-lower and upper triangles, L_kk^-1 and U_kk^-1;
+//      the inverses of its unit-lower and upper triangles, L_kk^-1 and U_kk^-1
+//      (lu_diag.cuh);
 //   2. L21 = A21 U_kk^-1 and the panel's U12 = L_kk^-1 A12 as GEMMs (out of
 //      place, then copied back), so the triangular solves of the panel also
 //      run on the GEMM engine; a narrow update of the panel's other columns.
 // After the panel: its U block row by block forward substitution, then one
-// trailing update A22 -= L21 U12 with K = 512.
+// trailing update A22 -= L21 U12 with K = 768, split into the next panel's
+// columns (main stream) and the rest (a side stream, overlapping the next
+// panel's factorization).
 //   mode F64  : FP64 factors, GEMMs on the FP64 pipe (CUDA cores).
-//   mode TF32 : FP32 factors, GEMMs on the tcgen05 tensor cores in TF32 with
-//               FP32 accumulation (gemm_tc.cu), then right-preconditioned FP64
-//               GMRES on A with the FP64 residual (GMRES-IR).
-// Triangular solves with the factors use the stored diagonal-block inverses:
-// per block one small matvec and one column-panel GEMV.
+//   mode mixed: FP32 factors, GEMMs on the tcgen05 tensor cores (FP16
+//               operands scaled by powers of two, or TF32; FP32 accumulation,
+//               gemm_tc.cu), then right-preconditioned FP64 GMRES on A with
+//               the FP64 residual (GMRES-IR).
+// Triangular solves with the factors use the stored diagonal-block inverses
+// (one persistent launch per sweep, tri_sweep_kernel).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <vector>
 
 #include "internal.cuh"
+#include "lu_diag.cuh"
 
 namespace rb {
 
@@ -72,91 +77,9 @@ __global__ void apply_A_kernel(const double *__restrict__ x, const double *__res
     out[3 * e + a] = x[3 * e + a] - (X[3 * a] * y[3 * e] + X[3 * a + 1] * y[3 * e + 1] + X[3 * a + 2] * y[3 * e + 2]);
 }
 
-// ---- diagonal block: factor (unpivoted) and invert both triangles ----------
-// One CTA of 1024 threads; the block lives in shared memory at row pitch
-// nb + 1 (threads reading different rows at one column hit different banks).
-//   factor:  for k: scale column k below the pivot, rank-1 update of the
-//            trailing block (warp per row, lanes across columns);
-//   invert:  in place, L^-1 column by column from the right (unit lower,
-//            Linv[i][j] = -(L[i][j] + sum_{j<q<i} Linv[i][q] L[q][j])) by
-//            threads 0..511, and U^-1 column by column from the left
-//            (Uinv[i][j] = -sum_{i<=q<j} Uinv[i][q] U[q][j] / U[j][j]) by
-//            threads 512..1023: 4 threads per row split the inner product;
-//            each column is copied aside first.
-constexpr int DIAG_T = 1024;
-
-template <typename T>
-__global__ void __launch_bounds__(DIAG_T) diag_factor_kernel(T *__restrict__ A, int ld, int k0, int nb, T *__restrict__ Linv,
-                                                             T *__restrict__ Uinv, int *__restrict__ err)
-{
-  extern __shared__ double sblk[];  // nb x (nb + 1)
-  __shared__ double colL[LU_NB], colU[LU_NB];
-  const int P = nb + 1;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int e = tid; e < nb * nb; e += DIAG_T) {
-    int r = e / nb, c = e - r * nb;
-    sblk[r * P + c] = (double)A[(size_t)(k0 + r) * ld + k0 + c];
-  }
-  __syncthreads();
-  for (int k = 0; k < nb; k++) {
-    const double piv = sblk[k * P + k];
-    if (tid == 0 && !(fabs(piv) > 1e-300)) err[0] = 1;
-    const double ip = 1.0 / piv;
-    for (int r = k + 1 + warp; r < nb; r += DIAG_T / 32) {
-      const double l = sblk[r * P + k] * ip;
-      __syncwarp();
-      for (int c = k + 1 + lane; c < nb; c += 32) sblk[r * P + c] -= l * sblk[k * P + c];
-      if (lane == 0) sblk[r * P + k] = l;
-    }
-    __syncthreads();
-  }
-  for (int e = tid; e < nb * nb; e += DIAG_T) {
-    int r = e / nb, c = e - r * nb;
-    A[(size_t)(k0 + r) * ld + k0 + c] = (T)sblk[r * P + c];
-  }
-  __syncthreads();
-  const bool lower = tid < DIAG_T / 2;
-  const int t = tid & (DIAG_T / 2 - 1);
-  const int i = t >> 2, sub = t & 3;  // row and its quarter of the inner product
-  for (int s = 0; s < nb; s++) {
-    const int jl = nb - 1 - s, ju = s;
-    if (lower) {
-      if (t > jl && t < nb) colL[t] = sblk[t * P + jl];
-    } else if (t <= ju) {
-      colU[t] = sblk[t * P + ju];
-    }
-    __syncthreads();
-    double acc = 0.0;
-    if (lower) {
-      if (i > jl && i < nb)
-        for (int q = jl + 1 + sub; q < i; q += 4) acc += sblk[i * P + q] * colL[q];
-    } else if (i < ju) {
-      for (int q = i + sub; q < ju; q += 4) acc += sblk[i * P + q] * colU[q];
-    }
-    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-    if (sub == 0) {
-      if (lower) {
-        if (i > jl && i < nb) sblk[i * P + jl] = -(colL[i] + acc);
-      } else {
-        const double d = 1.0 / colU[ju];
-        if (i < ju) sblk[i * P + ju] = -acc * d;
-        else if (i == ju) sblk[i * P + ju] = d;
-      }
-    }
-    __syncthreads();
-  }
-  for (int e = tid; e < nb * LU_NB; e += DIAG_T) {
-    int ii = e / LU_NB, j = e - ii * LU_NB;
-    double l = 0.0, u = 0.0;
-    if (j < nb) {
-      l = (ii > j) ? sblk[ii * P + j] : (ii == j ? 1.0 : 0.0);
-      u = (ii <= j) ? sblk[ii * P + j] : 0.0;
-    }
-    Linv[(size_t)(k0 + ii) * LU_NB + j] = (T)l;
-    Uinv[(size_t)(k0 + ii) * LU_NB + j] = (T)u;
-  }
-}
+// ---- diagonal block: factor (unpivoted) and invert both triangles: one CTA,
+// blocked by 32 in shared memory (lu_diag.cuh)
+static_assert(DG_N == LU_NB, "the diagonal-block kernel works on LU_NB x LU_NB blocks");
 
 // ---- CUDA-core GEMM: C[m x n] (=|-=) A[m x k] B[k x n]; 64x64 tile, k-slices of 16
 template <typename T>
@@ -433,8 +356,7 @@ template <typename T>
 static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaStream_t st, int *tc_used)
 {
   const int n3 = I.n3, ld = I.ld;
-  const int smax = LU_NB * (LU_NB + 1) * (int)sizeof(double);
-  RB_CUDA(cudaFuncSetAttribute(diag_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  RB_CUDA(cudaFuncSetAttribute(diag_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
   // RADB200_LU_TIMING=1 prints the time of each phase (synchronizes per phase);
   // RADB200_LU_LOOKAHEAD=0 runs every phase on the caller's stream
   const bool timing = getenv("RADB200_LU_TIMING") != nullptr;
@@ -499,7 +421,7 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
     // the previous step updated these columns there first)
     for (int j0 = K0; j0 < pend; j0 += LU_NB) {
       const int jb = std::min(LU_NB, pend - j0);
-      diag_factor_kernel<T><<<1, DIAG_T, (size_t)jb * (jb + 1) * sizeof(double), sm>>>(A, ld, j0, jb, Linv, Uinv, d_err);
+      diag_factor_kernel<T><<<1, DG_T, DG_SMEM, sm>>>(A, ld, j0, jb, Linv, Uinv, d_err);
       RB_TRY(check_launch("diag_factor_kernel"));
       RB_TRY(phase(0));
       const int rest = j0 + jb, m = n3 - rest;
