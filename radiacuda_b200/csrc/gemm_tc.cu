@@ -707,9 +707,27 @@ __global__ void tc_f16_transpose_kernel(const float *__restrict__ B, int ldb, in
 }
 
 // the epilogue's factor 1 / (sA sB)
-__global__ void tc_f16_outscale_kernel(const unsigned *__restrict__ mx, float *__restrict__ osc)
+// also clears the two maxima for the next update on this slot (every kernel
+// that reads them runs before this one on the stream)
+__global__ void tc_f16_outscale_kernel(unsigned *__restrict__ mx, float *__restrict__ osc)
 {
   osc[0] = 1.f / (f16_scale(mx[0]) * f16_scale(mx[1]));
+  mx[0] = 0u;
+  mx[1] = 0u;
+}
+
+// cudaFuncSetAttribute once per kernel and device (a driver call per launch
+// showed up in the LU's host enqueue time)
+template <typename K>
+static int set_smem_once(K kernel, int bytes, int which)
+{
+  static bool done[3][64] = {};
+  int dev = 0;
+  RB_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && done[which][dev]) return 0;
+  RB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  if (dev >= 0 && dev < 64) done[which][dev] = true;
+  return 0;
 }
 
 // B^T scratch, [n x ldbt] floats, ldbt = k rounded up to 4; one per slot so
@@ -784,8 +802,10 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
     DBuf &ah = g_tc_ah_slots[slot & 1], &bh = g_tc_bh_slots[slot & 1], &mx = g_tc_mx_slots[slot & 1];
     RB_TRY(ah.alloc((size_t)m * kp * sizeof(__half)));
     RB_TRY(bh.alloc((size_t)n * kp * sizeof(__half)));
-    RB_TRY(mx.alloc(4 * sizeof(unsigned)));
-    RB_CUDA(cudaMemsetAsync(mx.p, 0, 2 * sizeof(unsigned), st));
+    if (!mx.p) {  // the maxima start at zero; tc_f16_outscale_kernel clears them after each update
+      RB_TRY(mx.alloc(4 * sizeof(unsigned)));
+      RB_CUDA(cudaMemsetAsync(mx.p, 0, 4 * sizeof(unsigned), st));
+    }
     const int64_t tot = (int64_t)m * k + (int64_t)k * n;
     const int nb = (int)std::min<int64_t>((tot + 255) / 256, 148 * 8);
     tc_absmax_kernel<<<std::max(nb, 1), 256, 0, st>>>(A, lda, m, k, B, ldb, n, mx.as<unsigned>());
@@ -802,7 +822,7 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
     CUtensorMap ma, mb;
     RB_TRY(encode_map(&ma, ah.p, m, k, kp, TC_BM, true));
     RB_TRY(encode_map(&mb, bh.p, n, k, kp, TC_BN, true));
-    RB_CUDA(cudaFuncSetAttribute(tc_update_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TM_SMEM));
+    RB_TRY(set_smem_once(tc_update_tma_kernel<true>, TM_SMEM, 0));
     tc_update_tma_kernel<true><<<grid, TM_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(),
                                                                   overwrite, osc);
     return check_launch("tc_update_tma_kernel<f16>");
@@ -820,12 +840,12 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
     CUtensorMap ma, mb;
     RB_TRY(encode_map(&ma, A, m, k, lda, TC_BM));
     RB_TRY(encode_map(&mb, g_tc_bt.as<float>(), n, k, ldbt, TC_BN));
-    RB_CUDA(cudaFuncSetAttribute(tc_update_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TM_SMEM));
+    RB_TRY(set_smem_once(tc_update_tma_kernel<false>, TM_SMEM, 1));
     tc_update_tma_kernel<false><<<grid, TM_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(),
                                                                    overwrite, nullptr);
     return check_launch("tc_update_tma_kernel");
   }
-  RB_CUDA(cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+  RB_TRY(set_smem_once(tc_update_kernel, TC_SMEM, 2));
   tc_update_kernel<<<grid, TC_THREADS, TC_SMEM, st>>>(C, ldc, m, n, k, A, lda, g_tc_bt.as<float>(), ldbt,
                                                       g_tc_err_flag.as<int>(), overwrite);
   return check_launch("tc_update_kernel");
@@ -920,7 +940,8 @@ int tc_gemm_f32(float *C, int ldc, int m, int n, int k, float *A, int lda, const
                 int *used, int overwrite, int slot, int max_ctas)
 {
   *used = 0;
-  if (getenv("RADB200_NO_TC")) return 0;
+  static const bool no_tc = getenv("RADB200_NO_TC") != nullptr;
+  if (no_tc) return 0;
   if (k < 1 || m <= 0 || n <= 0 || (ldc % 4) || (lda % 4) || (ldb % 4) || ((uintptr_t)C & 15) || ((uintptr_t)A & 15) ||
       ((uintptr_t)B & 15))
     return 0;
@@ -930,6 +951,22 @@ int tc_gemm_f32(float *C, int ldc, int m, int n, int k, float *A, int lda, const
   RB_TRY(launch_tc(C, ldc, m, n, k, A, lda, B, ldb, st, overwrite, max_ctas, -1, slot));
   *used = g_tc_tma == 2 ? 2 : 1;  // 2: the operands went to the tensor cores as FP16
   return 0;
+}
+
+// C = A B where C is the same memory as A (c_is_a, n <= TC_BN: every row
+// tile of C is written by the one CTA that reads those rows of A, after its
+// MMAs have consumed them; with FP16 operands A is read from its converted
+// copy anyway) or as B (B is transposed or converted into scratch before the
+// update runs).  Only the TMA-fed kernels give these guarantees: with the
+// cp.async kernel or no tensor cores *used = 0 and the caller goes out of place.
+int tc_gemm_f32_inplace(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb,
+                        cudaStream_t st, int *used, bool c_is_a, int slot)
+{
+  *used = 0;
+  if (g_tc_state < 0) RB_TRY(tc_selftest());
+  if (g_tc_state <= 0 || g_tc_tma == 0) return 0;
+  if (c_is_a && n > TC_BN) return 0;
+  return tc_gemm_f32(C, ldc, m, n, k, A, lda, B, ldb, st, used, 1, slot, 0);
 }
 
 int tc_error_flag(int *flag)

@@ -287,6 +287,8 @@ int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_sec
 // different slots); max_ctas > 0 caps the persistent grid
 int tc_gemm_f32(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb, cudaStream_t st,
                 int *used, int overwrite = 0, int slot = 0, int max_ctas = 0);
+int tc_gemm_f32_inplace(float *C, int ldc, int m, int n, int k, float *A, int lda, const float *B, int ldb,
+                        cudaStream_t st, int *used, bool c_is_a, int slot = 0);
 int tc_error_flag(int *flag);  // 2 when a tensor-core CTA hit its wait limit
 
 // ---- kernels (launch wrappers) ---------------------------------------------

@@ -144,9 +144,27 @@ __global__ void copy2d_kernel(T *__restrict__ dst, int ldd, const T *__restrict_
   }
 }
 
+// host time spent enqueueing each kind of LU work (RADB200_LU_TIMING=2):
+// 0 GEMMs of the panel and U block rows, 1 trailing updates, 2 diagonal blocks, 3 copies
+static bool g_lu_host_timing = false;
+static double g_lu_host[4];
+struct LuHostSpan {
+  int i;
+  std::chrono::steady_clock::time_point t0;
+  explicit LuHostSpan(int k) : i(k)
+  {
+    if (g_lu_host_timing) t0 = std::chrono::steady_clock::now();
+  }
+  ~LuHostSpan()
+  {
+    if (g_lu_host_timing) g_lu_host[i] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+
 template <typename T>
 static int copy2d(T *dst, int ldd, const T *src, int lds, int rows, int cols, cudaStream_t st)
 {
+  LuHostSpan hs(3);
   int64_t tot = (int64_t)rows * cols;
   int nb = (int)std::min<int64_t>((tot + 255) / 256, 148 * 16);
   copy2d_kernel<T><<<std::max(nb, 1), 256, 0, st>>>(dst, ldd, src, lds, rows, cols);
@@ -158,6 +176,7 @@ static int gemm(T *C, int ldc, int m, int n, int k, T *A, int lda, const T *B, i
                 int *tc_used)
 {
   if (m <= 0 || n <= 0) return 0;
+  LuHostSpan hs(0);
   if (sizeof(T) == 4) {
     int used = 0;
     RB_TRY(tc_gemm_f32((float *)C, ldc, m, n, k, (float *)A, lda, (const float *)B, ldb, st, &used, overwrite));
@@ -167,6 +186,24 @@ static int gemm(T *C, int ldc, int m, int n, int k, T *A, int lda, const T *B, i
   if (grid.y > 65535) { set_error("GEMM grid too large"); return RADB200_E_ARG; }
   gemm_simt_kernel<T><<<grid, 256, 0, st>>>(C, ldc, m, n, k, A, lda, B, ldb, overwrite);
   return check_launch("gemm_simt_kernel");
+}
+
+// dst = A B where dst is the same memory as A (c_is_a) or as B: in place on
+// the tensor cores when they can (tc_gemm_f32_inplace), else into tmp (pitch
+// ldt) and copied back
+template <typename T>
+static int gemm_to(T *dst, int ldd, int m, int n, int k, T *A, int lda, const T *B, int ldb, bool c_is_a, T *tmp,
+                   int ldt, cudaStream_t st, int *tc_used)
+{
+  if (m <= 0 || n <= 0) return 0;
+  if (sizeof(T) == 4) {
+    LuHostSpan hs(0);
+    int used = 0;
+    RB_TRY(tc_gemm_f32_inplace((float *)dst, ldd, m, n, k, (float *)A, lda, (const float *)B, ldb, st, &used, c_is_a));
+    if (used) { *tc_used = 1; return 0; }
+  }
+  RB_TRY(gemm<T>(tmp, ldt, m, n, k, A, lda, B, ldb, 1, st, tc_used));
+  return copy2d<T>(dst, ldd, tmp, ldt, m, n, st);
 }
 
 // ---- triangular solves with the factors (in place on x, FP64) ----
@@ -358,8 +395,29 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
   const int n3 = I.n3, ld = I.ld;
   RB_CUDA(cudaFuncSetAttribute(diag_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
   // RADB200_LU_TIMING=1 prints the time of each phase (synchronizes per phase);
-  // RADB200_LU_LOOKAHEAD=0 runs every phase on the caller's stream
-  const bool timing = getenv("RADB200_LU_TIMING") != nullptr;
+  // RADB200_LU_TIMING=2 prints the host's time to enqueue the factorization
+  // against its device time (no synchronization inside), which shows whether
+  // the launches keep the device fed; RADB200_LU_LOOKAHEAD=0 runs every phase
+  // on the caller's stream
+  const char *tv = getenv("RADB200_LU_TIMING");
+  const int timing_mode = tv ? std::max(1, atoi(tv)) : 0;
+  const bool timing = timing_mode == 1;
+  cudaEvent_t tq0 = nullptr, tq1 = nullptr;
+  auto tq_host = std::chrono::steady_clock::now();
+  // RADB200_LU_TIMING=3: events on the main stream between its kinds of work
+  // (0 diagonal blocks, 1 L21, 2 U12 in the panel, 3 narrow panel updates,
+  // 4 waits for the side stream, 5 U block rows, 6 next panel's update),
+  // summed after the factorization: the main stream's critical path by kind
+  std::vector<cudaEvent_t> mk_ev;
+  std::vector<int> mk_cat;
+  if (timing_mode == 2) {
+    RB_CUDA(cudaEventCreate(&tq0));
+    RB_CUDA(cudaEventCreate(&tq1));
+    RB_CUDA(cudaEventRecord(tq0, st));
+    tq_host = std::chrono::steady_clock::now();
+    g_lu_host_timing = true;
+    for (double &h : g_lu_host) h = 0.0;
+  }
   const char *la = getenv("RADB200_LU_LOOKAHEAD");
   const bool lookahead = !(la && atoi(la) == 0);
   double tph[4] = {0, 0, 0, 0};
@@ -387,11 +445,21 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
     const char *fs = getenv("RADB200_LU_FREE_SMS");  // tuning override
     side_ctas = std::max(1, nsm - ((fs && atoi(fs) > 0) ? atoi(fs) : LU_SIDE_FREE_SMS));
   }
+  auto mark = [&](int cat) -> int {
+    if (timing_mode != 3) return 0;
+    cudaEvent_t e;
+    RB_CUDA(cudaEventCreate(&e));
+    RB_CUDA(cudaEventRecord(e, sm));
+    mk_ev.push_back(e);
+    mk_cat.push_back(cat);
+    return 0;
+  };
   bool side_pending = false;
   auto at = [&](int r, int c) { return A + (size_t)r * ld + c; };
   // C[m x n] -= A B with the update's timing events on stream q
   auto update = [&](T *C, int m, int n, int k, T *Ap, const T *Bp, cudaStream_t q, int slot, int cap) -> int {
     if (m <= 0 || n <= 0) return 0;
+    LuHostSpan hs(1);
     if (g_update_timing) {
       RB_TRY(g_upd_ev.grow());
       RB_CUDA(cudaEventRecord(g_upd_ev.ev[2 * g_upd_ev.used], q));
@@ -421,21 +489,28 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
     // the previous step updated these columns there first)
     for (int j0 = K0; j0 < pend; j0 += LU_NB) {
       const int jb = std::min(LU_NB, pend - j0);
-      diag_factor_kernel<T><<<1, DG_T, DG_SMEM, sm>>>(A, ld, j0, jb, Linv, Uinv, d_err);
-      RB_TRY(check_launch("diag_factor_kernel"));
+      {
+        LuHostSpan hs(2);
+        diag_factor_kernel<T><<<1, DG_T, DG_SMEM, sm>>>(A, ld, j0, jb, Linv, Uinv, d_err);
+        RB_TRY(check_launch("diag_factor_kernel"));
+      }
+      RB_TRY(mark(0));
       RB_TRY(phase(0));
       const int rest = j0 + jb, m = n3 - rest;
       if (m <= 0) break;
       // L21 = A21 U_jj^-1   (tmp: m x LU_NB)
-      RB_TRY(gemm<T>(tmp, LU_NB, m, jb, jb, at(rest, j0), ld, Uinv + (size_t)j0 * LU_NB, LU_NB, 1, sm, tc_used));
-      RB_TRY(copy2d<T>(at(rest, j0), ld, tmp, LU_NB, m, jb, sm));
+      RB_TRY(gemm_to<T>(at(rest, j0), ld, m, jb, jb, at(rest, j0), ld, Uinv + (size_t)j0 * LU_NB, LU_NB, true, tmp, LU_NB,
+                        sm, tc_used));
+      RB_TRY(mark(1));
       const int w = pend - rest;  // panel columns right of this step
       if (w > 0) {
         // U12 inside the panel = L_jj^-1 A12   (tmp: jb x w)
-        RB_TRY(gemm<T>(tmp, ld, jb, w, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, rest), ld, 1, sm, tc_used));
-        RB_TRY(copy2d<T>(at(j0, rest), ld, tmp, ld, jb, w, sm));
+        RB_TRY(gemm_to<T>(at(j0, rest), ld, jb, w, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, rest), ld, false, tmp, ld,
+                          sm, tc_used));
+        RB_TRY(mark(2));
         // narrow update of the panel: A[rest:, rest:pend] -= L21 U12
         RB_TRY(gemm<T>(at(rest, rest), ld, m, w, jb, at(rest, j0), ld, at(j0, rest), ld, 0, sm, tc_used));
+        RB_TRY(mark(3));
       }
       RB_TRY(phase(1));
     }
@@ -447,19 +522,22 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
       RB_CUDA(cudaStreamWaitEvent(sm, g_lu_streams.side_done, 0));
       side_pending = false;
     }
+    RB_TRY(mark(4));
     // ---- U block row of the trailing columns: forward substitution with the
     // panel's unit-lower diagonal block, 128 rows at a time
     for (int j0 = K0; j0 < pend; j0 += LU_NB) {
       const int jb = std::min(LU_NB, pend - j0);
       if (j0 > K0) RB_TRY(gemm<T>(at(j0, T0), ld, jb, mT, j0 - K0, at(j0, K0), ld, at(K0, T0), ld, 0, sm, tc_used));
-      RB_TRY(gemm<T>(tmp, ld, jb, mT, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, T0), ld, 1, sm, tc_used));
-      RB_TRY(copy2d<T>(at(j0, T0), ld, tmp, ld, jb, mT, sm));
+      RB_TRY(gemm_to<T>(at(j0, T0), ld, jb, mT, jb, Linv + (size_t)j0 * LU_NB, LU_NB, at(j0, T0), ld, false, tmp, ld, sm,
+                        tc_used));
     }
+    RB_TRY(mark(5));
     RB_TRY(phase(2));
     // ---- trailing update A22 -= L21 U12 with K = NBe: the next panel's
     // columns on the main stream, the rest on the side stream
     const int nxt = lookahead ? std::min(LU_OUTER, mT) : mT;
     RB_TRY(update(at(T0, T0), mT, nxt, NBe, at(T0, K0), at(K0, T0), sm, 0, 0));
+    RB_TRY(mark(6));
     if (mT > nxt) {
       RB_CUDA(cudaEventRecord(g_lu_streams.upd, sm));
       RB_CUDA(cudaStreamWaitEvent(ss, g_lu_streams.upd, 0));
@@ -476,7 +554,35 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
   }
   if (timing)
     fprintf(stderr, "[radb200 LU n=%d %s] diag %.3f s, panel %.3f s, U block rows %.3f s, trailing %.3f s\n", n3,
-            sizeof(T) == 4 ? "fp32/tf32" : "fp64", tph[0], tph[1], tph[2], tph[3]);
+            sizeof(T) == 4 ? "fp32" : "fp64", tph[0], tph[1], tph[2], tph[3]);
+  if (timing_mode == 3 && !mk_ev.empty()) {
+    RB_CUDA(cudaEventSynchronize(mk_ev.back()));
+    double cat[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (size_t i = 1; i < mk_ev.size(); i++) {
+      float ms = 0.f;
+      RB_CUDA(cudaEventElapsedTime(&ms, mk_ev[i - 1], mk_ev[i]));
+      cat[mk_cat[i]] += 1e-3 * ms;
+    }
+    for (cudaEvent_t e : mk_ev) cudaEventDestroy(e);
+    fprintf(stderr,
+            "[radb200 LU n=%d %s] main stream: diagonal blocks %.4f s, L21 %.4f s, panel U12 %.4f s, narrow updates "
+            "%.4f s, waits for the side stream %.4f s, U block rows %.4f s, next panel's update %.4f s\n",
+            n3, sizeof(T) == 4 ? "fp32" : "fp64", cat[0], cat[1], cat[2], cat[3], cat[4], cat[5], cat[6]);
+  }
+  if (timing_mode == 2) {
+    const double host = std::chrono::duration<double>(std::chrono::steady_clock::now() - tq_host).count();
+    RB_CUDA(cudaEventRecord(tq1, st));
+    RB_CUDA(cudaEventSynchronize(tq1));
+    float ms = 0.f;
+    RB_CUDA(cudaEventElapsedTime(&ms, tq0, tq1));
+    fprintf(stderr,
+            "[radb200 LU n=%d %s] host enqueue %.3f s (panel GEMMs %.3f, trailing updates %.3f, diagonal blocks %.3f, "
+            "copies %.3f), device %.3f s\n",
+            n3, sizeof(T) == 4 ? "fp32" : "fp64", host, g_lu_host[0], g_lu_host[1], g_lu_host[2], g_lu_host[3], 1e-3 * ms);
+    g_lu_host_timing = false;
+    cudaEventDestroy(tq0);
+    cudaEventDestroy(tq1);
+  }
   return 0;
 }
 
