@@ -387,7 +387,8 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
                                                                       const __grid_constant__ CUtensorMap tmB,
                                                                       float *__restrict__ C, int ldc, int m, int n, int k,
                                                                       int *__restrict__ err, int overwrite,
-                                                                      const float *__restrict__ scale)
+                                                                      const float *__restrict__ row_scale,
+                                                                      const float *__restrict__ col_scale)
 {
   constexpr int KC = F16 ? 2 * TM_KC : TM_KC;  // K elements per stage
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -510,7 +511,6 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
     const int q = warp & 3, hc = warp >> 2;
     float *W = reinterpret_cast<float *>(sbase + TM_NST * TM_STAGE) + warp * 32 * 32;
     const int lr = lane >> 3, lc = (lane & 7) * 4;
-    const float osc = F16 ? __ldg(scale) : 1.0f;
     for (int i = 0; i < my_tiles; i++) {
       const int tile = blockIdx.x + i * gridDim.x;
       int row0, col0;
@@ -537,6 +537,11 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
         }
       };
       auto store_slice = [&](const float4 *cs, int sl) {
+        // FP16 operands: the accumulator carries the row and column factors
+        // (read only for columns inside C: the factors hold n + 8 entries)
+        const int gcs = cbase + 32 * sl + lc;
+        const float4 csc = (F16 && gcs < n) ? __ldg(reinterpret_cast<const float4 *>(col_scale + gcs))
+                                            : make_float4(1.f, 1.f, 1.f, 1.f);
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           uint32_t v[16];
@@ -558,9 +563,15 @@ __global__ void __launch_bounds__(TM_THREADS, 1) tc_update_tma_kernel(const __gr
         for (int rr = 0; rr < 8; rr++) {
           const int rl = 4 * rr + lr;
           float4 t = *reinterpret_cast<const float4 *>(W + rl * 32 + (((lane & 7) ^ (rl & 7)) << 2));
-          if (F16) { t.x *= osc; t.y *= osc; t.z *= osc; t.w *= osc; }
           const int gr = rbase + rl, gc = cbase + 32 * sl + lc;
           if (gr < m) {
+            if (F16) {
+              const float rsc = __ldg(row_scale + gr);
+              t.x *= rsc * csc.x;
+              t.y *= rsc * csc.y;
+              t.z *= rsc * csc.z;
+              t.w *= rsc * csc.w;
+            }
             const float4 c4 = cs[rr];
             const float4 o = overwrite ? t : make_float4(c4.x - t.x, c4.y - t.y, c4.z - t.z, c4.w - t.w);
             float *dst = C + (size_t)gr * ldc + gc;
@@ -643,29 +654,6 @@ __global__ void tc_transpose_kernel(const float *__restrict__ B, int ldb, int k,
 // ---- FP16 operands: power-of-two scaling against the FP16 range -------------
 // max |A| (m x k) and max |B| (k x n) into mx[0], mx[1] (float bits; non-
 // negative floats order as unsigned integers)
-__global__ void tc_absmax_kernel(const float *__restrict__ A, int lda, int m, int k, const float *__restrict__ B, int ldb,
-                                 int n, unsigned *__restrict__ mx)
-{
-  __shared__ float red[2][8];
-  float a = 0.f, b = 0.f;
-  const int64_t na = (int64_t)m * k, nbt = (int64_t)k * n;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < na; e += (int64_t)gridDim.x * blockDim.x)
-    a = fmaxf(a, fabsf(A[(e / k) * lda + e % k]));
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nbt; e += (int64_t)gridDim.x * blockDim.x)
-    b = fmaxf(b, fabsf(B[(e / n) * ldb + e % n]));
-  for (int o = 16; o > 0; o >>= 1) {
-    a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
-    b = fmaxf(b, __shfl_xor_sync(0xffffffffu, b, o));
-  }
-  if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = a; red[1][threadIdx.x >> 5] = b; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)blockDim.x / 32; w++) { a = fmaxf(a, red[0][w]); b = fmaxf(b, red[1][w]); }
-    atomicMax(mx, __float_as_uint(a));
-    atomicMax(mx + 1, __float_as_uint(b));
-  }
-}
-
 // the power of two that brings max |x| to at most 2^14 (1 for an all-zero operand)
 __device__ __forceinline__ float f16_scale(unsigned maxbits)
 {
@@ -676,45 +664,73 @@ __device__ __forceinline__ float f16_scale(unsigned maxbits)
   return ldexpf(1.f, 14 - e);
 }
 
-// Ah[r][c] = FP16(sA A[r][c]) for c < k, 0 for k <= c < kp
-__global__ void tc_f16_rows_kernel(const float *__restrict__ A, int lda, int m, int k, const unsigned *__restrict__ mx,
-                                   __half *__restrict__ Ah, int kp)
+// Ah[r][c] = FP16(s_r A[r][c]) for c < k, 0 for k <= c < kp, with s_r the
+// power of two that brings row r's largest magnitude to at most 2^14; irs[r] =
+// 1 / s_r (exact).  A warp per row: the maximum, then the conversion (the row
+// is read again from L1/L2).
+__global__ void tc_f16_rows_kernel(const float *__restrict__ A, int lda, int m, int k, __half *__restrict__ Ah, int kp,
+                                   float *__restrict__ irs)
 {
-  const float sa = f16_scale(mx[0]);
-  const int64_t tot = (int64_t)m * kp;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-    const int r = (int)(e / kp), c = (int)(e % kp);
-    Ah[e] = __float2half_rn(c < k ? sa * A[(size_t)r * lda + c] : 0.f);
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < m; r += nw) {
+    const float *row = A + (size_t)r * lda;
+    float mx = 0.f;
+    for (int c = lane; c < k; c += 32) mx = fmaxf(mx, fabsf(row[c]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const float sr = f16_scale(__float_as_uint(mx));
+    if (lane == 0) irs[r] = 1.f / sr;
+    __half2 *dst = reinterpret_cast<__half2 *>(Ah + (size_t)r * kp);
+    for (int c2 = lane; c2 < kp / 2; c2 += 32) {
+      const int c = 2 * c2;
+      dst[c2] = __floats2half2_rn(c < k ? sr * row[c] : 0.f, c + 1 < k ? sr * row[c + 1] : 0.f);
+    }
   }
 }
 
-// Bth[c][r] = FP16(sB B[r][c]) (n x kp, K contiguous)
-__global__ void tc_f16_transpose_kernel(const float *__restrict__ B, int ldb, int k, int n, const unsigned *__restrict__ mx,
-                                        __half *__restrict__ Bth, int kp)
+// Bth[c][r] = FP16(t_c B[r][c]) (n x kp, K contiguous), with t_c the power of
+// two that brings column c's largest magnitude to at most 2^14; ics[c] = 1 / t_c.
+// A block of 32 x 8 threads per 32 columns: the column maxima, then the
+// columns turned around 32 rows at a time through shared memory.
+__global__ void tc_f16_transpose_kernel(const float *__restrict__ B, int ldb, int k, int n, __half *__restrict__ Bth,
+                                        int kp, float *__restrict__ ics)
 {
   __shared__ float t[32][33];
-  const float sb = f16_scale(mx[1]);
-  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-  for (int i = threadIdx.y; i < 32; i += 8) {
-    const int r = r0 + i, c = c0 + threadIdx.x;
-    t[i][threadIdx.x] = (r < k && c < n) ? B[(size_t)r * ldb + c] : 0.f;
+  __shared__ float red[8][32];
+  __shared__ float sc[32];
+  const int c0 = blockIdx.x * 32, tx = threadIdx.x, ty = threadIdx.y;
+  const int c = c0 + tx;
+  float mx = 0.f;
+  if (c < n)
+    for (int r = ty; r < k; r += 8) mx = fmaxf(mx, fabsf(B[(size_t)r * ldb + c]));
+  red[ty][tx] = mx;
+  __syncthreads();
+  if (ty == 0) {
+    for (int i = 1; i < 8; i++) mx = fmaxf(mx, red[i][tx]);
+    const float tc = f16_scale(__float_as_uint(mx));
+    sc[tx] = tc;
+    if (c < n) ics[c] = 1.f / tc;
   }
   __syncthreads();
-  for (int i = threadIdx.y; i < 32; i += 8) {
-    const int c = c0 + i, r = r0 + threadIdx.x;
-    if (c < n && r < kp) Bth[(size_t)c * kp + r] = __float2half_rn(sb * t[threadIdx.x][i]);
+  for (int r0 = 0; r0 < kp; r0 += 32) {
+    for (int i = ty; i < 32; i += 8) {
+      const int r = r0 + i;
+      t[i][tx] = (r < k && c < n) ? B[(size_t)r * ldb + c] : 0.f;
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {
+      const int cc = c0 + i, r = r0 + tx;
+      if (cc < n && r < kp) Bth[(size_t)cc * kp + r] = __float2half_rn(sc[i] * t[tx][i]);
+    }
+    __syncthreads();
   }
 }
 
-// the epilogue's factor 1 / (sA sB)
-// also clears the two maxima for the next update on this slot (every kernel
-// that reads them runs before this one on the stream)
-__global__ void tc_f16_outscale_kernel(unsigned *__restrict__ mx, float *__restrict__ osc)
-{
-  osc[0] = 1.f / (f16_scale(mx[0]) * f16_scale(mx[1]));
-  mx[0] = 0u;
-  mx[1] = 0u;
-}
+// B^T scratch, [n x ldbt] floats, ldbt = k rounded up to 4; one per slot so
+// that updates on two streams (the LU's look-ahead) never share it
+static DBuf g_tc_bt_slots[2];
+// FP16 path, per slot: A and B^T copies, the row and column factors
+static DBuf g_tc_ah_slots[2], g_tc_bh_slots[2], g_tc_rs_slots[2], g_tc_cs_slots[2];
 
 // cudaFuncSetAttribute once per kernel and device (a driver call per launch
 // showed up in the LU's host enqueue time)
@@ -730,11 +746,6 @@ static int set_smem_once(K kernel, int bytes, int which)
   return 0;
 }
 
-// B^T scratch, [n x ldbt] floats, ldbt = k rounded up to 4; one per slot so
-// that updates on two streams (the LU's look-ahead) never share it
-static DBuf g_tc_bt_slots[2];
-// FP16 path, per slot: A and B^T copies, the two maxima and the output factor
-static DBuf g_tc_ah_slots[2], g_tc_bh_slots[2], g_tc_mx_slots[2];
 
 // max_ctas > 0 caps the persistent grid (the self-test uses it to make every
 // CTA loop over several tiles)
@@ -797,34 +808,26 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
   }
   int grid = (int)std::min<long long>(tiles, max_ctas > 0 ? max_ctas : nsm);
   if (use_tma == 2) {
-    // FP16 operands scaled into range (A is left as it is)
+    // FP16 operands, each row of A and each column of B scaled by a power of
+    // two into range (A and B are left as they are)
     const int kp = (k + 7) / 8 * 8;
-    DBuf &ah = g_tc_ah_slots[slot & 1], &bh = g_tc_bh_slots[slot & 1], &mx = g_tc_mx_slots[slot & 1];
+    DBuf &ah = g_tc_ah_slots[slot & 1], &bh = g_tc_bh_slots[slot & 1];
+    DBuf &rs = g_tc_rs_slots[slot & 1], &cs = g_tc_cs_slots[slot & 1];
     RB_TRY(ah.alloc((size_t)m * kp * sizeof(__half)));
     RB_TRY(bh.alloc((size_t)n * kp * sizeof(__half)));
-    if (!mx.p) {  // the maxima start at zero; tc_f16_outscale_kernel clears them after each update
-      RB_TRY(mx.alloc(4 * sizeof(unsigned)));
-      RB_CUDA(cudaMemsetAsync(mx.p, 0, 4 * sizeof(unsigned), st));
-    }
-    const int64_t tot = (int64_t)m * k + (int64_t)k * n;
-    const int nb = (int)std::min<int64_t>((tot + 255) / 256, 148 * 8);
-    tc_absmax_kernel<<<std::max(nb, 1), 256, 0, st>>>(A, lda, m, k, B, ldb, n, mx.as<unsigned>());
-    RB_TRY(check_launch("tc_absmax_kernel"));
-    const int nra = (int)std::min<int64_t>(((int64_t)m * kp + 255) / 256, 148 * 16);
-    tc_f16_rows_kernel<<<std::max(nra, 1), 256, 0, st>>>(A, lda, m, k, mx.as<unsigned>(), ah.as<__half>(), kp);
+    RB_TRY(rs.alloc((size_t)m * sizeof(float)));
+    RB_TRY(cs.alloc((size_t)(n + 8) * sizeof(float)));  // the epilogue reads 4 at a time past a ragged end
+    const int nra = (int)std::min<int64_t>(((int64_t)m + 7) / 8, 148 * 16);
+    tc_f16_rows_kernel<<<std::max(nra, 1), 256, 0, st>>>(A, lda, m, k, ah.as<__half>(), kp, rs.as<float>());
     RB_TRY(check_launch("tc_f16_rows_kernel"));
-    tc_f16_transpose_kernel<<<dim3((n + 31) / 32, (kp + 31) / 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, mx.as<unsigned>(),
-                                                                                     bh.as<__half>(), kp);
+    tc_f16_transpose_kernel<<<(n + 31) / 32, dim3(32, 8), 0, st>>>(B, ldb, k, n, bh.as<__half>(), kp, cs.as<float>());
     RB_TRY(check_launch("tc_f16_transpose_kernel"));
-    float *osc = reinterpret_cast<float *>(mx.as<unsigned>() + 2);
-    tc_f16_outscale_kernel<<<1, 1, 0, st>>>(mx.as<unsigned>(), osc);
-    RB_TRY(check_launch("tc_f16_outscale_kernel"));
     CUtensorMap ma, mb;
     RB_TRY(encode_map(&ma, ah.p, m, k, kp, TC_BM, true));
     RB_TRY(encode_map(&mb, bh.p, n, k, kp, TC_BN, true));
     RB_TRY(set_smem_once(tc_update_tma_kernel<true>, TM_SMEM, 0));
     tc_update_tma_kernel<true><<<grid, TM_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(),
-                                                                  overwrite, osc);
+                                                                  overwrite, rs.as<float>(), cs.as<float>());
     return check_launch("tc_update_tma_kernel<f16>");
   }
   RB_TRY(g_tc_bt.alloc((size_t)n * ldbt * sizeof(float)));
@@ -842,7 +845,7 @@ static int launch_tc(float *C, int ldc, int m, int n, int k, float *A, int lda, 
     RB_TRY(encode_map(&mb, g_tc_bt.as<float>(), n, k, ldbt, TC_BN));
     RB_TRY(set_smem_once(tc_update_tma_kernel<false>, TM_SMEM, 1));
     tc_update_tma_kernel<false><<<grid, TM_THREADS, TM_SMEM, st>>>(ma, mb, C, ldc, m, n, k, g_tc_err_flag.as<int>(),
-                                                                   overwrite, nullptr);
+                                                                   overwrite, nullptr, nullptr);
     return check_launch("tc_update_tma_kernel");
   }
   RB_TRY(set_smem_once(tc_update_kernel, TC_SMEM, 2));
