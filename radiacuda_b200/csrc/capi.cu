@@ -47,11 +47,19 @@ int check_launch(const char *what)
 // block of that device to the driver and tries again;
 // radb200_release_cached_memory returns all of them.  Blocks are keyed by
 // device ordinal and the pool is guarded by a mutex, so host threads and
-// device switches do not mix blocks up.  The pool is never destroyed (blocks
-// outlive static DBufs).
+// device switches do not mix blocks up.  A large block released when the
+// cache is full displaces the least recently released blocks of its device (a
+// workload that changes its buffer sizes, e.g. from FP64 to FP32 matrices,
+// keeps its new blocks instead of paying cudaMalloc and cudaFree every time).
+// The pool is never destroyed (blocks outlive static DBufs).
 namespace {
+struct BigBlock {
+  void *p;
+  uint64_t seq;  // release order
+};
 struct BigPool {
-  std::map<int, std::multimap<size_t, void *>> blocks;      // device -> size -> block (large)
+  std::map<int, std::multimap<size_t, BigBlock>> blocks;    // device -> size -> block (large)
+  uint64_t seq = 0;
   std::map<int, std::map<size_t, std::vector<void *>>> small;  // device -> class -> blocks
   size_t total = 0, cap = 0, small_total = 0, small_cap = 0;
   bool init = false;
@@ -89,7 +97,7 @@ void big_flush(BigPool &bp, int dev)
   for (auto it = bp.blocks.begin(); it != bp.blocks.end();) {
     if (dev >= 0 && it->first != dev) { ++it; continue; }
     if (it->first != cur) cudaSetDevice(it->first);
-    for (auto &kv : it->second) { cudaFree(kv.second); bp.total -= kv.first; }
+    for (auto &kv : it->second) { cudaFree(kv.second.p); bp.total -= kv.first; }
     if (it->first != cur) cudaSetDevice(cur);
     it = bp.blocks.erase(it);
   }
@@ -139,7 +147,7 @@ void *pool_alloc(size_t b, size_t *got)
     auto &mine = bp.blocks[dev];
     auto it = mine.lower_bound(b);
     if (it != mine.end() && it->first <= b + b / 4) {
-      void *p = it->second;
+      void *p = it->second.p;
       *got = it->first;
       bp.total -= it->first;
       mine.erase(it);
@@ -171,10 +179,21 @@ void pool_free(void *p, size_t b)
       bp.small_total += b;
       return;
     }
-  } else if (bp.total + b <= bp.cap && cudaDeviceSynchronize() == cudaSuccess) {
-    bp.blocks[current_device()].emplace(b, p);
-    bp.total += b;
-    return;
+  } else if (b <= bp.cap && cudaDeviceSynchronize() == cudaSuccess) {
+    auto &mine = bp.blocks[current_device()];
+    while (bp.total + b > bp.cap && !mine.empty()) {  // make room: the oldest blocks go
+      auto old = mine.begin();
+      for (auto it = mine.begin(); it != mine.end(); ++it)
+        if (it->second.seq < old->second.seq) old = it;
+      cudaFree(old->second.p);
+      bp.total -= old->first;
+      mine.erase(old);
+    }
+    if (bp.total + b <= bp.cap) {
+      mine.emplace(b, BigBlock{p, ++bp.seq});
+      bp.total += b;
+      return;
+    }
   }
   cudaGetLastError();
   cudaFree(p);
