@@ -834,8 +834,8 @@ def RlxAuto(intrc: int, prec: float, maxiter: int, meth: int = 4, *opts) -> list
     """Automatic relaxation (radpy RlxAuto).  meth 3/4/5/8/9/10 run the
     device-resident Jacobi/Anderson solver (same fixed point as the
     reference's methods), 11 the Newton-Krylov solver.  New: 12 = dense FP64
-    LU direct solve, 13 = TF32 tensor-core LU + FP64 GMRES refinement (linear
-    materials only).  Options 'ZeroM->True|False', 'omega->x'.
+    LU direct solve, 13 = FP32 LU with tensor-core updates (FP16 or TF32
+    operands) + FP64 GMRES refinement (linear materials only).  Options 'ZeroM->True|False', 'omega->x'.
     Returns [misfit, max|M|, max|H|, iterations]."""
     it = _get(intrc, Interaction)
     reset, omega = True, 0.0
