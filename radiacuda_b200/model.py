@@ -333,7 +333,7 @@ class Container(Obj):
 # --------------------------------------------------------------------------
 # flattening
 # --------------------------------------------------------------------------
-@dataclass
+@dataclass(slots=True)
 class Leaf:
     handle: int
     obj: Obj
@@ -343,20 +343,32 @@ class Leaf:
 def collect_leaves(objs: Dict[int, Obj], handle: int,
                    outer: Optional[List[Tuple[int, Trf]]] = None,
                    out: Optional[List[Leaf]] = None) -> List[Leaf]:
-    """Depth-first walk in Radia's order (radintrc.cpp:249-345)."""
+    """Depth-first walk in Radia's order (radintrc.cpp:249-345).  Leaves
+    without transformations of their own share their container's list (the
+    lists are only read)."""
     if outer is None:
         outer = []
     if out is None:
         out = []
-    o = objs.get(handle)
-    if o is None:
-        raise RadiaError(f"Radia::Error002: unknown element {handle}")
-    lst = outer + o.trfs
-    if isinstance(o, Container):
+    get = objs.get
+    append = out.append
+
+    def walk(h: int, outer_l: List[Tuple[int, Trf]]) -> None:
+        o = get(h)
+        if o is None:
+            raise RadiaError(f"Radia::Error002: unknown element {h}")
+        lst = outer_l + o.trfs if o.trfs else outer_l
+        if not isinstance(o, Container):
+            append(Leaf(h, o, lst))
+            return
         for m in o.members:
-            collect_leaves(objs, m, lst, out)
-    else:
-        out.append(Leaf(handle, o, lst))
+            c = get(m)
+            if c is not None and not c.trfs and not isinstance(c, Container):
+                append(Leaf(m, c, lst))
+            else:
+                walk(m, lst)
+
+    walk(handle, outer)
     return out
 
 
@@ -580,6 +592,19 @@ def _m_slots(kinds_objs):
             ("poly", 3, np.array(poly_rows, dtype=np.int64), poly_objs)]
 
 
+def _mat_groups(relax_leaves):
+    """Element rows of each material object, with the elements' objects."""
+    groups: Dict[int, tuple] = {}
+    for e, lf in enumerate(relax_leaves):
+        mat = lf.obj.mat
+        g = groups.get(id(mat))
+        if g is None:
+            g = groups[id(mat)] = (mat, [], [])
+        g[1].append(e)
+        g[2].append(lf.obj)
+    return [(mat, np.array(rows, dtype=np.int64), objs_g) for mat, rows, objs_g in groups.values()]
+
+
 def pack_interaction(objs, handle, srcobj, rand) -> InteractionPack:
     """Relaxable elements, their materials and the external sources of the
     object tree under handle (plus srcobj).  Cached like pack_sources: the
@@ -592,15 +617,19 @@ def pack_interaction(objs, handle, srcobj, rand) -> InteractionPack:
     fp = _int_key(leaves + sleaves)
     hit = _INT_CACHE.get(key)
     if hit is not None and hit[0].shape == fp.shape and np.array_equal(hit[0], fp):
-        _, pack, eslots, xslots, _ = hit
+        _, pack, eslots, xslots, _, mgroups = hit
         _refresh_m(pack.elems, eslots)
         if pack.ext is not None:
             _refresh_m(pack.ext, xslots)
         mats = pack.mat
-        for e, lf in enumerate(pack.leaves):
-            o = lf.obj
-            if o.mat.kind != 2:
-                mats[e] = o.mat.record(o.m)
+        for mat, rows, objs_g in mgroups:
+            if mat.kind == 2:
+                continue
+            if mat.kind == 0 and mat.mr is not None:  # one record for all its elements
+                mats[rows] = mat.record(None)
+            else:
+                for e, o in zip(rows, objs_g):
+                    mats[e] = mat.record(o.m)
         return InteractionPack(
             elems={k: v.copy() for k, v in pack.elems.items()},
             ext=({k: v.copy() for k, v in pack.ext.items()} if pack.ext is not None else None),
@@ -647,7 +676,7 @@ def pack_interaction(objs, handle, srcobj, rand) -> InteractionPack:
         leaves=relax_leaves, main=mains)
     if len(_INT_CACHE) >= _SRC_CACHE_MAX:
         _INT_CACHE.pop(next(iter(_INT_CACHE)))
-    _INT_CACHE[key] = (fp, pack, _m_slots(eko), _m_slots(xko), leaves + sleaves)
+    _INT_CACHE[key] = (fp, pack, _m_slots(eko), _m_slots(xko), leaves + sleaves, _mat_groups(relax_leaves))
     return InteractionPack(
         elems={k: v.copy() for k, v in pack.elems.items()},
         ext=({k: v.copy() for k, v in pack.ext.items()} if pack.ext is not None else None),
