@@ -302,10 +302,16 @@ static void build_topo_range(const RadB200Geom *G, bool tensor, int pa, int pb, 
     int f0 = G->poly_info[4 * pg], nf = G->poly_info[4 * pg + 1];
     const double *M = G->poly + (size_t)pg * RADB200_POLY_STRIDE + 3;
     int v0 = (int)(h.tv.size() / 3), e0 = (int)h.tel.size(), t0 = (int)h.tt.size(), ff0 = (int)(h.tfn.size() / 3);
-    std::vector<double> V;  // local vertices
-    std::vector<std::vector<int>> loops(nf);
+    // per-polyhedron scratch, reused across polyhedra of this thread (cleared,
+    // capacity kept: a 20,000-tetrahedron model otherwise makes ~10^5 small
+    // allocations per upload)
+    static thread_local std::vector<double> V, Pall;  // local vertices; every face's vertices in 3-D
+    static thread_local std::vector<std::vector<int>> loops;
+    V.clear();
+    Pall.clear();
+    loops.resize(nf);  // exactly nf loops: build_tet_record scans all of them
+    for (int k = 0; k < nf; k++) loops[k].clear();
     // every face's vertices back in 3-D: P = R^T (x, y, coordZ)
-    std::vector<double> Pall;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (int k = 0; k < nf; k++) {
       const double *R = G->face + (size_t)(f0 + k) * RADB200_FACE_STRIDE;
@@ -351,8 +357,11 @@ static void build_topo_range(const RadB200Geom *G, bool tensor, int pa, int pb, 
       continue;
     }
     h.tv.insert(h.tv.end(), V.begin(), V.end());
-    std::vector<int2> edges;
-    std::vector<double> g_e, G_e;
+    static thread_local std::vector<int2> edges;
+    static thread_local std::vector<double> g_e, G_e;
+    edges.clear();
+    g_e.clear();
+    G_e.clear();
     for (int k = 0; k < nf; k++) {
       const double *R = G->face + (size_t)(f0 + k) * RADB200_FACE_STRIDE;
       double n[3] = {R[6], R[7], R[8]};
