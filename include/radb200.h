@@ -330,17 +330,27 @@ RADB200_API int radb200_relax(int64_t handle, int method, double prec, int max_i
                   double *status);
 
 /* ---- dense direct solve (linear materials) --- no counterpart in the reference.
- * Solves (I - X N) M = X H_ext + Mr by a blocked LU of A = I - X N on the
- * device.  mode: RADB200_LU_F64 = FP64 LU (+ one FP64 refinement step);
- * RADB200_LU_TF32 = LU with TF32 tensor-core trailing updates (tcgen05,
- * FP32 accumulate) followed by FP64 GMRES iterative refinement to rtol.
- * The factorization is kept with the interaction for later solves (adjoint).
- * status: [4] = final relative FP64 residual, refinement (GMRES) iterations,
- * factor seconds, total seconds.                                             */
+ * Solves (I - X N) M = X H_ext + Mr by a blocked unpivoted LU of
+ * A = I - X N on the device, then FP64 GMRES on A (the FP64 operator) with
+ * the factors as right preconditioner, to rtol.  mode: RADB200_LU_F64 = FP64
+ * factors; RADB200_LU_TF32 = FP32 factors whose updates run on the tcgen05
+ * tensor cores (FP16 operands scaled per row and column by powers of two, or
+ * TF32 operands; FP32 accumulation).  A pivot at or below 1e-12 of the
+ * largest |A_ii| makes the factorization restart on A + sigma I (sigma = 1e-3
+ * of that scale, at least 1e-3); GMRES still solves with A, so the shifted
+ * factors only precondition it (radb200_lu_shift reports sigma).  For
+ * chi >= 0 this never happens.  The factorization is kept with the
+ * interaction for later solves (adjoint).  status: [4] = final relative FP64
+ * residual, refinement (GMRES) iterations, factor seconds, total seconds.
+ * RADB200_E_NUMERIC when A + sigma I also meets such a pivot.               */
 #define RADB200_LU_F64  0
 #define RADB200_LU_TF32 1
 RADB200_API int radb200_direct_solve(int64_t handle, int mode, double rtol, int max_iter,
                          double *M_out, double *status);
+
+/* The diagonal shift sigma of the interaction's current factorization: 0 when
+ * the factors are of A itself.                                               */
+RADB200_API int radb200_lu_shift(int64_t handle, double *sigma);
 
 /* ---- adjoint --- no counterpart in the reference.
  * Given the converged magnetization of the last solve and dL/dM [3N] (each

@@ -47,6 +47,7 @@ def lib():
         L.radb200_intrc_set_extfield.argtypes = [_i64, _dp]
         L.radb200_relax.argtypes = [_i64, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, _dp, _dp, _dp]
         L.radb200_direct_solve.argtypes = [_i64, C.c_int, C.c_double, C.c_int, _dp, _dp]
+        L.radb200_lu_shift.argtypes = [_i64, _dp]
         L.radb200_adjoint_solve.argtypes = [_i64, _dp, C.c_double, C.c_int, _dp, _dp]
         L.radb200_adjoint_grad.argtypes = [_i64, _dp, _dp, _dp, _dp, _dp]
         L.radb200_field_vjp.argtypes = [_i64, _dp, _dp, _i64, C.c_int, _dp, _dp, _dp, _dp]
@@ -217,6 +218,12 @@ class NativeInteraction:
         st = np.zeros(4)
         check(lib().radb200_direct_solve(self.handle, mode, rtol, max_iter, _p(M), _p(st)), "radb200_direct_solve")
         return M, st
+
+    def lu_shift(self) -> float:
+        """sigma of the current factorization (A + sigma I), 0 for A itself."""
+        v = C.c_double(0.0)
+        check(lib().radb200_lu_shift(self.handle, C.byref(v)), "radb200_lu_shift")
+        return v.value
 
     def adjoint_solve(self, dLdM: np.ndarray, rtol: float = 1e-12, max_iter: int = 500):
         g = np.ascontiguousarray(dLdM, dtype=np.float64)

@@ -1137,6 +1137,15 @@ int radb200_direct_solve(int64_t handle, int mode, double rtol, int max_iter, do
   return 0;
 }
 
+int radb200_lu_shift(int64_t handle, double *sigma)
+{
+  Intrc *I = find_intrc(handle);
+  if (!I) return RADB200_E_HANDLE;
+  if (!sigma) { set_error("null sigma"); return RADB200_E_ARG; }
+  *sigma = I->lu_mode >= 0 ? I->lu_shift : 0.0;
+  return 0;
+}
+
 int radb200_adjoint_solve(int64_t handle, const double *dLdM, double rtol, int max_iter, double *lambda_out, double *status)
 {
   Intrc *I = find_intrc(handle);

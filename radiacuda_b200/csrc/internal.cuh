@@ -221,6 +221,7 @@ struct Intrc {
   int lu_tc = 0;                      // the factorization ran on the tensor cores
   int lu_mode = -1;                   // factors valid for this mode (-1 none)
   int lu_of_d = 0;                    // 1: the factors are of I - D N at the converged state of solve lu_solve_id
+  double lu_shift = 0.0;              // sigma when the factors are of A + sigma I (a pivot fell below the threshold)
   int lu_solve_id = -1;
   int solve_id = 0;                   // counts relaxations / direct solves on this interaction
   uint64_t stamp = 0;                 // hash of the element records, frames and materials

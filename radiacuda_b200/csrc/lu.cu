@@ -390,7 +390,7 @@ struct LuStreams {
 static LuStreams g_lu_streams;
 
 template <typename T>
-static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaStream_t st, int *tc_used)
+static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, double tiny, cudaStream_t st, int *tc_used)
 {
   const int n3 = I.n3, ld = I.ld;
   RB_CUDA(cudaFuncSetAttribute(diag_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
@@ -491,7 +491,7 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, cudaS
       const int jb = std::min(LU_NB, pend - j0);
       {
         LuHostSpan hs(2);
-        diag_factor_kernel<T><<<1, DG_T, DG_SMEM, sm>>>(A, ld, j0, jb, Linv, Uinv, d_err);
+        diag_factor_kernel<T><<<1, DG_T, DG_SMEM, sm>>>(A, ld, j0, jb, Linv, Uinv, d_err, tiny);
         RB_TRY(check_launch("diag_factor_kernel"));
       }
       RB_TRY(mark(0));
@@ -957,15 +957,41 @@ int lu_build(Intrc &I, int mode, double *factor_seconds)
   return lu_build_x(I, mode, I.mat.as<double>(), 0, factor_seconds);
 }
 
+// max |A_ii| (as float bits: non-negative floats order like their bits)
+template <typename T>
+__global__ void diag_absmax_kernel(const T *__restrict__ A, int ld, int n3, unsigned *__restrict__ out)
+{
+  float m = 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x)
+    m = fmaxf(m, (float)fabs((double)A[(size_t)i * ld + i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+template <typename T>
+__global__ void add_diag_kernel(T *__restrict__ A, int ld, int n3, double sigma)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n3) A[(size_t)i * ld + i] = (T)((double)A[(size_t)i * ld + i] + sigma);
+}
+
+// Pivots at or below LU_TINY of the largest |A_ii| stop the unpivoted
+// factorization; it is then redone on A + sigma I, sigma = LU_SHIFT of that
+// scale (at least LU_SHIFT), and the FP64 GMRES that refines every solve --
+// always with the unshifted operator -- takes the shifted factors as its
+// preconditioner.  For physical materials (chi >= 0) A is diagonally similar
+// to a symmetric positive-definite matrix, so every leading minor is positive
+// and the shift is never needed; it covers unphysical inputs (a negative
+// susceptibility that zeroes a self block) and rounding.
+constexpr double LU_TINY = 1e-12, LU_SHIFT = 1e-3;
+
 int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_seconds)
 {
   auto t0 = std::chrono::steady_clock::now();
   const int n3 = I.n3, ld = I.ld;
   I.lu_mode = -1;
   I.drop_lu_graphs();
-  DBuf err;
-  RB_TRY(err.alloc(sizeof(int)));
-  RB_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+  DBuf err;  // [pivot flag, max |A_ii| as float bits]
   dim3 bgrid((ld + 255) / 256 > 64 ? 64 : (ld + 255) / 256, n3);
   int tc_used = 0;
   size_t es = (mode == RADB200_LU_F64) ? sizeof(double) : sizeof(float);
@@ -974,27 +1000,63 @@ int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_sec
   if (mode == RADB200_LU_F64) {
     I.LU32.release();
     RB_TRY(I.LU64.alloc((size_t)n3 * ld * sizeof(double)));
-    if (I.N64.p) build_A_kernel<double, double><<<bgrid, 256>>>(I.N64.as<double>(), X, n3, ld, I.LU64.as<double>());
-    else build_A_kernel<double, float><<<bgrid, 256>>>(I.N32.as<float>(), X, n3, ld, I.LU64.as<double>());
-    RB_TRY(check_launch("build_A_kernel"));
-    double *inv = I.LUinv.as<double>();
-    RB_TRY(lu_factor<double>(I, I.LU64.as<double>(), inv, inv + (size_t)n3 * LU_NB, I.lu_scratch.as<double>(), err.as<int>(), 0,
-                             &tc_used));
   } else {
     I.LU64.release();
     RB_TRY(I.LU32.alloc((size_t)n3 * ld * sizeof(float)));
-    if (I.N64.p) build_A_kernel<float, double><<<bgrid, 256>>>(I.N64.as<double>(), X, n3, ld, I.LU32.as<float>());
-    else build_A_kernel<float, float><<<bgrid, 256>>>(I.N32.as<float>(), X, n3, ld, I.LU32.as<float>());
-    RB_TRY(check_launch("build_A_kernel"));
-    float *inv = I.LUinv.as<float>();
-    RB_TRY(lu_factor<float>(I, I.LU32.as<float>(), inv, inv + (size_t)n3 * LU_NB, I.lu_scratch.as<float>(), err.as<int>(), 0,
-                            &tc_used));
   }
+  RB_TRY(err.alloc(2 * sizeof(int)));
+  double tiny = 0.0;
+  I.lu_shift = 0.0;
   int herr = 0, tcflag = 0;
-  RB_CUDA(cudaMemcpy(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost));
-  RB_TRY(tc_error_flag(&tcflag));
-  if (tcflag) { I.lu_mode = -1; set_error("LU: a tensor-core update timed out waiting for its MMAs"); return RADB200_E_TIMEOUT; }
-  if (herr) { I.lu_mode = -1; set_error("LU: vanishing pivot (matrix not factorable without pivoting)"); return RADB200_E_NUMERIC; }
+  for (int attempt = 0; attempt < 2; attempt++) {
+    RB_CUDA(cudaMemset(err.p, 0, 2 * sizeof(int)));
+    unsigned *mx = reinterpret_cast<unsigned *>(err.as<int>() + 1);
+    const int nb = std::min((n3 + 255) / 256, 148 * 4);
+    if (mode == RADB200_LU_F64) {
+      if (I.N64.p) build_A_kernel<double, double><<<bgrid, 256>>>(I.N64.as<double>(), X, n3, ld, I.LU64.as<double>());
+      else build_A_kernel<double, float><<<bgrid, 256>>>(I.N32.as<float>(), X, n3, ld, I.LU64.as<double>());
+      RB_TRY(check_launch("build_A_kernel"));
+      if (attempt) add_diag_kernel<double><<<(n3 + 255) / 256, 256>>>(I.LU64.as<double>(), ld, n3, I.lu_shift);
+      else diag_absmax_kernel<double><<<nb, 256>>>(I.LU64.as<double>(), ld, n3, mx);
+    } else {
+      if (I.N64.p) build_A_kernel<float, double><<<bgrid, 256>>>(I.N64.as<double>(), X, n3, ld, I.LU32.as<float>());
+      else build_A_kernel<float, float><<<bgrid, 256>>>(I.N32.as<float>(), X, n3, ld, I.LU32.as<float>());
+      RB_TRY(check_launch("build_A_kernel"));
+      if (attempt) add_diag_kernel<float><<<(n3 + 255) / 256, 256>>>(I.LU32.as<float>(), ld, n3, I.lu_shift);
+      else diag_absmax_kernel<float><<<nb, 256>>>(I.LU32.as<float>(), ld, n3, mx);
+    }
+    RB_TRY(check_launch(attempt ? "add_diag_kernel" : "diag_absmax_kernel"));
+    if (!attempt) {
+      unsigned bits = 0;
+      RB_CUDA(cudaMemcpy(&bits, mx, sizeof(unsigned), cudaMemcpyDeviceToHost));
+      float scale = 0.f;
+      memcpy(&scale, &bits, sizeof(float));
+      tiny = LU_TINY * (double)scale;
+      if (!(tiny > 1e-300)) tiny = 1e-300;
+    }
+    if (mode == RADB200_LU_F64) {
+      double *inv = I.LUinv.as<double>();
+      RB_TRY(lu_factor<double>(I, I.LU64.as<double>(), inv, inv + (size_t)n3 * LU_NB, I.lu_scratch.as<double>(),
+                               err.as<int>(), tiny, 0, &tc_used));
+    } else {
+      float *inv = I.LUinv.as<float>();
+      RB_TRY(lu_factor<float>(I, I.LU32.as<float>(), inv, inv + (size_t)n3 * LU_NB, I.lu_scratch.as<float>(),
+                              err.as<int>(), tiny, 0, &tc_used));
+    }
+    RB_CUDA(cudaMemcpy(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    RB_TRY(tc_error_flag(&tcflag));
+    if (tcflag) { I.lu_mode = -1; set_error("LU: a tensor-core update timed out waiting for its MMAs"); return RADB200_E_TIMEOUT; }
+    if (!herr) break;
+    I.lu_shift = LU_SHIFT * std::max(1.0, tiny / LU_TINY);
+    if (timing_on())
+      fprintf(stderr, "RADB200_TIMING LU: pivot at or below %.3e; refactoring A + %.3e I\n", tiny, I.lu_shift);
+  }
+  if (herr) {
+    I.lu_mode = -1;
+    I.lu_shift = 0.0;
+    set_error("LU: vanishing pivot (A and A + sigma I not factorable without pivoting)");
+    return RADB200_E_NUMERIC;
+  }
   RB_TRY(tri_sync_alloc(I));
   I.lu_mode = mode;
   I.lu_of_d = of_d;

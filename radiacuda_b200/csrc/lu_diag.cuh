@@ -99,7 +99,7 @@ __device__ __forceinline__ void dg_store(double *O, int ldo, const DgAcc &a, dou
 constexpr int DG_FW = 8;               // warps of the sweep
 constexpr int DG_FR = DG_B / DG_FW;    // rows per warp
 __device__ __forceinline__ void dg_factor(double *D, double *LI, double *UI, double *rowA, double *rowX, int w, int lane,
-                                          int *err)
+                                          int *err, double tiny)
 {
   double a[DG_FR], x[DG_FR], y[DG_FR];
 #pragma unroll
@@ -119,7 +119,7 @@ __device__ __forceinline__ void dg_factor(double *D, double *LI, double *UI, dou
       }
       asm volatile("bar.sync 1, %0;" ::"n"(32 * DG_FW) : "memory");
       const double u = ra[lane], piv = ra[k], xk = rx[lane];
-      if (w == 0 && lane == 0 && !(fabs(piv) > 1e-300)) *err = 1;
+      if (w == 0 && lane == 0 && !(fabs(piv) > tiny)) *err = 1;
       const double ip = 1.0 / piv;
 #pragma unroll
       for (int i = 0; i < DG_FR; i++) {
@@ -150,10 +150,11 @@ __device__ __forceinline__ void dg_factor(double *D, double *LI, double *UI, dou
 
 // Factor the nb x nb block at (k0, k0) of A (row pitch ld) in place into L\U;
 // write L^-1 (unit lower) and U^-1 to rows k0.. of Linv and Uinv (pitch DG_N,
-// zero beyond column nb).  err[0] = 1 on a pivot of magnitude <= 1e-300.
+// zero beyond column nb).  err[0] = 1 on a pivot of magnitude <= tiny (or not
+// finite).
 template <typename T>
 __global__ void __launch_bounds__(DG_T) diag_factor_kernel(T *__restrict__ A, int ld, int k0, int nb, T *__restrict__ Linv,
-                                                           T *__restrict__ Uinv, int *__restrict__ err)
+                                                           T *__restrict__ Uinv, int *__restrict__ err, double tiny)
 {
   extern __shared__ double dg_smem[];
   double *S = dg_smem;                  // DG_N x DG_P
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(DG_T) diag_factor_kernel(T *__restrict__ A, in
   }
   __syncthreads();
 
-  if (warp < DG_FW) dg_factor(blk(0, 0), inv(LI, 0), inv(UI, 0), rowA, rowX, warp, lane, err);
+  if (warp < DG_FW) dg_factor(blk(0, 0), inv(LI, 0), inv(UI, 0), rowA, rowX, warp, lane, err, tiny);
   for (int b = 0; b < DG_NS; b++) {
     __syncthreads();
     const int m = DG_NS - 1 - b;  // sub-blocks below and right of b
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(DG_T) diag_factor_kernel(T *__restrict__ A, in
     }
     __syncthreads();
     if (warp < DG_FW) {
-      dg_factor(blk(b + 1, b + 1), inv(LI, b + 1), inv(UI, b + 1), rowA, rowX, warp, lane, err);
+      dg_factor(blk(b + 1, b + 1), inv(LI, b + 1), inv(UI, b + 1), rowA, rowX, warp, lane, err, tiny);
     } else {
       for (int t = warp - DG_FW + 4; t < 4 * m * m; t += DG_T / 32 - DG_FW) {
         const int q = t % 4, s = t / 4, i = b + 1 + s / m, j = b + 1 + s % m;  // t < 4: the diagonal sub-block, done
