@@ -43,7 +43,8 @@ namespace rb {
 // skipped (the derivative is singular there).
 __device__ __forceinline__ void cuboid_dQ(V3<double> q, V3<double> hd, const double *w, double *dq, double *dh)
 {
-  const double C = 1.0 / (4.0 * 3.14159265358979);
+  // the cuboid form's full-precision pi (radrec.cpp:130), as in the forward cuboid term
+  const double C = 1.0 / (4.0 * 3.141592653589793238);
   double gq0 = 0, gq1 = 0, gq2 = 0, gh0 = 0, gh1 = 0, gh2 = 0;
 #pragma unroll
   for (int c = 0; c < 8; c++) {

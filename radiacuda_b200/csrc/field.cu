@@ -81,6 +81,7 @@ __device__ __forceinline__ V3<double> eval_unit(const GeomView &g, int4 u, V3<do
     const double *pr = g.poly + (size_t)u.y * RADB200_POLY_STRIDE;
     double mx = __ldg(pr + 3), my = __ldg(pr + 4), mz = __ldg(pr + 5);
     int f0 = __ldg(g.poly_info + 4 * u.y), nf = __ldg(g.poly_info + 4 * u.y + 1);
+    // the reference's polygon face form uses this 15-digit pi (radplnr2.cpp:32)
     const double CH = 1.0 / (4.0 * 3.14159265358979);
     int inside = 1;
     double hx = 0, hy = 0, hz = 0;

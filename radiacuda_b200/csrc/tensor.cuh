@@ -41,6 +41,7 @@ __device__ __forceinline__ void elem_tensor(const GeomView &g, int kind, int idx
     else poly_fast<double, true>(g.tp, idx, q, Q);
     return;
   }
+  // the reference's polygon face form uses this 15-digit pi (radplnr2.cpp:32)
   const double CH = 1.0 / (4.0 * 3.14159265358979);
   int f0 = __ldg(g.poly_info + 4 * idx), nf = __ldg(g.poly_info + 4 * idx + 1);
 #pragma unroll
