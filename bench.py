@@ -649,7 +649,7 @@ FIELD_OPS_PER_TET = 4 * 16 + 6 * 5 + 6 * 40 + 4 * 51 + 3
 
 # Instructions the FP32 field kernel issues per (point, tetrahedron) pair,
 # from ncu's smsp__inst_executed.sum x 32 / pairs on the 20,000-point,
-# 20,000-tetrahedron case (profiles/field_tet_kernel_f32_20k_tets.md), and
+# 20,000-tetrahedron case (tests/profile_cases.py field --precision single), and
 # their split over the pipes.  The kernel is issue-bound: its roofline is the
 # SMs' issue rate, 4 warp-instructions (128 thread-instructions) per clock
 # per SM, divided by these instructions per pair.
