@@ -262,7 +262,7 @@ def run_ours(args, rank, world):
     if not e2e:
         e2e = [float("nan")]
 
-    # roofline of the LU trailing update (tcgen05 GEMM, K = 768): its flops
+    # roofline of the LU trailing update (tcgen05 GEMM, K = the panel width): its flops
     # (2 m^2 K per launch) over the event-timed launch durations, against the
     # dense rate of its operand type (FP16: the measured bf16 rate; TF32: half
     # of it); the HBM side (C read + written, panels once) beside it
@@ -282,9 +282,11 @@ def run_ours(args, rank, world):
     upd_tflops = upd_f.value / max(upd_s.value, 1e-30) / 1e12
     upd_gbs = upd_b.value / max(upd_s.value, 1e-30) / 1e9
     upd_bytes_per_launch = upd_b.value / max(upd_n.value, 1)
-    roof_upd = {"kernel": ("tc_update_tma_kernel<FP16 operands> (LU trailing update A22 -= L21 U12, K = 768; "
-                           "operands scaled by powers of two, FP32 accumulation)" if f16_ops else
-                           "tc_update_tma_kernel<TF32 operands> (LU trailing update A22 -= L21 U12, K = 768)"),
+    roof_upd = {"kernel": ("tc_update_tma_kernel<FP16 operands> (LU trailing update A22 -= L21 U12, K = 1024, "
+                           "then 768 for the last 30,000 rows; operands scaled per row and column by powers of two, "
+                           "FP32 accumulation)" if f16_ops else
+                           "tc_update_tma_kernel<TF32 operands> (LU trailing update A22 -= L21 U12, K = 1024, "
+                           "then 768 for the last 30,000 rows)"),
                 "bound": "tensor",
                 "achieved": round(upd_tflops, 1), "peak": round(tf32_peak, 1), "unit": "TFLOP/s",
                 "frac": round(upd_tflops / tf32_peak, 4),

@@ -8,7 +8,8 @@
 // positive semi-definite, so A is (close to) positive definite and needs no
 // row exchanges; a vanishing pivot is reported as RADB200_E_NUMERIC.
 //
-// Two levels: outer panels of 768 columns, 128-wide steps inside.  Step k
+// Two levels: outer panels of 1024 columns (768 for the last 30,000 rows),
+// 128-wide steps inside.  Step k
 // (width nb = 128) inside a panel:
 //   1. one CTA factors the diagonal block in shared memory (FP64) and writes
 //      the inverses of its unit-lower and upper triangles, L_kk^-1 and U_kk^-1
@@ -17,7 +18,7 @@
 //      place, then copied back), so the triangular solves of the panel also
 //      run on the GEMM engine; a narrow update of the panel's other columns.
 // After the panel: its U block row by block forward substitution, then one
-// trailing update A22 -= L21 U12 with K = 768, split into the next panel's
+// trailing update A22 -= L21 U12 with K = the panel width, split into the next panel's
 // columns (main stream) and the rest (a side stream, overlapping the next
 // panel's factorization).
 //   mode F64  : FP64 factors, GEMMs on the FP64 pipe (CUDA cores).
@@ -351,18 +352,39 @@ static double g_upd_bytes = 0.0, g_upd_flops = 0.0;
 // forward substitution over its 128-row sub-blocks, and the trailing matrix
 // receives ONE update with K = LU_OUTER: the C traffic of the dominant GEMM
 // drops by LU_OUTER / 128 against 128-wide steps.
-constexpr int LU_OUTER_DEFAULT = 768;  // swept 512, 768, 1024 on the 60,000^2 factorization
+// Outer panel widths: 1024 columns while at least LU_LATE_AT_DEFAULT rows
+// remain, then 768.  The trailing GEMMs dominate the early panels (a wider K
+// raises their rate: 489 -> 533 TFLOP/s), the main stream's panel chain the
+// late ones.  Swept on the 60,000^2 factorization (solve, s): 768 throughout
+// 0.494; 1024 then 768 below 20,000 / 30,000 / 40,000 rows 0.482 / 0.481 /
+// 0.482; 1280 then 768 0.482; 1536 then 768 0.487; 1024 then 512 0.495;
+// 1024 then 640 0.493; 1280 then 1024 0.497.
+constexpr int LU_OUTER_DEFAULT = 1024, LU_OUTER_LATE_DEFAULT = 768, LU_LATE_AT_DEFAULT = 30000;
 // the outer panel width: LU_OUTER_DEFAULT, or RADB200_LU_OUTER (a multiple of
-// 128 from 256 to 2048) for tuning
+// 128 from 256 to 2048) for tuning; RADB200_LU_OUTER_LATE (same range) is the
+// width once fewer than RADB200_LU_LATE_AT rows remain (tuning: the trailing
+// GEMMs dominate the early panels, the panel chain the late ones)
+static int lu_width_env(const char *name, int dflt)
+{
+  const char *e = getenv(name);
+  int v = e ? atoi(e) : dflt;
+  return (v >= 256 && v <= 2048 && v % LU_NB == 0) ? v : dflt;
+}
 static int lu_outer()
 {
   static int w = 0;
-  if (!w) {
-    const char *e = getenv("RADB200_LU_OUTER");
-    int v = e ? atoi(e) : LU_OUTER_DEFAULT;
-    w = (v >= 256 && v <= 2048 && v % LU_NB == 0) ? v : LU_OUTER_DEFAULT;
-  }
+  if (!w) w = lu_width_env("RADB200_LU_OUTER", LU_OUTER_DEFAULT);
   return w;
+}
+static int lu_outer_at(int remaining)
+{
+  static int late = 0, at = -1;
+  if (!late) {
+    late = lu_width_env("RADB200_LU_OUTER_LATE", LU_OUTER_LATE_DEFAULT);
+    const char *e = getenv("RADB200_LU_LATE_AT");
+    at = e ? std::max(0, atoi(e)) : LU_LATE_AT_DEFAULT;
+  }
+  return remaining < at ? late : lu_outer();
 }
 
 // One-panel look-ahead: the trailing update of outer step k is split into the
@@ -481,9 +503,8 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, doubl
     }
     return 0;
   };
-  const int LU_OUTER = lu_outer();
-  for (int K0 = 0; K0 < n3; K0 += LU_OUTER) {
-    const int NBe = std::min(LU_OUTER, n3 - K0);
+  for (int K0 = 0, NBe = 0; K0 < n3; K0 += NBe) {
+    NBe = std::min(lu_outer_at(n3 - K0), n3 - K0);
     const int pend = K0 + NBe;  // end of the panel's columns
     // ---- factor the panel columns [K0, pend) over rows [K0, n3) (main stream;
     // the previous step updated these columns there first)
@@ -535,7 +556,7 @@ static int lu_factor(Intrc &I, T *A, T *Linv, T *Uinv, T *tmp, int *d_err, doubl
     RB_TRY(phase(2));
     // ---- trailing update A22 -= L21 U12 with K = NBe: the next panel's
     // columns on the main stream, the rest on the side stream
-    const int nxt = lookahead ? std::min(LU_OUTER, mT) : mT;
+    const int nxt = lookahead ? std::min(lu_outer_at(mT), mT) : mT;  // the next panel's width
     RB_TRY(update(at(T0, T0), mT, nxt, NBe, at(T0, K0), at(K0, T0), sm, 0, 0));
     RB_TRY(mark(6));
     if (mT > nxt) {
