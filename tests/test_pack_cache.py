@@ -61,3 +61,26 @@ def test_interaction_cache_follows_magnetization_and_materials(rad):
     cached = model.pack_interaction(rad._objs, h, 0, rand)
     model.clear_source_cache()
     assert _same_pack(cached, model.pack_interaction(rad._objs, h, 0, rand))
+
+
+def test_interaction_cache_refreshes_magnetization_dependent_records(rad):
+    """A linear material given by |Mr| takes its easy axis from each element's
+    magnetization, so its records change with M on a cache hit; a material
+    with a fixed Mr vector shares one record among its elements."""
+    h = MD.mixed_sym(rad)
+    rand = tuple(rad._rand)
+    leaves = model.collect_leaves(rad._objs, h)
+    half = len(leaves) // 2
+    m_abs = rad.MatLin([0.3, 0.1], 1.1)               # easy axis along each element's M
+    m_vec = rad.MatLin([0.05, 0.15], [0.0, 0.6, 0.8])  # fixed easy axis
+    for k, lf in enumerate(leaves):
+        lf.obj.m = np.array([0.3, 0.1 * (k + 1), 0.5])  # the |Mr| law needs a magnetization to take its axis from
+        rad.MatApl(lf.handle, m_abs if k < half else m_vec)
+    model.pack_interaction(rad._objs, h, 0, rand)
+    for k, lf in enumerate(leaves):
+        lf.obj.m = np.array([np.cos(0.3 * k), np.sin(0.3 * k), 0.2])
+    cached = model.pack_interaction(rad._objs, h, 0, rand)
+    model.clear_source_cache()
+    fresh = model.pack_interaction(rad._objs, h, 0, rand)
+    assert _same_pack(cached, fresh)
+    assert not np.array_equal(cached.mat[0], cached.mat[1])  # the |Mr| records differ per element
