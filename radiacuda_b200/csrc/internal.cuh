@@ -218,6 +218,7 @@ struct Intrc {
   DBuf LU32, LU64, lu_scratch;
   DBuf LUinv;                         // [2][3N x 128] inverses of the diagonal blocks (L, then U)
   DBuf tri_sync;                      // counters and flags of the one-launch triangular sweeps
+  DBuf sweep_m;                       // FP32 factors: per block Linv_k L_{k,k-1}, then Uinv_k U_{k,k+1} (128 x 128 each)
   int lu_tc = 0;                      // the factorization ran on the tensor cores
   int lu_mode = -1;                   // factors valid for this mode (-1 none)
   int lu_of_d = 0;                    // 1: the factors are of I - D N at the converged state of solve lu_solve_id

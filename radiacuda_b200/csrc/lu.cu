@@ -666,7 +666,7 @@ template <typename T> constexpr int tri_rows() { return sizeof(T) == 4 ? 16 : 8;
 
 template <typename T, bool UPPER>
 __global__ void __launch_bounds__(256, 2) tri_sweep_kernel(const T *__restrict__ A, int ld, const T *__restrict__ Inv, int n3,
-                                                        double *x, int *sync, int *err)
+                                                        double *x, int *sync, int *err, const float *__restrict__ Msub)
 {
   constexpr int NR = tri_rows<T>(), NB = LU_NB / (8 * NR);  // rows per batch, batches
   constexpr bool STAGE_INV = sizeof(T) == 4;  // Inv_k in shared memory (dynamic, LU_NB^2 floats)
@@ -687,16 +687,23 @@ __global__ void __launch_bounds__(256, 2) tri_sweep_kernel(const T *__restrict__
     // this warp's rows: (warp * NB + batch) * NR + i, accumulated in shared
     // memory by the warp's lane 0 (every row belongs to one warp)
     if (threadIdx.x < LU_NB) acc_s[threadIdx.x] = threadIdx.x < nb ? x[k0 + threadIdx.x] : 0.0;
-    // the diagonal block's inverse, needed last, on the chain's critical path:
-    // staged now (visible after the barriers below), while the chain is
-    // still far from this block
-    if (STAGE_INV)
+    // with coupling blocks (FP32 factors, Msub): everything but the block
+    // before this one in sweep order is done first and multiplied by the
+    // inverse while that block is solved; x_k = y_k - M_k x_j then remains
+    const bool use_m = STAGE_INV && Msub != nullptr && t > 0;
+    // the matrix needed last, on the chain's critical path (M_k, or the
+    // diagonal block's inverse): staged now (visible after the barriers
+    // below), while the chain is still far from this block
+    if constexpr (STAGE_INV) {
+      const float *src = use_m ? Msub + (size_t)k * LU_NB * LU_NB : Inv + (size_t)k0 * LU_NB;
       for (int e = threadIdx.x; e < LU_NB * LU_NB / 4; e += blockDim.x) {
         const int r = e / (LU_NB / 4);
-        sinv4[e] = r < nb ? __ldg(reinterpret_cast<const float4 *>(Inv + (size_t)(k0 + r) * LU_NB) + (e % (LU_NB / 4)))
-                          : make_float4(0.f, 0.f, 0.f, 0.f);
+        sinv4[e] = (use_m || r < nb) ? __ldg(reinterpret_cast<const float4 *>(src + (size_t)r * LU_NB) + (e % (LU_NB / 4)))
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
       }
-    for (int s = 0; s < t; s++) {
+    }
+    const int s_end = use_m ? t - 1 : t;
+    for (int s = 0; s < s_end; s++) {
       const int j = UPPER ? nblk - 1 - s : s;
       const int j0 = j * LU_NB, nbj = min(LU_NB, n3 - j0);
       const bool full = (nbj == LU_NB);
@@ -754,6 +761,59 @@ __global__ void __launch_bounds__(256, 2) tri_sweep_kernel(const T *__restrict__
           }
       }
     }
+    if (use_m) {
+      // y_k = Inv_k acc into acc_s (Inv_k through L2: off the chain)
+      __syncthreads();
+      if (threadIdx.x < LU_NB) xs[threadIdx.x] = threadIdx.x < nb ? acc_s[threadIdx.x] : 0.0;
+      __syncthreads();
+#pragma unroll
+      for (int b = 0; b < NB; b++) {
+        RowSlice<T> v[NR];
+#pragma unroll
+        for (int i = 0; i < NR; i++) {
+          const int r = (warp * NB + b) * NR + i;
+          if (r < nb) v[i].load(Inv + (size_t)(k0 + r) * LU_NB, lane);
+          else v[i].zero();
+        }
+#pragma unroll
+        for (int i = 0; i < NR; i++) {
+          const int r = (warp * NB + b) * NR + i;
+          const double w = warp_sum(v[i].dot(xs, lane));
+          if (lane == 0) acc_s[r] = w;
+        }
+      }
+      // the block before this one in sweep order
+      const int j = UPPER ? k + 1 : k - 1;
+      const int j0 = j * LU_NB, nbj = min(LU_NB, n3 - j0);
+      if (threadIdx.x == 0) {
+        long long it = 0;
+        while (ld_acquire_s32(flags + j) == 0) {
+          if (++it > TRI_SPIN || ld_acquire_s32(err) != 0) { s_bad = 1; atomicExch(err, 1); break; }
+        }
+      }
+      __syncthreads();  // the flag seen; every warp done with xs
+      if (s_bad) return;
+      if (threadIdx.x < LU_NB) xs[threadIdx.x] = threadIdx.x < nbj ? __ldcg(x + j0 + threadIdx.x) : 0.0;
+      __syncthreads();
+#pragma unroll
+      for (int b = 0; b < NB; b++) {
+        RowSlice<T> v[NR];
+#pragma unroll
+        for (int i = 0; i < NR; i++) v[i].set(sinv4[((warp * NB + b) * NR + i) * (LU_NB / 4) + lane]);
+#pragma unroll
+        for (int i = 0; i < NR; i++) {
+          const int r = (warp * NB + b) * NR + i;
+          const double w = warp_sum(v[i].dot(xs, lane));
+          if (lane == 0 && r < nb) x[k0 + r] = acc_s[r] - w;
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        st_release_s32(flags + k, 1);
+      }
+      continue;
+    }
     // x_k = Inv_k acc (rows of Inv beyond nb hold zero columns)
     __syncthreads();
     if (threadIdx.x < LU_NB) xs[threadIdx.x] = threadIdx.x < nb ? acc_s[threadIdx.x] : 0.0;
@@ -785,12 +845,77 @@ __global__ void __launch_bounds__(256, 2) tri_sweep_kernel(const T *__restrict__
   }
 }
 
+// Coupling blocks of FP32 factors for the sweeps: Mf[k] = Linv_k L_{k,k-1}
+// (k >= 1) and Mb[k] = Uinv_k U_{k,k+1} (k < nblk - 1), 128 x 128 each, rows
+// beyond block k's size and columns beyond its neighbour's zero.  With them a
+// sweep finishes block k as x_k = y_k - M_k x_j once x_j of the block before
+// it (in sweep order) appears, y_k = Inv_k (b_k - the other products) having
+// been formed while waiting.  One CTA per block and direction, FP32 products
+// of 128 terms, 8 x 8 outputs per thread.
+__global__ void __launch_bounds__(256) sweep_m_kernel(const float *__restrict__ A, int ld, const float *__restrict__ Linv,
+                                                      const float *__restrict__ Uinv, int n3, float *__restrict__ Mf,
+                                                      float *__restrict__ Mb)
+{
+  __shared__ float sI[LU_NB][33];      // 32 columns of the inverse
+  __shared__ float sB[32][LU_NB + 4];  // the matching 32 rows of the coupling block
+  const int nblk = (n3 + LU_NB - 1) / LU_NB;
+  const int k = blockIdx.x >> 1, upper = blockIdx.x & 1;
+  if (upper ? k >= nblk - 1 : k < 1) return;
+  const int k0 = k * LU_NB, nb = min(LU_NB, n3 - k0);
+  const int j0 = (upper ? k + 1 : k - 1) * LU_NB, nbj = min(LU_NB, n3 - j0);
+  const float *Inv = (upper ? Uinv : Linv) + (size_t)k0 * LU_NB;
+  float *out = (upper ? Mb : Mf) + (size_t)k * LU_NB * LU_NB;
+  const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int c = 0; c < 8; c++) acc[i][c] = 0.f;
+  for (int q0 = 0; q0 < LU_NB; q0 += 32) {
+    for (int e = threadIdx.x; e < LU_NB * 32; e += 256) {
+      const int r = e / 32, q = e % 32;
+      sI[r][q] = r < nb ? Inv[(size_t)r * LU_NB + q0 + q] : 0.f;
+      const int qr = e / LU_NB, c = e % LU_NB;
+      sB[qr][c] = (q0 + qr < nb && c < nbj) ? A[(size_t)(k0 + q0 + qr) * ld + j0 + c] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < 32; q++) {
+      float a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) a[i] = sI[tr * 8 + i][q];
+#pragma unroll
+      for (int c = 0; c < 8; c++) b[c] = sB[q][tc * 8 + c];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int c = 0; c < 8; c++) acc[i][c] = fmaf(a[i], b[c], acc[i][c]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int c = 0; c < 8; c++) out[(size_t)(tr * 8 + i) * LU_NB + tc * 8 + c] = acc[i][c];
+}
+
 // RADB200_TRI_SWEEP=0: the per-block launches below instead (A/B comparisons)
 static bool tri_sweep_enabled()
 {
   static int on = -1;
   if (on < 0) {
     const char *e = getenv("RADB200_TRI_SWEEP");
+    on = (e && atoi(e) == 0) ? 0 : 1;
+  }
+  return on == 1;
+}
+
+// RADB200_SWEEP_M=0: FP32 sweeps without coupling blocks (A/B comparisons)
+static bool sweep_m_enabled()
+{
+  static int on = -1;
+  if (on < 0) {
+    const char *e = getenv("RADB200_SWEEP_M");
     on = (e && atoi(e) == 0) ? 0 : 1;
   }
   return on == 1;
@@ -820,7 +945,7 @@ static int tri_sync_alloc(Intrc &I)
 
 template <typename T>
 static int lu_solve_sweeps(const T *A, const T *Linv, const T *Uinv, int n3, int ld, double *x, int *sync,
-                           cudaStream_t st)
+                           const float *Mf, const float *Mb, cudaStream_t st)
 {
   const int nblk = (n3 + LU_NB - 1) / LU_NB;
   const size_t per = (size_t)nblk + 1;
@@ -829,9 +954,9 @@ static int lu_solve_sweeps(const T *A, const T *Linv, const T *Uinv, int n3, int
   // FP32 factors: the inverses staged in dynamic shared memory (the limit is
   // raised in tri_sync_alloc, before any capture)
   const size_t dyn = sizeof(T) == 4 ? (size_t)LU_NB * LU_NB * sizeof(float) : 0;
-  tri_sweep_kernel<T, false><<<grid, 256, dyn, st>>>(A, ld, Linv, n3, x, sync, g_tri_err.as<int>());
+  tri_sweep_kernel<T, false><<<grid, 256, dyn, st>>>(A, ld, Linv, n3, x, sync, g_tri_err.as<int>(), Mf);
   RB_TRY(check_launch("tri_sweep_kernel"));
-  tri_sweep_kernel<T, true><<<grid, 256, dyn, st>>>(A, ld, Uinv, n3, x, sync + per, g_tri_err.as<int>());
+  tri_sweep_kernel<T, true><<<grid, 256, dyn, st>>>(A, ld, Uinv, n3, x, sync + per, g_tri_err.as<int>(), Mb);
   return check_launch("tri_sweep_kernel");
 }
 
@@ -846,9 +971,10 @@ int tri_sweep_error(int *flag)
 }
 
 template <typename T>
-static int lu_solve(const T *A, const T *Linv, const T *Uinv, int n3, int ld, double *x, int *sync, cudaStream_t st)
+static int lu_solve(const T *A, const T *Linv, const T *Uinv, int n3, int ld, double *x, int *sync, cudaStream_t st,
+                    const float *Mf = nullptr, const float *Mb = nullptr)
 {
-  if (sync && tri_sweep_enabled()) return lu_solve_sweeps<T>(A, Linv, Uinv, n3, ld, x, sync, st);
+  if (sync && tri_sweep_enabled()) return lu_solve_sweeps<T>(A, Linv, Uinv, n3, ld, x, sync, Mf, Mb, st);
   for (int k0 = 0; k0 < n3; k0 += LU_NB) {
     int nb = std::min(LU_NB, n3 - k0);
     block_matvec_kernel<T><<<1, 256, 0, st>>>(Linv, k0, nb, x);
@@ -883,7 +1009,10 @@ static int lu_solve_direct(Intrc &I, int transposed, double *x, cudaStream_t st)
   if (I.lu_mode == RADB200_LU_TF32) {
     const float *L = I.LUinv.as<float>(), *U = L + (size_t)n3 * LU_NB;
     return transposed ? lu_solve_t<float>(I.LU32.as<float>(), L, U, n3, ld, x, st)
-                      : lu_solve<float>(I.LU32.as<float>(), L, U, n3, ld, x, I.tri_sync.as<int>(), st);
+                      : lu_solve<float>(I.LU32.as<float>(), L, U, n3, ld, x, I.tri_sync.as<int>(), st,
+                                        I.sweep_m.p ? I.sweep_m.as<float>() : nullptr,
+                                        I.sweep_m.p ? I.sweep_m.as<float>() + (size_t)((n3 + LU_NB - 1) / LU_NB) * LU_NB * LU_NB
+                                                    : nullptr);
   }
   set_error("no LU factors on this interaction");
   return RADB200_E_ARG;
@@ -1079,6 +1208,15 @@ int lu_build_x(Intrc &I, int mode, const double *X, int of_d, double *factor_sec
     return RADB200_E_NUMERIC;
   }
   RB_TRY(tri_sync_alloc(I));
+  I.sweep_m.release();
+  if (mode != RADB200_LU_F64 && sweep_m_enabled() && n3 > LU_NB) {
+    const int nblk = (n3 + LU_NB - 1) / LU_NB;
+    RB_TRY(I.sweep_m.alloc(2 * (size_t)nblk * LU_NB * LU_NB * sizeof(float)));
+    const float *inv = I.LUinv.as<float>();
+    float *Mf = I.sweep_m.as<float>(), *Mb = Mf + (size_t)nblk * LU_NB * LU_NB;
+    sweep_m_kernel<<<2 * nblk, 256>>>(I.LU32.as<float>(), ld, inv, inv + (size_t)n3 * LU_NB, n3, Mf, Mb);
+    RB_TRY(check_launch("sweep_m_kernel"));
+  }
   I.lu_mode = mode;
   I.lu_of_d = of_d;
   I.lu_solve_id = I.solve_id;
