@@ -142,9 +142,11 @@ RADB200_API int radb200_update_stats(int64_t *launches, double *seconds, double 
  * roofline denominator of the transcendental-bound assembly / field kernels. */
 RADB200_API int radb200_measure_fma_peak(int fp64, double *tflops);
 /* Diagnostics, no counterpart in the reference: runs (once) the self-test of
- * the tcgen05 TF32 GEMM kernels of the LU against a CUDA-core GEMM.
- * state: 0 tensor-core path disabled, 1 the cp.async-fed kernel in use,
- * 2 the TMA-fed kernel in use; err: max relative deviation seen.            */
+ * the LU's tcgen05 GEMM kernels against a CUDA-core GEMM.
+ * state: 0 tensor-core path disabled, 1 the cp.async-fed kernel (TF32) in
+ * use, 2 the TMA-fed kernel with TF32 operands, 3 the TMA-fed kernel with
+ * FP16 operands scaled per row and column; err: max relative deviation seen
+ * by the first kernel of the chain.                                         */
 RADB200_API int radb200_tc_selftest(int *state, double *err);
 
 /* ---- field evaluation ------------------------------------------------------
@@ -358,7 +360,7 @@ RADB200_API int radb200_lu_shift(int64_t handle, double *sigma);
  * with D = dM/dH at the converged state (radmater.cpp:206-277) and returns
  * lambda [3N], by FP64 GMRES on the transposed operator preconditioned with
  * A^T = U^T L^T: the kept factors of the direct solve (linear materials), or
- * otherwise a factorization of A = I - D N (TF32 tensor cores above 3,072
+ * otherwise a factorization of A = I - D N (on the tensor cores above 3,072
  * unknowns), kept until the next solve.  status: [4] = final relative
  * residual, GMRES iterations, 1 if LU-preconditioned (0: block-Jacobi split
  * after a factorization breakdown), seconds.                                */

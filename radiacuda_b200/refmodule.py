@@ -22,7 +22,9 @@ import numpy as np
 
 MODULE_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "shim", "_ref")
 
-_LU_MODES = {"f64": 0, "tf32": 1}
+# "tf32" (the ABI's name, RADB200_LU_TF32) and "mixed" select the FP32 factors
+# with tensor-core updates (FP16 or TF32 operands, whichever passed the self-test)
+_LU_MODES = {"f64": 0, "tf32": 1, "mixed": 1}
 
 
 def module_path() -> str:
